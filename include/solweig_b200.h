@@ -1,0 +1,274 @@
+/*
+ * solweig_b200.h -- C ABI of the B200 (sm_100a) SOLWEIG radiation chain.
+ *
+ * Plain C: pointers, sizes and POD tables.  Every entry point returns 0 on
+ * success or a non-zero status (a CUDA error code, or SW100_E_* below); the
+ * message of the last failure on the calling thread is available from
+ * sw100_last_error().  No entry point aborts the process, and none allocates
+ * device memory: scratch space is a caller-provided `workspace` whose size
+ * the matching *_workspace_bytes() query returns.
+ *
+ * Memory: unless a parameter is documented as a host pointer, array
+ * arguments are DEVICE pointers on the current device.  Rasters are
+ * row-major float32 (rows, cols), npix = rows * cols.  Patch bit cubes are
+ * word-planar: word w of pixel i of cube k lives at
+ * bits[(k * SW100_CUBE_WORDS + w) * npix + i]; bit (p & 31) of word (p >> 5)
+ * is patch p.  `stream` is a cudaStream_t (NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside Synn-Arch/Solweig_Project):
+ *   sw100_svf_sweep   <- solweig_gpu/shadow.py:409-625 svf_calculator, with
+ *                        shadow.py:166-322 shadow() for each patch; native
+ *                        counterpart native/cuda/src/sw_api.cu:209-250
+ *                        (sw_run_march_svf_shadow per patch + sw_run_fold)
+ *   sw100_sun_march   <- solweig_gpu/solweig.py:1079-1224
+ *                        shadowingfunction_wallheight_23 (one call per
+ *                        daytime step); native counterpart
+ *                        native/cuda/src/sw_api.cu:218-228
+ *                        (sw_run_march_wallheight23)
+ *   sw100_time_loop   <- solweig_gpu/utci_process.py:917-1067, the time loop
+ *                        of run_utci_window around Solweig_2022a_calc
+ *                        (solweig_gpu/solweig.py:1950-2311) and
+ *                        utci_calculator; native counterpart
+ *                        native/cuda/src/sw_api.cu:253-344 (sw_run_rad_day,
+ *                        sw_run_rad_night, sw_utci_*)
+ *   sw100_utci        <- solweig_gpu/calculate_utci.py:259-330 utci_calculator;
+ *                        native counterpart native/cuda/src/sw_api.cu:327-344
+ *   sw100_abi_version, sw100_last_error
+ *                     <- native/cuda/src/sw_api.cu:29-37 (sw_last_error,
+ *                        sw_abi_version)
+ */
+#ifndef SOLWEIG_B200_H
+#define SOLWEIG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SW100_ABI_VERSION 1
+
+#define SW100_MAX_PATCHES 160   /* patch option 2 uses 153 */
+#define SW100_MAX_RINGS 16
+#define SW100_MAX_ANNULI 16     /* annuli per altitude band (12 in option 2) */
+#define SW100_CUBE_WORDS 5      /* ceil(153 / 32) */
+#define SW100_MAX_CLASSES 8     /* land-cover property classes */
+#define SW100_N_GVF_AZ 18       /* ground view factor search azimuths */
+#define SW100_MAX_GVF_STEPS 64  /* bound on the `second` walk length */
+#define SW100_SVF_PLANES 16     /* 15 SVF planes + SVFtotal */
+
+/* status codes beyond CUDA's */
+#define SW100_E_ARG 1001         /* invalid argument */
+#define SW100_E_SIZE 1002        /* size outside the supported range */
+#define SW100_E_WORKSPACE 1003   /* workspace missing or too small */
+
+/* One executed step of a march: source offset (dx rows, dy cols) and the
+ * float32 height drop dz, built on the host with the reference's float32
+ * trigonometry so that the executed sequence is bit-identical. */
+typedef struct {
+  int32_t dx;
+  int32_t dy;
+  float dz;
+  int32_t pad;
+} sw100_step;
+
+/* ------------------------------------------------------- site planes -- */
+/* Per-site rasters (device pointers, npix each unless noted). */
+typedef struct {
+  const float* dsm;          /* building DSM `a` */
+  const float* vegdsm;       /* canopy top (trees + dsm, 0 where no tree) */
+  const float* vegdsm2;      /* trunk zone top (0.25 trees + dsm) */
+  const float* bush;         /* may be NULL when all zero */
+  float vmax;                /* max over dsm, vegdsm, vegdsm2 (march early exit) */
+  int32_t bush_any;          /* bush.max() > 0 */
+  /* time-loop statics */
+  const float* svfbuveg;     /* svf - (1 - svfveg) * (1 - transVeg) */
+  const float* hsvf;         /* tan(acos(sqrt(svf))), float32 as the reference rounds it */
+  const float* tan_alfa;     /* tan(svfalfa), svfalfa = asin(exp(log(1 - tmp) / 2)) */
+  const float* buildings;    /* 1 ground, 0 building (dsm - dem < 2) */
+  const float* walls;        /* wall height */
+  const float* aspect_rad;   /* wall aspect * pi / 180 */
+  const float* tgk;          /* land-cover TgK, Tstart, albedo, emissivity */
+  const float* tstart;
+  const float* alb;
+  const float* emis;
+  const uint8_t* class_idx;  /* index into sw100_time_step.tg_factor per pixel */
+  const float* windcoeff;
+  const uint32_t* bits;      /* 3 cubes from sw100_svf_sweep: sh, vegsh, vbshvegsh */
+  /* patches whose SVF march ran at most one step: there vbshvegsh is 1 or 2
+   * and its cube bit means "vbshvegsh == 1"; elsewhere it means "!= 0" */
+  uint32_t single_step[SW100_CUBE_WORDS];
+} sw100_site_planes;
+
+/* ---------------------------------------------------------------- SVF -- */
+typedef struct {
+  int32_t n_patches;                          /* 153 */
+  int32_t n_rings;                            /* 8 */
+  int32_t bush_any;                           /* bush.max() > 0 */
+  int32_t pad0;
+  int32_t step_offset[SW100_MAX_PATCHES];     /* into the step table */
+  int32_t step_count[SW100_MAX_PATCHES];
+  int32_t ring[SW100_MAX_PATCHES];            /* altitude band of the patch */
+  int32_t dir_flags[SW100_MAX_PATCHES];       /* bit0 E, 1 S, 2 W, 3 N */
+  int32_t ring_annuli[SW100_MAX_RINGS];       /* annuli per band */
+  float w_iso[SW100_MAX_RINGS][SW100_MAX_ANNULI];
+  float w_aniso[SW100_MAX_RINGS][SW100_MAX_ANNULI];
+  float tail;                                 /* 3.0459e-4 (shadow.py:587) */
+  float trans;                                /* 0.03 (shadow.py:612) */
+} sw100_svf_plan;
+
+/* out_planes: SW100_SVF_PLANES * npix floats in the reference's 19-tuple
+ * order without the cubes, then SVFtotal: svf, svfaveg, svfE, svfEaveg,
+ * svfEveg, svfN, svfNaveg, svfNveg, svfS, svfSaveg, svfSveg, svfveg, svfW,
+ * svfWaveg, svfWveg, svftotal.  out_bits: 3 cubes (sh, vegsh, vbshvegsh).
+ * plan and steps are device copies of the host tables. */
+int sw100_svf_workspace_bytes(int rows, int cols, int n_steps, int64_t* bytes);
+int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                    const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
+                    void* workspace, int64_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------ time series -- */
+typedef struct {
+  int32_t step_offset;     /* into the sun step table */
+  int32_t step_count;
+  int32_t facesh_mode;     /* 0: az-90 >= 0 and az+90 < 2pi ; 1: wrapped */
+  float facesh_lo;         /* float32 thresholds on the wall aspect (rad) */
+  float facesh_hi;
+  float psi_term;          /* (1 - psi) as float32 */
+  int32_t t;               /* time-step index of this daytime row */
+  int32_t pad;
+} sw100_sun_step;
+
+typedef struct {
+  int8_t dx[SW100_MAX_GVF_STEPS];
+  int8_t dy[SW100_MAX_GVF_STEPS];
+  int32_t facesh_mode;
+  float facesh_lo;
+  float facesh_hi;
+  int32_t dir_flags;        /* bit0 E, 1 S, 2 W, 3 N */
+} sw100_gvf_azimuth;
+
+/* per patch and step: increments of the 153-patch sums in the reference's
+ * association (solweig.py:683-731 Kside, :1514-1635 define_patch) */
+typedef struct {
+  float kside_d[4];         /* ((diffsh * lumChi) * anglIncC) * ster; index sh * 2 + vegsh */
+  float anilum[4];          /* diffsh * lv */
+  float kref_veg;           /* (shaded_surface * ster) * cos(alt) */
+  float kref_sun;           /* (sunlit_surface * ster) * cos(alt) */
+  float kref_sh;            /* (shaded_surface * ster) * cos(alt) */
+  float yi_k;               /* yi_ of shaded_or_sunlit, Kside call (float32) */
+  float yi_l;               /* yi_ of shaded_or_sunlit, Lcyl call (float32) */
+  float thr_sun;            /* sunlit <=> hsvf + yi < thr_sun */
+  float thr_shd;            /* shaded <=> hsvf + yi > thr_shd */
+  float ld_sky;             /* Lsky_down[p] */
+  float ls_sky;             /* Lsky_side[p] */
+  float ster;
+  float cos_alt;
+  float sin_alt;
+  float sun_cos;            /* (sunlit wall surface * ster) * cos(alt) */
+  float sun_sin;
+  int32_t flags;            /* bit0: Lcyl sunlit/shaded branch taken */
+  int32_t pad;
+  double veg_cos;           /* (vegetation_surface * ster) * cos(alt), float64 */
+  double veg_sin;
+  double sh_cos;            /* (shaded_surface * ster) * cos(alt), float64 */
+  double sh_sin;
+} sw100_patch_step;
+
+typedef struct {
+  int32_t is_day;
+  int32_t day_row;          /* row of this step in the sun-march output, -1 at night */
+  int32_t tw_mode;          /* TsWaveDelay: 1 -> Tgmap1 updated, 0 -> lag only */
+  int32_t tw_first;         /* firstdaytime == 1 at this step */
+  float tw_a;               /* (1 - weight1) */
+  float tw_b;               /* weight1 */
+  float ta32;               /* Ta as float32 */
+  float ta4;                /* (Ta + 273.15) ** 4 as float32 */
+  float sbc;                /* 5.67051e-8 as float32 */
+  float altmax32;
+  float cig;                /* CI_TgG as float32 */
+  float lwall;              /* Lwall of sunonsurface_2018a */
+  float radI, radD, radG;   /* float32 */
+  float sin_alt;            /* float32(sin(altitude)) for Kdown / Kup */
+  float cos_alt;            /* float32(cos(altitude)) for KsideI */
+  float albedo_b;
+  float first, second;      /* ground-view-factor walk lengths (rounded) */
+  float tan_beta;           /* tan(zen) float32 for cylindric_wedge */
+  float qa;                 /* tan(beta) / 2 */
+  float refl_k;             /* (1 - ewall) as float32 */
+  float night_lup_base;     /* night: float32 (0 + Ta) + 0 + 273.15 */
+  float absK, absL, Fside, Fup, Fcyl;
+  float absl_sbc;           /* absL * SBC (float32) */
+  float rh32;               /* RH for UTCI */
+  float ws32;               /* wind speed */
+  float ta_mat;             /* float32(Ta) + float32(uhii) */
+  int32_t landcover;        /* Tg = max(Tg, 0) when land cover is used */
+  float tg_factor[SW100_MAX_CLASSES]; /* sin(...) of the Tg wave per TmaxLST class */
+  int32_t pad1;
+  /* UTCI polynomial of this step in (D = Tmrt - Ta, va):
+   * utci = sum_i D^i sum_j utci_c[i * 7 + j] va^j, coefficients folded from
+   * the 210-term regression with this step's Ta and Pa */
+  double utci_c[49];
+} sw100_time_step;
+
+/* All tables of one site's time loop (device pointers). */
+typedef struct {
+  const sw100_time_step* steps;     /* n_t */
+  int32_t n_t;
+  int32_t n_day;
+  const sw100_sun_step* sun;        /* n_day */
+  const sw100_step* sun_table;      /* concatenated sun-march step tables */
+  const sw100_patch_step* patch;    /* n_t * n_patches */
+  int32_t n_patches;
+  int32_t pad;
+  const sw100_gvf_azimuth* gvf;     /* SW100_N_GVF_AZ */
+} sw100_series;
+
+/* Output selection bits for sw100_time_loop (reference variable names). */
+#define SW100_OUT_UTCI   (1 << 0)
+#define SW100_OUT_TMRT   (1 << 1)
+#define SW100_OUT_KUP    (1 << 2)
+#define SW100_OUT_KDOWN  (1 << 3)
+#define SW100_OUT_LUP    (1 << 4)
+#define SW100_OUT_LDOWN  (1 << 5)
+#define SW100_OUT_SHADOW (1 << 6)
+
+/* Sun march for every daytime row of the series in one launch.  Writes the
+ * per-row ground-view-factor source records (4 floats per pixel:
+ * shadow, Lup, albedo, flag bits) to gsrc (n_day * npix * 4 floats) and,
+ * when debug8 is non-NULL, the 8 planes of the reference return tuple
+ * (vegsh, sh, vbshvegsh, wallsh, wallsun, wallshve, facesh, facesun) at
+ * debug8[(d * 8 + k) * npix]. */
+int sw100_sun_march_workspace_bytes(int rows, int cols, int64_t* bytes);
+int sw100_sun_march(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
+                    float* gsrc, float* debug8, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* All steps of one site's time loop: sun march of the daytime rows, then
+ * one launch for ground view factors, thermal lag (state carried in
+ * registers), K/L fluxes, Tmrt and UTCI.  `state` holds the 6 thermal planes
+ * (Tgmap1, E, S, W, N, TgOut1), read at the start and written at the end.
+ * `outputs` receives, for each bit set in `out_mask` (in bit order), an
+ * n_t * npix block. */
+int sw100_time_loop_workspace_bytes(int rows, int cols, int n_day, int64_t* bytes);
+int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
+                    float* state, uint32_t out_mask, float* outputs, void* workspace,
+                    int64_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------- UTCI -- */
+/* utci_calculator over n float32 elements: saturation vapour pressure from
+ * Ta, then the 210-term regression in float64; -999 where any input is
+ * <= -999 (calculate_utci.py:259-330). */
+int sw100_utci(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n,
+               float* out, void* stream);
+
+/* ------------------------------------------------------------ support -- */
+int sw100_abi_version(void);
+const char* sw100_last_error(void);
+/* number of kernels this library has launched since it was loaded */
+int64_t sw100_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOLWEIG_B200_H */

@@ -1,0 +1,261 @@
+// C ABI of the library (see include/solweig_b200.h for the contract).
+//
+// Mirrors the reference's native ABI conventions (native/cuda/src/sw_api.cu:
+// extern "C", status return, last-error string per thread) but never
+// allocates: every scratch buffer comes from the caller's workspace, so the
+// entry points can be captured in CUDA graphs and driven from any allocator.
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "sw_common.cuh"
+#include "sw_internal.cuh"
+
+namespace sw100 {
+__global__ void pack4_kernel(const float* a, const float* b, const float* c, const float* d, size_t n, float4* out);
+__global__ void svf_sweep_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
+                                 const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
+                                 uint32_t* bits);
+__global__ void svf_bush_flags_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
+                                      const sw100_step* steps, uint32_t* flags);
+__global__ void sun_march_kernel(const float4* src4, SitePlanes site, int rows, int cols,
+                                 const sw100_sun_step* sun_steps, const sw100_time_step* tsteps,
+                                 const sw100_step* table, float vmax, float4* gsrc, float* debug8);
+__global__ void time_loop_kernel(SitePlanes site, int rows, int cols, const sw100_time_step* tsteps, int n_t,
+                                 const sw100_patch_step* patch_steps, int n_patches,
+                                 const sw100_gvf_azimuth* gvf_az, const float4* gsrc, float* state,
+                                 uint32_t out_mask, float* outputs);
+__global__ void utci_kernel(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n,
+                            float* out);
+}  // namespace sw100
+
+using namespace sw100;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<int64_t> g_launches{0};
+
+constexpr int64_t kMaxPixels = int64_t(1) << 31;  // int32 pixel offsets inside kernels
+constexpr int64_t kAlign = 256;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail((int)e, "%s: %s", what, cudaGetErrorString(e));
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return 0;
+}
+
+int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+int check_grid(int rows, int cols) {
+  if (rows <= 0 || cols <= 0) return fail(SW100_E_SIZE, "grid %d x %d must be positive", rows, cols);
+  if ((int64_t)rows * cols >= kMaxPixels) return fail(SW100_E_SIZE, "grid %d x %d too large", rows, cols);
+  return 0;
+}
+
+int check_ptr(const void* p, const char* name) {
+  if (!p) return fail(SW100_E_ARG, "%s must not be NULL", name);
+  return 0;
+}
+
+int check_workspace(const void* ws, int64_t have, int64_t need) {
+  if (need > 0 && (!ws || have < need))
+    return fail(SW100_E_WORKSPACE, "workspace of %lld bytes required, %lld given", (long long)need,
+                (long long)(ws ? have : 0));
+  if (ws && (reinterpret_cast<uintptr_t>(ws) % 16) != 0) return fail(SW100_E_ARG, "workspace must be 16-byte aligned");
+  return 0;
+}
+
+int launch_pack(const sw100_site_planes& s, int rows, int cols, float4* out, cudaStream_t st) {
+  const size_t n = (size_t)rows * cols;
+  const int threads = 256;
+  const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 16);
+  pack4_kernel<<<blocks, threads, 0, st>>>(s.dsm, s.vegdsm, s.vegdsm2, s.bush_any ? s.bush : nullptr, n, out);
+  return check_launch("pack4_kernel");
+}
+
+int validate_site_march(const sw100_site_planes* s) {
+  int rc;
+  if ((rc = check_ptr(s, "site"))) return rc;
+  if ((rc = check_ptr(s->dsm, "site->dsm"))) return rc;
+  if ((rc = check_ptr(s->vegdsm, "site->vegdsm"))) return rc;
+  if ((rc = check_ptr(s->vegdsm2, "site->vegdsm2"))) return rc;
+  if (s->bush_any && !s->bush) return fail(SW100_E_ARG, "site->bush is NULL but bush_any is set");
+  return 0;
+}
+
+int validate_site_loop(const sw100_site_planes* s) {
+  int rc;
+  if ((rc = validate_site_march(s))) return rc;
+  const void* ptrs[] = {s->svfbuveg, s->hsvf, s->tan_alfa, s->buildings, s->walls, s->aspect_rad, s->tgk,
+                        s->tstart, s->alb, s->emis, s->class_idx, s->windcoeff, s->bits};
+  const char* names[] = {"svfbuveg", "hsvf", "tan_alfa", "buildings", "walls", "aspect_rad", "tgk",
+                         "tstart", "alb", "emis", "class_idx", "windcoeff", "bits"};
+  for (int i = 0; i < 13; ++i)
+    if (!ptrs[i]) return fail(SW100_E_ARG, "site->%s must not be NULL", names[i]);
+  return 0;
+}
+
+int validate_series(const sw100_series* s) {
+  int rc;
+  if ((rc = check_ptr(s, "series"))) return rc;
+  if (s->n_t <= 0) return fail(SW100_E_ARG, "series->n_t must be positive");
+  if (s->n_day < 0 || s->n_day > s->n_t) return fail(SW100_E_ARG, "series->n_day out of range");
+  if (s->n_day > 65535) return fail(SW100_E_SIZE, "too many daytime steps");
+  if (s->n_patches <= 0 || s->n_patches > 153) return fail(SW100_E_SIZE, "series->n_patches must be 1..153");
+  if ((rc = check_ptr(s->steps, "series->steps"))) return rc;
+  if ((rc = check_ptr(s->patch, "series->patch"))) return rc;
+  if ((rc = check_ptr(s->gvf, "series->gvf"))) return rc;
+  if (s->n_day > 0) {
+    if ((rc = check_ptr(s->sun, "series->sun"))) return rc;
+    if ((rc = check_ptr(s->sun_table, "series->sun_table"))) return rc;
+  }
+  return 0;
+}
+
+int launch_sun_march(const sw100_site_planes& site, int rows, int cols, const sw100_series& ser, const float4* src4,
+                     float4* gsrc, float* debug8, cudaStream_t st) {
+  if (ser.n_day == 0) return 0;
+  dim3 block(32, 8);
+  dim3 grid((cols + 31) / 32, (rows + 7) / 8, ser.n_day);
+  sun_march_kernel<<<grid, block, 0, st>>>(src4, make_site(site), rows, cols, ser.sun, ser.steps, ser.sun_table,
+                                           site.vmax, gsrc, debug8);
+  return check_launch("sun_march_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw100_abi_version(void) { return SW100_ABI_VERSION; }
+
+const char* sw100_last_error(void) { return g_last_error.c_str(); }
+
+int64_t sw100_launch_count(void) { return g_launches.load(); }
+
+int sw100_svf_workspace_bytes(int rows, int cols, int n_steps, int64_t* bytes) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(bytes, "bytes"))) return rc;
+  if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
+  *bytes = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4);
+  return 0;
+}
+
+int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                    const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits, void* workspace,
+                    int64_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_march(site))) return rc;
+  if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(out_planes, "out_planes")) ||
+      (rc = check_ptr(out_bits, "out_bits")))
+    return rc;
+  int64_t need = 0;
+  if ((rc = sw100_svf_workspace_bytes(rows, cols, n_steps, &need))) return rc;
+  if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* src4 = static_cast<float4*>(workspace);
+  uint32_t* flags = reinterpret_cast<uint32_t*>(static_cast<char*>(workspace) + align_up((int64_t)rows * cols * 16));
+  if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
+  dim3 block(32, 4);
+  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  if (site->bush_any) {
+    cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)n_steps * 4, st);
+    if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+    svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags);
+    if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
+  }
+  svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
+                                           site->vmax, out_planes, out_bits);
+  return check_launch("svf_sweep_kernel");
+}
+
+int sw100_sun_march_workspace_bytes(int rows, int cols, int64_t* bytes) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(bytes, "bytes"))) return rc;
+  *bytes = align_up((int64_t)rows * cols * 16);
+  return 0;
+}
+
+int sw100_sun_march(const sw100_site_planes* site, int rows, int cols, const sw100_series* series, float* gsrc,
+                    float* debug8, void* workspace, int64_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_loop(site))) return rc;
+  if ((rc = validate_series(series))) return rc;
+  if ((rc = check_ptr(gsrc, "gsrc"))) return rc;
+  int64_t need = 0;
+  if ((rc = sw100_sun_march_workspace_bytes(rows, cols, &need))) return rc;
+  if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* src4 = static_cast<float4*>(workspace);
+  if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
+  return launch_sun_march(*site, rows, cols, *series, src4, reinterpret_cast<float4*>(gsrc), debug8, st);
+}
+
+int sw100_time_loop_workspace_bytes(int rows, int cols, int n_day, int64_t* bytes) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(bytes, "bytes"))) return rc;
+  if (n_day < 0) return fail(SW100_E_ARG, "n_day must be >= 0");
+  const int64_t plane4 = align_up((int64_t)rows * cols * 16);
+  *bytes = plane4 * (1 + (int64_t)n_day);
+  return 0;
+}
+
+int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw100_series* series, float* state,
+                    uint32_t out_mask, float* outputs, void* workspace, int64_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_loop(site))) return rc;
+  if ((rc = validate_series(series))) return rc;
+  if ((rc = check_ptr(state, "state"))) return rc;
+  if (out_mask & ~0x7Fu) return fail(SW100_E_ARG, "unknown output bits 0x%x", out_mask);
+  if (out_mask && !outputs) return fail(SW100_E_ARG, "outputs must not be NULL");
+  int64_t need = 0;
+  if ((rc = sw100_time_loop_workspace_bytes(rows, cols, series->n_day, &need))) return rc;
+  if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t plane4 = align_up((int64_t)rows * cols * 16);
+  float4* src4 = static_cast<float4*>(workspace);
+  float4* gsrc = reinterpret_cast<float4*>(static_cast<char*>(workspace) + plane4);
+  if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
+  if ((rc = launch_sun_march(*site, rows, cols, *series, src4, gsrc, nullptr, st))) return rc;
+  dim3 block(32, 4);
+  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  time_loop_kernel<<<grid, block, 0, st>>>(make_site(*site), rows, cols, series->steps, series->n_t, series->patch,
+                                           series->n_patches, series->gvf, gsrc, state, out_mask, outputs);
+  return check_launch("time_loop_kernel");
+}
+
+int sw100_utci(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n, float* out,
+               void* stream) {
+  int rc;
+  if (n < 0) return fail(SW100_E_ARG, "n must be >= 0");
+  if (n == 0) return 0;
+  if ((rc = check_ptr(ta, "ta")) || (rc = check_ptr(rh, "rh")) || (rc = check_ptr(tmrt, "tmrt")) ||
+      (rc = check_ptr(va, "va")) || (rc = check_ptr(out, "out")))
+    return rc;
+  const int threads = 256;
+  const int blocks = (int)std::min<int64_t>((n + threads - 1) / threads, 148 * 32);
+  utci_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(ta, rh, tmrt, va, n, out);
+  return check_launch("utci_kernel");
+}
+
+}  // extern "C"

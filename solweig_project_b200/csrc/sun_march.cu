@@ -1,0 +1,125 @@
+// Wall-height sun march for every daytime step of a site in one launch.
+//
+// Reference: solweig_gpu/solweig.py:1079-1224 (shadowingfunction_wallheight_23)
+// and the per-step shadow / ground-view-factor inputs of solweig.py:2094-2130
+// and :75-128 (sunonsurface_2018a's Lup and sunwall planes).
+//
+// grid.z indexes the daytime step; one thread per pixel marches the step's
+// table (index 0 = the self comparison, dzprev carried) and then writes the
+// packed ground-view-factor source record {shadow, Lup, albedo, flags} that
+// the time-loop kernel gathers 396 times per pixel and step.
+#include "sw_common.cuh"
+#include "sw_internal.cuh"
+
+namespace sw100 {
+
+struct MarchOut {
+  float vegsh, sh, vbsh, wallsh, wallsun, wallshve, facesh, facesun;
+};
+
+__device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, int rows, int cols, int r, int c,
+                                              float a, float vegdem_p, float bush_p, float walls_p,
+                                              float aspect_p, const sw100_step* __restrict__ steps, int n,
+                                              float vmax, const sw100_sun_step& S) {
+  const float bushplant = bush_p > 1.f ? 1.f : 0.f;
+  float sh = 0.f, vbsh = 0.f;
+  float vegsh = bushplant;
+  float f = a;
+  float shvoveg = vegdem_p;
+  float dzprev = 0.f;
+  const float wallbol = walls_p > 0.f ? 1.f : 0.f;
+  for (int k = 0; k < n; ++k) {
+    const sw100_step st = load_step(&steps[k]);
+    const int sr = r + st.dx, sc = c + st.dy;
+    const float dz = st.dz;
+    float temp = 0.f, tv = 0.f, tv2 = 0.f, tlf = 0.f, tlg = 0.f;
+    if (in_grid(sr, sc, rows, cols)) {
+      const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
+      temp = __fsub_rn(v.x, dz);
+      tv = __fsub_rn(v.y, dz);
+      tv2 = __fsub_rn(v.z, dz);
+      tlf = __fsub_rn(v.y, dzprev);
+      tlg = __fsub_rn(v.z, dzprev);
+    }
+    f = tmax(f, temp);
+    shvoveg = tmax(shvoveg, tv);
+    sh = (f > a) ? 1.f : 0.f;
+    float vegsh2 = (tv > a ? 1.f : 0.f) + (tv2 > a ? 1.f : 0.f) + (tlf > a ? 1.f : 0.f) + (tlg > a ? 1.f : 0.f);
+    dzprev = dz;
+    if (vegsh2 == 4.f) vegsh2 = 0.f;
+    if (vegsh2 > 0.f) vegsh2 = 1.f;
+    vegsh = tmax(vegsh, vegsh2);
+    if (vegsh * sh > 0.f) vegsh = 0.f;
+    vbsh = vbsh + vegsh;
+    // Nothing above this pixel can be reached any more: every later source
+    // height minus a larger drop stays at or below the pixel, its running
+    // building maximum and its running vegetation maximum (out-of-grid reads
+    // are 0, covered by a >= 0 and shvoveg >= 0).
+    const float top = __fsub_rn(vmax, dz);
+    if (a >= 0.f && shvoveg >= 0.f && top <= a && top <= shvoveg) break;
+  }
+  MarchOut o;
+  float facesh;
+  if (S.facesh_mode == 0) {
+    facesh = ((aspect_p < S.facesh_lo || aspect_p >= S.facesh_hi) ? 1.f : 0.f) - wallbol + 1.f;
+  } else {
+    facesh = ((aspect_p > S.facesh_lo || aspect_p <= S.facesh_hi) ? 1.f : 0.f) * -1.f + 1.f;
+  }
+  sh = 1.f - sh;
+  if (vbsh > 0.f) vbsh = 1.f;
+  vbsh = vbsh - vegsh;
+  if (vegsh > 0.f) vegsh = 1.f;
+  shvoveg = (shvoveg - a) * vegsh;
+  vegsh = 1.f - vegsh;
+  vbsh = 1.f - vbsh;
+  const float shvo = f - a;
+  const float facesun = ((facesh + wallbol == 1.f) && walls_p > 0.f) ? 1.f : 0.f;
+  float wallsun = walls_p - shvo;
+  if (wallsun < 0.f) wallsun = 0.f;
+  if (facesh == 1.f) wallsun = 0.f;
+  const float wallsh = walls_p - wallsun;
+  float wallshve = shvoveg * wallbol;
+  wallshve = wallshve - wallsh;
+  if (wallshve < 0.f) wallshve = 0.f;
+  wallsun = wallsun - wallshve;
+  if (wallsun < 0.f) wallsun = 0.f;
+  if (wallshve > walls_p) wallshve = walls_p;
+  o.vegsh = vegsh; o.sh = sh; o.vbsh = vbsh; o.wallsh = wallsh; o.wallsun = wallsun;
+  o.wallshve = wallshve; o.facesh = facesh; o.facesun = facesun;
+  return o;
+}
+
+__global__ void __launch_bounds__(256) sun_march_kernel(const float4* __restrict__ src4, SitePlanes site, int rows,
+                                                         int cols, const sw100_sun_step* __restrict__ sun_steps,
+                                                         const sw100_time_step* __restrict__ tsteps,
+                                                         const sw100_step* __restrict__ table, float vmax,
+                                                         float4* __restrict__ gsrc, float* __restrict__ debug8) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  const int d = blockIdx.z;  // daytime step row
+  if (r >= rows || c >= cols) return;
+  const size_t npix = (size_t)rows * cols;
+  const size_t p = (size_t)r * cols + c;
+  const sw100_sun_step S = sun_steps[d];
+  const float4 self = src4[p];
+  const float walls_p = site.walls[p];
+  const MarchOut o = march_sun(src4, rows, cols, r, c, self.x, self.y, self.w, walls_p, site.aspect_rad[p],
+                               table + S.step_offset, S.step_count, vmax, S);
+  const float shadow = o.sh - (1.f - o.vegsh) * S.psi_term;
+  // sunonsurface_2018a inputs at this pixel (solweig.py:118-128, gvf_2018a :342)
+  const sw100_time_step& P = tsteps[S.t];
+  const float bld = site.buildings[p];
+  const float tg = ground_temperature(site, P, p);
+  const float sbc_emis = P.sbc * site.emis[p];
+  const float lup = sbc_emis * pow4f(tg * shadow + P.ta32 + 273.15f) - sbc_emis * P.ta4;
+  const float sunwall = ((o.wallsun / walls_p) * bld == 1.f) ? 1.f : 0.f;
+  const uint32_t flags = (bld != 0.f ? 1u : 0u) | (sunwall != 0.f ? 2u : 0u) | (bld == 1.f ? 4u : 0u);
+  gsrc[d * npix + p] = make_float4(shadow, lup, site.alb[p], __uint_as_float(flags));
+  if (debug8) {
+    float* o8 = debug8 + (size_t)d * 8 * npix + p;
+    o8[0 * npix] = o.vegsh; o8[1 * npix] = o.sh; o8[2 * npix] = o.vbsh; o8[3 * npix] = o.wallsh;
+    o8[4 * npix] = o.wallsun; o8[5 * npix] = o.wallshve; o8[6 * npix] = o.facesh; o8[7 * npix] = o.facesun;
+  }
+}
+
+}  // namespace sw100

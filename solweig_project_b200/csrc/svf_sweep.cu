@@ -1,0 +1,217 @@
+// SVF patch sweep: all 153 sky patches of one site in one launch.
+//
+// Reference: solweig_gpu/shadow.py:166-322 (shadow(), one patch march) and
+// shadow.py:409-625 (svf_calculator: patch loop, annulus weights, tails).
+//
+// One thread owns one pixel and marches every patch for it; the per-patch
+// step tables (dx, dy, dz), built on the host with the reference's float32
+// trigonometry, are read as warp-uniform broadcasts.  Each step gathers one
+// float4 {dsm, vegdsm, vegdsm2, bush} at the shifted source: all lanes of a
+// warp shift by the same (dx, dy), so the gather is a contiguous 512-byte
+// row segment served from L1/L2 (consecutive steps shift by at most one
+// pixel).  The 15 SVF accumulators are updated in the reference's order
+// (patch-major, annulus-minor), so the sums are bit-identical; the three
+// patch masks are packed into 5-word bit cubes per pixel (60 B/px instead of
+// the reference's 1836 B/px of float cubes).
+#include "sw_common.cuh"
+
+namespace sw100 {
+
+struct SvfAcc {
+  float svf, svfE, svfS, svfW, svfN;
+  float veg, vegE, vegS, vegW, vegN;
+  float aveg, avegE, avegS, avegW, avegN;
+};
+
+// One patch march for one pixel (shadow.py:228-316).  Returns final sh
+// (1 = sky visible), vegsh and vbshvegsh as floats.
+__device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int rows, int cols, int r,
+                                            int c, float a, float veg2_p, float bush_p,
+                                            const sw100_step* __restrict__ steps, int n,
+                                            const uint32_t* __restrict__ bflags, bool bush_any,
+                                            float vmax, float& sh_out, float& veg_out, float& vb_out) {
+  const bool bushplant = bush_p > 1.f;
+  float f = a;
+  float sh = 0.f;
+  float vegsh = bushplant ? 1.f : 0.f;  // zeros + bushplant
+  int vbsh = 0;                         // integer count of vegsh over steps >= 2
+  float g = 0.f;
+  const bool may_exit = !(bush_any && bushplant);
+  for (int k = 0; k < n; ++k) {
+    const sw100_step st = load_step(&steps[k]);
+    const int sr = r + st.dx, sc = c + st.dy;
+    const float dz = st.dz;
+    float temp = 0.f, tv = 0.f, tv2 = 0.f, tb = 0.f;
+    if (in_grid(sr, sc, rows, cols)) {
+      const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
+      temp = __fsub_rn(v.x, dz);
+      tv = __fsub_rn(v.y, dz);
+      tv2 = __fsub_rn(v.z, dz);
+      tb = __fsub_rn(v.w, dz);
+    }
+    f = tmax(f, temp);
+    if (f > a) sh = 1.f;
+    else if (f <= a) sh = 0.f;
+    const bool fab = tv > a;
+    const bool gab = tv2 > a;
+    const float vegsh2 = (fab ? 1.f : 0.f) - (gab ? 1.f : 0.f);
+    vegsh = tmax(vegsh, vegsh2);
+    if (vegsh * sh > 0.f) vegsh = 0.f;
+    vbsh += (vegsh > 0.f) ? 1 : 0;
+    if (k == 0) {
+      float first = __fsub_rn(tv, temp);
+      if (first <= 0.f) first = 1000.f;
+      if (first < dz) vegsh = 1.f;
+      vegsh = vegsh * ((veg2_p > a) ? 1.f : 0.f);
+      vbsh = 0;
+    }
+    if (bush_any && bflags[k]) {
+      g = tmax(g, tb);
+      g = g * (bushplant ? 1.f : 0.f);
+    }
+    if (may_exit && k >= 1) {
+      // nothing later can change sh / vegsh / vbsh>0: building shadow is
+      // final, or no source can rise above this pixel any more
+      // (out-of-grid reads are 0, so the height test needs a >= 0)
+      const bool done = (sh == 1.f) || (a >= 0.f && __fsub_rn(vmax, dz) <= a);
+      if (done) {
+        if (vegsh > 0.f && vbsh == 0 && k + 1 < n) vbsh = 1;
+        break;
+      }
+    }
+  }
+  sh = 1.f - sh;
+  float vb = (vbsh > 0) ? 1.f : 0.f;
+  vb = vb - vegsh;
+  if (bush_any) {
+    g = g - bush_p;
+    if (g > 0.f) g = 1.f;
+    if (g < 0.f) g = 0.f;
+    vegsh = vegsh - (bushplant ? 1.f : 0.f) + g;
+    if (vegsh < 0.f) vegsh = 0.f;
+  }
+  if (vegsh > 0.f) vegsh = 1.f;
+  vegsh = 1.f - vegsh;
+  vb = 1.f - vb;
+  sh_out = sh;
+  veg_out = vegsh;
+  vb_out = vb;
+}
+
+__global__ void __launch_bounds__(128) svf_sweep_kernel(
+    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
+    const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
+    float* __restrict__ out, uint32_t* __restrict__ bits) {
+  __shared__ sw100_svf_plan plan;
+  {
+    const int* s = reinterpret_cast<const int*>(plan_g);
+    int* d = reinterpret_cast<int*>(&plan);
+    const int nw = sizeof(sw100_svf_plan) / 4;
+    for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < nw; i += blockDim.x * blockDim.y) d[i] = s[i];
+  }
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  if (r >= rows || c >= cols) return;
+  const size_t npix = (size_t)rows * cols;
+  const size_t p = (size_t)r * cols + c;
+  const float4 self = src4[p];
+  const float a = self.x, veg2_p = self.z, bush_p = self.w;
+  const bool bush_any = plan.bush_any != 0;
+
+  SvfAcc A = {};
+  uint32_t wsh[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+  uint32_t wveg[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+  uint32_t wvb[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+
+  for (int q = 0; q < plan.n_patches; ++q) {
+    const int off = plan.step_offset[q];
+    float sh, veg, vb;
+    march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, plan.step_count[q],
+                bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);
+    const uint32_t bit = 1u << (q & 31);
+    if (sh != 0.f) wsh[q >> 5] |= bit;
+    if (veg != 0.f) wveg[q >> 5] |= bit;
+    // marches of at most one step leave vbshvegsh in {1, 2}: their bit keeps
+    // "== 1"; every other patch keeps "!= 0" (values {0, 1})
+    if (plan.step_count[q] <= 1 ? (vb == 1.f) : (vb != 0.f)) wvb[q >> 5] |= bit;
+    const int ring = plan.ring[q];
+    const int fl = plan.dir_flags[q];
+    const int na = plan.ring_annuli[ring];
+    for (int k = 0; k < na; ++k) {
+      const float wi = plan.w_iso[ring][k];
+      const float wa = plan.w_aniso[ring][k];
+      A.svf = A.svf + wi * sh;
+      const float wsh_ = wa * sh;
+      if (fl & 1) A.svfE = A.svfE + wsh_;
+      if (fl & 2) A.svfS = A.svfS + wsh_;
+      if (fl & 4) A.svfW = A.svfW + wsh_;
+      if (fl & 8) A.svfN = A.svfN + wsh_;
+      A.veg = A.veg + wi * veg;
+      A.aveg = A.aveg + wi * vb;
+      const float wv = wa * veg, wb = wa * vb;
+      if (fl & 1) { A.vegE = A.vegE + wv; A.avegE = A.avegE + wb; }
+      if (fl & 2) { A.vegS = A.vegS + wv; A.avegS = A.avegS + wb; }
+      if (fl & 4) { A.vegW = A.vegW + wv; A.avegW = A.avegW + wb; }
+      if (fl & 8) { A.vegN = A.vegN + wv; A.avegN = A.avegN + wb; }
+    }
+  }
+  // tails and clamps (shadow.py:587-613)
+  const float tail = plan.tail;
+  A.svfS = A.svfS + tail;
+  A.svfW = A.svfW + tail;
+  auto clamp1 = [](float& x) { if (x > 1.f) x = 1.f; };
+  clamp1(A.svf); clamp1(A.svfE); clamp1(A.svfS); clamp1(A.svfW); clamp1(A.svfN);
+  const float last = (veg2_p == 0.f) ? tail : 0.f;
+  A.vegS = A.vegS + last;
+  A.vegW = A.vegW + last;
+  A.avegS = A.avegS + last;
+  A.avegW = A.avegW + last;
+  clamp1(A.veg); clamp1(A.vegE); clamp1(A.vegS); clamp1(A.vegW); clamp1(A.vegN);
+  clamp1(A.aveg); clamp1(A.avegE); clamp1(A.avegS); clamp1(A.avegW); clamp1(A.avegN);
+  const float total = A.svf - (1.f - A.veg) * (1.f - plan.trans);
+  // reference tuple order (shadow.py:625) without the cubes, then SVFtotal
+  const float vals[SW100_SVF_PLANES] = {A.svf,  A.aveg,  A.svfE, A.avegE, A.vegE, A.svfN, A.avegN, A.vegN,
+                                        A.svfS, A.avegS, A.vegS, A.veg,   A.svfW, A.avegW, A.vegW, total};
+#pragma unroll
+  for (int k = 0; k < SW100_SVF_PLANES; ++k) out[k * npix + p] = vals[k];
+#pragma unroll
+  for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+    bits[(0 * SW100_CUBE_WORDS + w) * npix + p] = wsh[w];
+    bits[(1 * SW100_CUBE_WORDS + w) * npix + p] = wveg[w];
+    bits[(2 * SW100_CUBE_WORDS + w) * npix + p] = wvb[w];
+  }
+}
+
+// Whole-grid bush test of shadow.py:295 (`torch.max(fabovea * bush) > 0`):
+// flag the steps at which any pixel with bush > 0 sees vegetation above it.
+__global__ void svf_bush_flags_kernel(const float4* __restrict__ src4, int rows, int cols,
+                                      const sw100_svf_plan* __restrict__ plan, const sw100_step* __restrict__ steps,
+                                      uint32_t* __restrict__ flags) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  if (r >= rows || c >= cols) return;
+  const float4 self = src4[(size_t)r * cols + c];
+  if (!(self.w > 0.f)) return;
+  const float a = self.x;
+  const int np = plan->n_patches;
+  for (int q = 0; q < np; ++q) {
+    const int off = plan->step_offset[q], n = plan->step_count[q];
+    for (int k = 0; k < n; ++k) {
+      const sw100_step st = steps[off + k];
+      const int sr = r + st.dx, sc = c + st.dy;
+      float tv = 0.f;
+      if (in_grid(sr, sc, rows, cols)) tv = __fsub_rn(src4[(size_t)sr * cols + sc].y, st.dz);
+      if (tv > a && flags[off + k] == 0u) atomicExch(&flags[off + k], 1u);
+    }
+  }
+}
+
+// Packs {dsm, vegdsm, vegdsm2, bush} into one float4 plane.
+__global__ void pack4_kernel(const float* __restrict__ a, const float* __restrict__ b, const float* __restrict__ c,
+                             const float* __restrict__ d, size_t n, float4* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = make_float4(a[i], b[i], c[i], d ? d[i] : 0.f);
+}
+
+}  // namespace sw100

@@ -1,0 +1,370 @@
+// The whole time loop of one site in one launch.
+//
+// Reference: solweig_gpu/utci_process.py:917-1067 (run_utci_window's loop)
+// around solweig_gpu/solweig.py:1950-2311 (Solweig_2022a_calc) with
+// cyl = 1, anisotropic_sky = 1, usevegdem = 1, onlyglobal = 1:
+//   * ground view factors, 18 azimuths x `second` steps
+//     (gvf_2018a / sunonsurface_2018a, solweig.py:75-402), including the
+//     reference's stale-border temporaries (a ray that leaves the grid keeps
+//     the last in-grid sample);
+//   * thermal lag TsWaveDelay_2015a (solweig.py:451-488) with the six state
+//     planes held in registers across the steps;
+//   * cylindric_wedge, Kdown, Kup_veg_2015a, Kside_veg_v2022a
+//     (solweig.py:404-449, 490-522, 564-832);
+//   * Lcyl_v2022a / define_patch_characteristics (solweig.py:1439-1760);
+//   * Tmrt (solweig.py:2291-2299) and UTCI (calculate_utci.py:259-330),
+//     NaN outside buildings == 1 (utci_process.py:1047-1049).
+//
+// One thread owns one pixel for all steps.  Per-step scalars and the per-patch
+// constant table are staged in shared memory once per step for the block.
+// The 153-patch sums read the packed bit cubes of the SVF sweep (60 B per
+// pixel) instead of three float cubes; their per-patch increments are host
+// constants evaluated in the reference's association, so each sum is the
+// same sequence of float32 additions (float64 where the reference promotes).
+#include <cmath>
+
+#include "sw_common.cuh"
+#include "sw_internal.cuh"
+
+namespace sw100 {
+
+constexpr int kMaxPatchSmem = 153;
+
+struct GvfAzSmem {
+  int8_t dx[SW100_MAX_GVF_STEPS];
+  int8_t dy[SW100_MAX_GVF_STEPS];
+  int32_t facesh_mode;
+  float facesh_lo;
+  float facesh_hi;
+  int32_t dir_flags;
+};
+
+__device__ __forceinline__ float facesh_value(int mode, float lo, float hi, float aspect, float wallbol) {
+  if (mode == 0) return ((aspect < lo || aspect >= hi) ? 1.f : 0.f) - wallbol + 1.f;
+  return ((aspect > lo || aspect <= hi) ? 1.f : 0.f) * -1.f + 1.f;
+}
+
+// float32 transcendental rounded once from double
+__device__ __forceinline__ float atan_r(float x) { return (float)atan((double)x); }
+__device__ __forceinline__ float sin_r(float x) { return (float)sin((double)x); }
+__device__ __forceinline__ float cos_r(float x) { return (float)cos((double)x); }
+
+// cylindric_wedge (solweig.py:404-449) + NaN -> 0.5 (solweig.py:2168)
+__device__ __forceinline__ float cylindric_wedge(float ta, float tb, float qa) {
+  const float tt = ta * tb;
+  const float xa = 1.f - 2.f / tt;
+  const float ha = 2.f / tt;
+  const float ba = 1.f / ta;
+  const float hkil = (2.f * ba) * ha;
+  float ukil = 0.f;
+  if (xa < 0.f) {
+    const float za = sqrtf(ba * ba - (qa * qa) / 4.f);
+    const float phi = atan_r(za / qa);
+    const float cphi = cos_r(phi);
+    const float A = (sin_r(phi) - phi * cphi) / (1.f - cphi);
+    ukil = ((2.f * ba) * xa) * A;
+  }
+  const float ssurf = hkil + ukil;
+  const float twopi_ba = 6.28318548202514648f * ba;  // float32(2 * pi) * ba
+  float fsh = (twopi_ba - ssurf) / twopi_ba;
+  if (fsh != fsh) fsh = 0.5f;
+  return fsh;
+}
+
+// UTCI polynomial in (D_Tmrt, va) for this step: sum_i D^i sum_j c[i][j] va^j
+__device__ __forceinline__ float utci_poly(const double* c, float d, float va) {
+  const double D = d, V = va;
+  double acc = 0.0;
+#pragma unroll
+  for (int i = 6; i >= 0; --i) {
+    double q = 0.0;
+#pragma unroll
+    for (int j = 6 - i; j >= 0; --j) q = q * V + c[i * 7 + j];
+    acc = acc * D + q;
+  }
+  return (float)acc;
+}
+
+struct GvfSums {
+  float Lup, alb, albnosh;
+  float LupE, albE, albnoshE, LupS, albS, albnoshS, LupW, albW, albnoshW, LupN, albN, albnoshN;
+};
+
+__global__ void __launch_bounds__(128) time_loop_kernel(
+    SitePlanes site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
+    const sw100_patch_step* __restrict__ patch_steps, int n_patches,
+    const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, float* __restrict__ state,
+    uint32_t out_mask, float* __restrict__ outputs) {
+  // PP is filled with 16-byte vector stores: the array must be 16-byte
+  // aligned (the struct itself only requires 8)
+  __shared__ __align__(16) sw100_time_step P;
+  __shared__ __align__(16) sw100_patch_step PP[kMaxPatchSmem];
+  __shared__ GvfAzSmem AZ[SW100_N_GVF_AZ];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nthr = blockDim.x * blockDim.y;
+  for (int i = tid; i < SW100_N_GVF_AZ * SW100_MAX_GVF_STEPS; i += nthr) {
+    const int a = i / SW100_MAX_GVF_STEPS, n = i % SW100_MAX_GVF_STEPS;
+    AZ[a].dx[n] = gvf_az[a].dx[n];
+    AZ[a].dy[n] = gvf_az[a].dy[n];
+  }
+  if (tid < SW100_N_GVF_AZ) {
+    AZ[tid].facesh_mode = gvf_az[tid].facesh_mode;
+    AZ[tid].facesh_lo = gvf_az[tid].facesh_lo;
+    AZ[tid].facesh_hi = gvf_az[tid].facesh_hi;
+    AZ[tid].dir_flags = gvf_az[tid].dir_flags;
+  }
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  const bool live = (r < rows) && (c < cols);
+  const size_t npix = (size_t)rows * cols;
+  const size_t p = live ? (size_t)r * cols + c : 0;
+
+  // per-pixel statics
+  float bld = 0.f, walls = 0.f, aspect = 0.f, emis = 0.f, alb = 0.f, svfbuveg = 0.f, hsvf = 0.f, tan_alfa = 0.f,
+        wind = 0.f;
+  uint32_t wsh[SW100_CUBE_WORDS] = {}, wveg[SW100_CUBE_WORDS] = {}, wvb[SW100_CUBE_WORDS] = {};
+  float st[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // Tgmap1, E, S, W, N, TgOut1
+  if (live) {
+    bld = site.buildings[p];
+    walls = site.walls[p];
+    aspect = site.aspect_rad[p];
+    emis = site.emis[p];
+    alb = site.alb[p];
+    svfbuveg = site.svfbuveg[p];
+    hsvf = site.hsvf[p];
+    tan_alfa = site.tan_alfa[p];
+    wind = site.windcoeff[p];
+#pragma unroll
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+      wsh[w] = site.bits[(0 * SW100_CUBE_WORDS + w) * npix + p];
+      wveg[w] = site.bits[(1 * SW100_CUBE_WORDS + w) * npix + p];
+      wvb[w] = site.bits[(2 * SW100_CUBE_WORDS + w) * npix + p];
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) st[k] = state[k * npix + p];
+  }
+  const float wallbol = walls > 0.f ? 1.f : 0.f;
+  const float nb = bld * -1.f + 1.f;
+
+  for (int t = 0; t < n_t; ++t) {
+    __syncthreads();
+    {
+      const int* s = reinterpret_cast<const int*>(&tsteps[t]);
+      int* d = reinterpret_cast<int*>(&P);
+      for (int i = tid; i < (int)(sizeof(sw100_time_step) / 4); i += nthr) d[i] = s[i];
+      const int4* ps = reinterpret_cast<const int4*>(patch_steps + (size_t)t * n_patches);
+      int4* pd = reinterpret_cast<int4*>(PP);
+      const int n16 = n_patches * (int)(sizeof(sw100_patch_step) / 16);
+      for (int i = tid; i < n16; i += nthr) pd[i] = ps[i];
+    }
+    __syncthreads();
+    if (!live) continue;
+
+    float shadow = 0.f, Lup, LupE, LupS, LupW, LupN;
+    float Kdown = 0.f, Kup = 0.f, KupE = 0.f, KupS = 0.f, KupW = 0.f, KupN = 0.f;
+    float Kside = 0.f;
+    if (P.is_day) {
+      const float4* G = gsrc + (size_t)P.day_row * npix;
+      const float4 own = G[p];
+      shadow = own.x;
+      const float lup_own = own.y;
+      const float tg = ground_temperature(site, P, p);
+      // ---------------- ground view factors (18 azimuths)
+      GvfSums S = {};
+      const int second_i = (int)P.second;
+      const float first = P.first, second = P.second;
+      const float f1 = first + 1.f, s1 = second + 1.f;
+      for (int az = 0; az < SW100_N_GVF_AZ; ++az) {
+        float f = bld;
+        float tbu = 0.f, tsh = 0.f, tlup = 0.f, talb = 0.f, talbsh = 0.f, twall = 0.f;
+        float wsh_ = 0.f, wLupsh = 0.f, walbsh = 0.f, walbnosh = 0.f;
+        float wLwall = 0.f, walbwall = 0.f, wwall = 0.f, walbwallnosh = 0.f;
+        float tempbub = 0.f, tempbubwall = 0.f;
+        float s_wall = 0.f, s_Lwall = 0.f, s_Lupsh = 0.f, s_albwall = 0.f, s_albsh = 0.f, s_albwallnosh = 0.f,
+              s_albnosh = 0.f;
+        for (int n = 0; n < second_i; ++n) {
+          const int sr = r + AZ[az].dx[n], sc = c + AZ[az].dy[n];
+          if (in_grid(sr, sc, rows, cols)) {
+            const float4 g = G[(size_t)sr * cols + sc];
+            const uint32_t fl = __float_as_uint(g.w);
+            tbu = (fl & 1u) ? 1.f : 0.f;
+            tsh = g.x;
+            tlup = g.y;
+            talb = g.z;
+            talbsh = g.z * g.x;
+            twall = (fl & 2u) ? 1.f : 0.f;
+          }
+          f = tmin(f, tbu);
+          wsh_ = wsh_ + tsh * f;
+          wLupsh = wLupsh + tlup * f;
+          walbsh = walbsh + talbsh * f;
+          walbnosh = walbnosh + talb * f;
+          const float tempb = twall * f;
+          const float tempbwall = f * -1.f + 1.f;
+          tempbub = (tempb + tempbub) > 0.f ? 1.f : 0.f;
+          tempbubwall = (tempbwall + tempbubwall) > 0.f ? 1.f : 0.f;
+          wLwall = wLwall + tempbub * P.lwall;
+          walbwall = walbwall + tempbub * P.albedo_b;
+          wwall = wwall + tempbub;
+          walbwallnosh = walbwallnosh + tempbubwall * P.albedo_b;
+          if ((float)(n + 1) <= first) {
+            s_wall = wwall; s_Lwall = wLwall; s_Lupsh = wLupsh; s_albwall = walbwall; s_albsh = walbsh;
+            s_albwallnosh = walbwallnosh; s_albnosh = walbnosh;
+          }
+        }
+        const float wsi_f = s_wall > 0.f ? 1.f : 0.f;
+        const float wi_f = s_albwallnosh > 0.f ? 1.f : 0.f;
+        const float wsi_s = wwall > 0.f ? 1.f : 0.f;
+        const float wi_s = walbwallnosh > 0.f ? 1.f : 0.f;
+        const float facesh = facesh_value(AZ[az].facesh_mode, AZ[az].facesh_lo, AZ[az].facesh_hi, aspect, wallbol);
+        float keep = ((wwall == second) ? 1.f : 0.f) - facesh;
+        if (keep == -1.f) keep = 0.f;
+        const bool kz = keep == 1.f;
+        const float gLup1 = ((s_Lwall + s_Lupsh) / f1) * wsi_f + (s_Lupsh / first) * (1.f - wsi_f);
+        if (kz) wLwall = 0.f;
+        const float gLup2 = ((wLwall + wLupsh) / s1) * wsi_s + (wLupsh / second) * (1.f - wsi_s);
+        const float galb1 = ((s_albwall + s_albsh) / f1) * wsi_f + (s_albsh / first) * (1.f - wsi_f);
+        if (kz) walbwall = 0.f;
+        const float galb2 = ((walbwall + walbsh) / s1) * wsi_s + (walbsh / second) * (1.f - wsi_s);
+        const float gan1 = ((s_albwallnosh + s_albnosh) / f1) * wi_f + (s_albnosh / first) * (1.f - wi_f);
+        const float gan2 = ((walbwallnosh + walbnosh) / second) * wi_s + (walbnosh / second) * (1.f - wi_s);
+        const float gLup = (gLup1 * 0.5f + gLup2 * 0.4f) / 0.9f + lup_own * nb;
+        const float galb = (galb1 * 0.5f + galb2 * 0.4f) / 0.9f + (alb * nb) * shadow;
+        const float gan = ((gan1 * 0.5f + gan2 * 0.4f) / 0.9f) * bld + alb * nb;
+        S.Lup = S.Lup + gLup;
+        S.alb = S.alb + galb;
+        S.albnosh = S.albnosh + gan;
+        const int df = AZ[az].dir_flags;
+        if (df & 1) { S.LupE = S.LupE + gLup; S.albE = S.albE + galb; S.albnoshE = S.albnoshE + gan; }
+        if (df & 2) { S.LupS = S.LupS + gLup; S.albS = S.albS + galb; S.albnoshS = S.albnoshS + gan; }
+        if (df & 4) { S.LupW = S.LupW + gLup; S.albW = S.albW + galb; S.albnoshW = S.albnoshW + gan; }
+        if (df & 8) { S.LupN = S.LupN + gLup; S.albN = S.albN + galb; S.albnoshN = S.albnoshN + gan; }
+      }
+      const float lup_air = (P.sbc * emis) * P.ta4;
+      const float gvfLup = S.Lup / 18.f + lup_air;
+      const float gvfalb = S.alb / 18.f, gvfalbnosh = S.albnosh / 18.f;
+      const float gvfLupE = S.LupE / 9.f + lup_air, gvfLupS = S.LupS / 9.f + lup_air;
+      const float gvfLupW = S.LupW / 9.f + lup_air, gvfLupN = S.LupN / 9.f + lup_air;
+      const float gvfalbE = S.albE / 9.f, gvfalbS = S.albS / 9.f, gvfalbW = S.albW / 9.f, gvfalbN = S.albN / 9.f;
+      const float ganE = S.albnoshE / 9.f, ganS = S.albnoshS / 9.f, ganW = S.albnoshW / 9.f, ganN = S.albnoshN / 9.f;
+      // ---------------- thermal lag (state in registers)
+      const float tgtemp = tg * shadow + P.ta32;
+      const float g0[6] = {gvfLup, gvfLupE, gvfLupS, gvfLupW, gvfLupN, tgtemp};
+      float lagged[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        if (P.tw_first) st[k] = g0[k];
+        const float v = g0[k] * P.tw_a + st[k] * P.tw_b;
+        if (P.tw_mode) st[k] = v;
+        lagged[k] = v;
+      }
+      Lup = lagged[0]; LupE = lagged[1]; LupS = lagged[2]; LupW = lagged[3]; LupN = lagged[4];
+      // ---------------- shortwave
+      const float fsh = cylindric_wedge(tan_alfa, P.tan_beta, P.qa);
+      const float albF = (P.albedo_b * (1.f - svfbuveg)) * (P.radG * (1.f - fsh) + P.radD * fsh);
+      const float kup_b = P.radD * svfbuveg + albF;
+      Kup = (gvfalb * P.radI) * P.sin_alt + kup_b * gvfalbnosh;
+      KupE = (gvfalbE * P.radI) * P.sin_alt + kup_b * ganE;
+      KupS = (gvfalbS * P.radI) * P.sin_alt + kup_b * ganS;
+      KupW = (gvfalbW * P.radI) * P.sin_alt + kup_b * ganW;
+      KupN = (gvfalbN * P.radI) * P.sin_alt + kup_b * ganN;
+      const float ksideI = (shadow * P.radI) * P.cos_alt;
+      float ksideD = 0.f, kref_sun = 0.f, kref_sh = 0.f, kref_veg = 0.f, anilum = 0.f;
+      for (int q = 0; q < n_patches; ++q) {
+        const sw100_patch_step& Q = PP[q];
+        const uint32_t b = 1u << (q & 31);
+        const int w = q >> 5;
+        const bool sh = wsh[w] & b, veg = wveg[w] & b;
+        const bool vb1 = wvb[w] & b;
+        const bool vb0 = !vb1 && !(site.single_step[w] & b);
+        const int di = (sh ? 2 : 0) + (veg ? 1 : 0);
+        ksideD = ksideD + Q.kside_d[di];
+        anilum = anilum + Q.anilum[di];
+        if (!veg || vb0) kref_veg = kref_veg + Q.kref_veg;
+        if (!sh && vb1) {
+          const float td = hsvf + Q.yi_k;
+          if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
+          if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
+        }
+      }
+      Kside = (((ksideI + ksideD) + kref_sun) + kref_sh) + kref_veg;
+      const float dRad = anilum * P.radD;
+      Kdown = ((P.radI * shadow) * P.sin_alt + dRad) + albF;
+    } else {
+      Lup = (P.sbc * emis) * pow4f(P.night_lup_base);
+      LupE = LupS = LupW = LupN = Lup;
+    }
+    // ---------------- longwave (Lcyl_v2022a / define_patch_characteristics)
+    float ld_sky = 0.f, ld_veg = 0.f, ld_sh = 0.f, ld_sun = 0.f, ld_ref = 0.f;
+    float ls_sky = 0.f, ls_veg = 0.f, ls_sh = 0.f, ls_sun = 0.f, ls_ref = 0.f;
+    for (int q = 0; q < n_patches; ++q) {
+      const sw100_patch_step& Q = PP[q];
+      const uint32_t b = 1u << (q & 31);
+      const int w = q >> 5;
+      const bool sh = wsh[w] & b, veg = wveg[w] & b;
+      const bool vb1 = wvb[w] & b;
+      const bool vb0 = !vb1 && !(site.single_step[w] & b);
+      if (sh && veg) { ld_sky = ld_sky + Q.ld_sky; ls_sky = ls_sky + Q.ls_sky; }
+      if (!veg || vb0) { ls_veg = add64(ls_veg, Q.veg_cos); ld_veg = add64(ld_veg, Q.veg_sin); }
+      const bool tsh = !sh && vb1;
+      if (Q.flags & 1) {
+        if (tsh) {
+          const float td = hsvf + Q.yi_l;
+          if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
+          if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
+        }
+      } else if (tsh) {
+        ls_sh = add64(ls_sh, Q.sh_cos);
+        ld_sh = add64(ld_sh, Q.sh_sin);
+      }
+    }
+    const float refl = (((ld_sky + Lup) * P.refl_k) * 0.5f) / 3.14159274101257324f;
+    for (int q = 0; q < n_patches; ++q) {
+      const sw100_patch_step& Q = PP[q];
+      const uint32_t b = 1u << (q & 31);
+      const int w = q >> 5;
+      const bool vb0 = !(wvb[w] & b) && !(site.single_step[w] & b);
+      if (!(wsh[w] & b) || !(wveg[w] & b) || vb0) {
+        const float rs = refl * Q.ster;
+        ls_ref = ls_ref + rs * Q.cos_alt;
+        ld_ref = ld_ref + rs * Q.sin_alt;
+      }
+    }
+    const float Lside = (((ls_sky + ls_veg) + ls_sh) + ls_sun) + ls_ref;
+    const float Ldown = (((ld_sky + ld_veg) + ld_sh) + ld_sun) + ld_ref;
+    // ---------------- Tmrt (cyl == 1, anisotropic sky)
+    const float Knorth = KupN * 0.5f, Keast = KupE * 0.5f, Ksouth = KupS * 0.5f, Kwest = KupW * 0.5f;
+    const float Lnorth = LupN * 0.5f, Least = LupE * 0.5f, Lsouth = LupS * 0.5f, Lwest = LupW * 0.5f;
+    const float sstr = P.absK * (Kside * P.Fcyl + (Kdown + Kup) * P.Fup + (((Knorth + Keast) + Ksouth) + Kwest) * P.Fside) +
+                       P.absL * ((Ldown + Lup) * P.Fup + Lside * P.Fcyl + (((Lnorth + Least) + Lsouth) + Lwest) * P.Fside);
+    const float tmrt = sqrtf(sqrtf(sstr / P.absl_sbc)) - 273.2f;
+    // ---------------- outputs
+    float* o = outputs + (size_t)t * npix + p;
+    const size_t blk = (size_t)n_t * npix;
+    int slot = 0;
+    if (out_mask & SW100_OUT_UTCI) {
+      float u;
+      if (!(bld == 1.f)) {
+        u = __int_as_float(0x7fc00000);
+      } else {
+        float va = wind * P.ws32;
+        va = (va < 0.15f) ? 0.15f : va;
+        if (P.ta_mat <= -999.f || P.rh32 <= -999.f || va <= -999.f || tmrt <= -999.f) u = -999.f;
+        else u = utci_poly(P.utci_c, tmrt - P.ta_mat, va);
+      }
+      o[slot++ * blk] = u;
+    }
+    if (out_mask & SW100_OUT_TMRT) o[slot++ * blk] = tmrt;
+    if (out_mask & SW100_OUT_KUP) o[slot++ * blk] = Kup;
+    if (out_mask & SW100_OUT_KDOWN) o[slot++ * blk] = Kdown;
+    if (out_mask & SW100_OUT_LUP) o[slot++ * blk] = Lup;
+    if (out_mask & SW100_OUT_LDOWN) o[slot++ * blk] = Ldown;
+    if (out_mask & SW100_OUT_SHADOW) o[slot++ * blk] = shadow;
+  }
+  if (live) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) state[k * npix + p] = st[k];
+  }
+}
+
+}  // namespace sw100

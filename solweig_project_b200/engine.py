@@ -1,0 +1,269 @@
+"""Device-side driver of the radiation chain for one site.
+
+:class:`DeviceSite` owns the site's rasters in HBM, runs the SVF sweep and the
+time loop through the C ABI (``_native``) and hands back device tensors.
+torch provides device memory and the stream; all compute is the library's.
+
+Layout in HBM (npix = rows * cols):
+  static rasters          float32 planes, row-major
+  SVF result              16 float32 planes + 3 x 5 uint32 bit-cube words
+  packed march source     float4 {dsm, vegdsm, vegdsm2, bush}  (workspace)
+  sun-march records       n_day x npix float4 {shadow, Lup, albedo, flags} (workspace)
+  thermal state           6 float32 planes, carried across calls
+  outputs                 n_out x n_t x npix float32
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import tables as T
+from . import timeseries as TS
+
+F32 = np.float32
+SVF_NAMES = ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg", "svfNveg", "svfS", "svfSaveg",
+             "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg", "svftotal")
+STATE_NAMES = ("Tgmap1", "Tgmap1E", "Tgmap1S", "Tgmap1W", "Tgmap1N", "TgOut1")
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise N.NativeUnavailable("no CUDA device: the B200 backend runs on the GPU only")
+    N.load()
+
+
+def _dev(x, device, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).to(device, non_blocking=True)
+
+
+def _table(arr: np.ndarray, device) -> torch.Tensor:
+    """Upload a structured numpy table as raw bytes."""
+    raw = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
+    if raw.size == 0:
+        raw = np.zeros(16, np.uint8)
+    return torch.from_numpy(raw.copy()).to(device, non_blocking=True)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def march_inputs(dsm, trees, dem):
+    """Derived march rasters exactly as compute_utci / run_utci_window build
+    them (utci_process.py:667-681, 1377-1385), float32 IEEE arithmetic."""
+    a = np.asarray(dsm, F32)
+    t1 = np.asarray(trees, F32).copy()
+    t2 = np.asarray(dem, F32)
+    t1[t1 < 0.] = 0.
+    vegdem = t1 + t2
+    vegdem2 = t1 * F32(0.25) + t2
+    bush = np.logical_not(vegdem2 * vegdem).astype(F32) * vegdem
+    vegdsm = t1 + a
+    vegdsm[vegdsm == a] = 0
+    vegdsm2 = t1 * F32(0.25) + a
+    vegdsm2[vegdsm2 == a] = 0
+    amax = F32(max(a.max(), vegdem.max()))
+    buildings = a - t2
+    buildings[buildings < 2.] = 1.
+    buildings[buildings >= 2.] = 0.
+    return vegdsm, vegdsm2, bush, amax, buildings
+
+
+@dataclass
+class SvfResult:
+    planes: torch.Tensor      # (16, rows, cols) float32, SVF_NAMES order
+    bits: torch.Tensor        # (3, 5, rows, cols) int32 words (sh, vegsh, vbshvegsh)
+    single_step: np.ndarray   # uint32[5] patches with <= 1 march step
+
+    def plane(self, name):
+        return self.planes[SVF_NAMES.index(name)]
+
+    def cubes(self, n_patches=153):
+        """Dense (rows, cols, P) float32 cubes (shmat, vegshmat, vbshvegshmat)
+        as the reference returns them (shadow.py:625)."""
+        b = self.bits.view(torch.int32)
+        rows, cols = b.shape[2], b.shape[3]
+        q = torch.arange(n_patches, device=b.device)
+        words = b[:, q // 32]                                   # (3, P, rows, cols)
+        shift = (q % 32).view(1, -1, 1, 1)
+        bit = ((words >> shift) & 1).to(torch.float32)
+        single = torch.tensor([(int(self.single_step[k // 32]) >> (k % 32)) & 1 for k in range(n_patches)],
+                              device=b.device, dtype=torch.bool).view(-1, 1, 1)
+        sh, veg, vb = bit[0], bit[1], bit[2]
+        vb = torch.where(single, 2.0 - vb, vb)
+        return tuple(x.permute(1, 2, 0).contiguous() for x in (sh, veg, vb))
+
+
+class DeviceSite:
+    """One site: rasters resident on the device, SVF sweep and time loop."""
+
+    def __init__(self, dsm, trees, dem, walls, aspect_deg, scale, *, landcover=None, lc_class=None,
+                 windcoeff=None, amaxvalue=None, params: TS.ModelParams = None, device="cuda"):
+        require_cuda()
+        self.device = torch.device(device)
+        self.params = params or TS.ModelParams()
+        a = np.asarray(dsm, F32)
+        self.rows, self.cols = a.shape
+        if self.rows * self.cols >= 2 ** 31:
+            raise ValueError("grid too large")
+        vegdsm, vegdsm2, bush, amax, buildings = march_inputs(a, trees, dem)
+        self.amax = F32(amaxvalue) if amaxvalue is not None else amax
+        self.bush_any = bool(bush.max() > 0)
+        self.vmax = F32(max(a.max(), vegdsm.max(), vegdsm2.max()))
+        self.scale = float(scale)
+        d = self.device
+        self.t = {
+            "dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
+            "bush": _dev(bush, d) if self.bush_any else None, "buildings": _dev(buildings, d),
+            "walls": _dev(np.asarray(walls, F32), d),
+            "aspect_rad": _dev((np.asarray(aspect_deg, F32) * F32(np.pi)) / F32(180.), d),
+            "windcoeff": _dev(np.ones((self.rows, self.cols), F32) if windcoeff is None else
+                              np.asarray(windcoeff, F32), d),
+        }
+        self.props = TS.landcover_props(landcover, lc_class, self.rows, self.cols)
+        for k in ("tgk", "tstart", "alb", "emis"):
+            self.t[k] = _dev(getattr(self.props, k), d)
+        self.svf_result: SvfResult | None = None
+        self.state = torch.zeros((6, self.rows, self.cols), dtype=torch.float32, device=d)
+        self._keep = []
+
+    # --------------------------------------------------------------- SVF
+    def site_struct(self) -> N.SitePlanes:
+        s = N.SitePlanes()
+        t = self.t
+        s.dsm, s.vegdsm, s.vegdsm2 = t["dsm"].data_ptr(), t["vegdsm"].data_ptr(), t["vegdsm2"].data_ptr()
+        s.bush = t["bush"].data_ptr() if t["bush"] is not None else 0
+        s.vmax = float(self.vmax)
+        s.bush_any = int(self.bush_any)
+        for k in ("svfbuveg", "hsvf", "tan_alfa", "buildings", "walls", "aspect_rad", "tgk", "tstart", "alb",
+                  "emis", "class_idx", "windcoeff", "bits"):
+            v = t.get(k)
+            setattr(s, k, v.data_ptr() if v is not None else 0)
+        if self.svf_result is not None:
+            for w in range(N.CUBE_WORDS):
+                s.single_step[w] = int(self.svf_result.single_step[w])
+        return s
+
+    def run_svf(self, patch_option=2) -> SvfResult:
+        plan, steps, single = T.svf_plan(self.rows, self.cols, self.scale, self.amax, self.bush_any, patch_option)
+        d = self.device
+        plan_d, steps_d = _table(plan, d), _table(steps, d)
+        planes = torch.empty((N.SVF_PLANES, self.rows, self.cols), dtype=torch.float32, device=d)
+        bits = torch.empty((3, N.CUBE_WORDS, self.rows, self.cols), dtype=torch.int32, device=d)
+        ws_bytes = N.workspace_bytes("sw100_svf_workspace_bytes", self.rows, self.cols, len(steps))
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=d)
+        site = self.site_struct()
+        N.call("sw100_svf_sweep", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), len(steps),
+               _ptr(planes), _ptr(bits), _ptr(ws), ws_bytes, _stream())
+        self._keep = [plan_d, steps_d, ws]
+        self.svf_result = SvfResult(planes, bits, single)
+        self._prepare_loop_statics()
+        return self.svf_result
+
+    def set_svf(self, planes16, bits, single_step):
+        """Install an SVF result computed earlier (cached bundle)."""
+        self.svf_result = SvfResult(planes16, bits, np.asarray(single_step, np.uint32))
+        self._prepare_loop_statics()
+
+    def _prepare_loop_statics(self):
+        """Per-pixel statics of the time loop derived from the SVF planes:
+        svfbuveg (utci_process.py:864), hsvf = tan(asvf) with asvf =
+        acos(sqrt(svf)) (utci_process.py:865, solweig.py:550) and
+        tan(svfalfa) (utci_process.py:892-897).  The two transcendental planes
+        are evaluated with torch's CPU kernels, the reference's rounding."""
+        svf = self.svf_result.plane("svf").detach().to("cpu")
+        svfveg = self.svf_result.plane("svfveg").detach().to("cpu")
+        tv = self.params.transVeg
+        svfbuveg = svf - (1.0 - svfveg) * (1.0 - tv)
+        hsvf = torch.tan(torch.acos(torch.sqrt(svf)))
+        tmp = svf + svfveg - 1.0
+        tmp[tmp < 0.0] = 0.0
+        tan_alfa = torch.tan(torch.asin(torch.exp(torch.log(1.0 - tmp) / 2.0)))
+        d = self.device
+        self.t["svfbuveg"] = svfbuveg.to(d)
+        self.t["hsvf"] = hsvf.to(d)
+        self.t["tan_alfa"] = tan_alfa.to(d)
+        self.t["bits"] = self.svf_result.bits
+
+    # ---------------------------------------------------------- time loop
+    def build_series(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, time_start=0,
+                     time_stop=None, initial_scalars=None):
+        ser = TS.build_series(met_file=met_file, altitude=altitude, azimuth=azimuth, zen=zen, jday=jday,
+                              dectime=dectime, altmax=altmax, location=location, scale=self.scale,
+                              amax=self.amax, rows=self.rows, cols=self.cols, props=self.props,
+                              params=self.params, time_start=time_start, time_stop=time_stop,
+                              initial_scalars=initial_scalars)
+        self.t["class_idx"] = torch.from_numpy(ser.class_idx).to(self.device)
+        return ser
+
+    def upload_series(self, ser: TS.Series):
+        d = self.device
+        dev = {"steps": _table(ser.steps, d), "sun": _table(ser.sun, d), "sun_table": _table(ser.sun_table, d),
+               "patch": _table(ser.patch, d), "gvf": _table(ser.gvf, d)}
+        s = N.Series()
+        s.steps, s.sun, s.sun_table = dev["steps"].data_ptr(), dev["sun"].data_ptr(), dev["sun_table"].data_ptr()
+        s.patch, s.gvf = dev["patch"].data_ptr(), dev["gvf"].data_ptr()
+        s.n_t, s.n_day, s.n_patches = len(ser.steps), len(ser.sun), ser.patch.shape[1]
+        return s, dev
+
+    def run_time_loop(self, ser: TS.Series, requested=("utci",), series_dev=None, workspace=None):
+        """All steps of the series in one library call; returns
+        {name: (n_t, rows, cols) device tensor}."""
+        if self.svf_result is None:
+            raise RuntimeError("run_svf() (or set_svf()) must come before the time loop")
+        names = [k for k in N.OUT_BITS if k in requested]
+        mask = 0
+        for k in names:
+            mask |= N.OUT_BITS[k]
+        n_t = len(ser.steps)
+        d = self.device
+        out = torch.empty((len(names), n_t, self.rows, self.cols), dtype=torch.float32, device=d)
+        s, dev = series_dev if series_dev is not None else self.upload_series(ser)
+        ws_bytes = N.workspace_bytes("sw100_time_loop_workspace_bytes", self.rows, self.cols, s.n_day)
+        ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else \
+            torch.empty(ws_bytes, dtype=torch.uint8, device=d)
+        site = self.site_struct()
+        N.call("sw100_time_loop", C.byref(site), self.rows, self.cols, C.byref(s), _ptr(self.state), mask,
+               _ptr(out), _ptr(ws), ws.numel(), _stream())
+        self._keep = [dev, ws]
+        return {k: out[i] for i, k in enumerate(names)}
+
+    def run_sun_march(self, ser: TS.Series):
+        """Sun-march records and the 8 reference planes per daytime row
+        (parity / debugging entry)."""
+        s, dev = self.upload_series(ser)
+        d = self.device
+        n_day = max(1, s.n_day)
+        gsrc = torch.empty((n_day, self.rows, self.cols, 4), dtype=torch.float32, device=d)
+        dbg = torch.empty((n_day, 8, self.rows, self.cols), dtype=torch.float32, device=d)
+        ws_bytes = N.workspace_bytes("sw100_sun_march_workspace_bytes", self.rows, self.cols)
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=d)
+        site = self.site_struct()
+        N.call("sw100_sun_march", C.byref(site), self.rows, self.cols, C.byref(s), _ptr(gsrc), _ptr(dbg), _ptr(ws),
+               ws_bytes, _stream())
+        self._keep = [dev, ws]
+        return gsrc[:s.n_day], dbg[:s.n_day]
+
+    def load_state(self, state: dict):
+        for k, name in enumerate(STATE_NAMES):
+            self.state[k].copy_(torch.as_tensor(np.asarray(state[name], F32)))
+
+    def state_dict(self):
+        return {name: self.state[k].clone() for k, name in enumerate(STATE_NAMES)}
+
+
+def utci(ta, rh, tmrt, va) -> torch.Tensor:
+    """utci_calculator on device tensors (calculate_utci.py:259-330)."""
+    require_cuda()
+    ta, rh, tmrt, va = (torch.as_tensor(x, dtype=torch.float32, device="cuda").contiguous() for x in (ta, rh, tmrt, va))
+    out = torch.empty_like(ta)
+    N.call("sw100_utci", _ptr(ta), _ptr(rh), _ptr(tmrt), _ptr(va), ta.numel(), _ptr(out), _stream())
+    return out

@@ -1,0 +1,300 @@
+"""Host-side march and patch tables for the CUDA kernels.
+
+The kernels consume precomputed tables instead of re-deriving the scalar
+geometry on the device: the reference evaluates that geometry with 0-dim
+float32 torch tensors (sin/cos/tan of the march azimuth, tan of the altitude,
+the branch bounds) and the exact float32 bits decide which pixels are shadowed.
+Here the transcendental calls go through the same torch CPU kernels and the
+remaining per-step arithmetic (round-half-even, products, the while-loop stop
+rule) is IEEE float32 in numpy, vectorised over the steps.
+
+* SVF patch layout and weights: ``solweig_gpu/shadow.py:324-406, 530-543``
+* SVF patch march tables: ``shadow.py:196-247`` (index from 1, azimuth 0
+  replaced by 1e-12, python-float branch bounds)
+* sun march tables: ``solweig_gpu/solweig.py:1092-1149`` (index from 0,
+  float32 tensor branch bounds)
+* ground-view-factor walk offsets: ``solweig.py:136-178``
+"""
+from __future__ import annotations
+
+import functools
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+F32 = np.float32
+
+# patch option -> (annulus bounds, band altitudes, azimuth start, patches per band)
+PATCH_LAYOUT = {
+    1: ([0, 12, 24, 36, 48, 60, 72, 84, 90], [6, 18, 30, 42, 54, 66, 78, 90],
+        [0, 4, 2, 5, 8, 0, 10, 0], [30, 30, 24, 24, 18, 12, 6, 1]),
+    2: ([0, 12, 24, 36, 48, 60, 72, 84, 90], [6, 18, 30, 42, 54, 66, 78, 90],
+        [0, 4, 2, 5, 8, 0, 10, 0], [31, 30, 28, 24, 19, 13, 7, 1]),
+}
+
+
+# --------------------------------------------------------------- patches
+@functools.lru_cache(maxsize=None)
+def sky_patches(patch_option: int = 2):
+    """(altitude, azimuth) float32 of every sky patch (shadow.py:352-406)."""
+    _, altint, azistart, nband = PATCH_LAYOUT[patch_option]
+    width = 360 / torch.tensor(nband)
+    alt, azi = [], []
+    for j, n in enumerate(nband):
+        for k in range(n):
+            alt.append(float(altint[j]))
+            azi.append((k * width[j] + torch.tensor(azistart[j])).item())
+    return np.array(alt, F32), np.array(azi, F32)
+
+
+@functools.lru_cache(maxsize=None)
+def sweep_azimuths(patch_option: int = 2) -> np.ndarray:
+    """Azimuth the SVF sweep marches for each patch (shadow.py:530-541).
+
+    Each band contributes int(360 / float32(360 / n)) entries, one short of
+    n for most bands; the vector starts as zeros, so later patches take the
+    shifted azimuths and the last ones keep 0."""
+    _, altint, azistart, nband = PATCH_LAYOUT[patch_option]
+    width = torch.tensor([360 / p for p in torch.tensor(nband)])
+    out = np.zeros(int(sum(nband)), F32)
+    i = 0
+    for j in range(len(altint)):
+        for k in range(int(360 / width[j])):
+            v = k * width[j] + torch.tensor(azistart[j])
+            if v > 360.:
+                v = v - 360.
+            out[i] = F32(v.item())
+            i += 1
+    return out
+
+
+def _annulus_weight(k: int, n) -> np.float32:
+    """Weight of annulus k over n azimuth bins (shadow.py:324-350)."""
+    nn = torch.tensor(90.0)
+    steprad = (360.0 / n) * (torch.pi / 180.0)
+    annulus = 91.0 - torch.tensor(k)
+    w = (1.0 / (2.0 * torch.pi)) * torch.sin(torch.pi / (2.0 * nn)) * \
+        torch.sin((torch.pi * (2.0 * annulus - 1.0)) / (2.0 * nn))
+    return F32((steprad * w).item())
+
+
+@functools.lru_cache(maxsize=None)
+def ring_weights(patch_option: int = 2):
+    """Per band: iso and aniso annulus weights (float32), annuli count."""
+    annulino, altint, _, nband = PATCH_LAYOUT[patch_option]
+    nb = torch.tensor(nband)
+    aniso = torch.ceil(nb / 2.0)
+    w_iso = np.zeros((N.MAX_RINGS, N.MAX_ANNULI), F32)
+    w_an = np.zeros((N.MAX_RINGS, N.MAX_ANNULI), F32)
+    count = np.zeros(N.MAX_RINGS, np.int32)
+    for i in range(len(altint)):
+        ks = range(annulino[i] + 1, annulino[i + 1] + 1)
+        count[i] = len(ks)
+        for j, k in enumerate(ks):
+            w_iso[i, j] = _annulus_weight(k, nb[i])
+            w_an[i, j] = _annulus_weight(k, aniso[i])
+    return w_iso, w_an, count
+
+
+# ------------------------------------------------------------ step tables
+def _march_steps(branch_y, ssin, scos, tan_a, ds, tanalt, idx):
+    """Per-step (dx, dy, dz) for the index vector (float32 arithmetic)."""
+    fi = idx.astype(F32)
+    m_scos = F32(-1.) * scos
+    if branch_y:
+        dy = ssin * fi
+        dx = m_scos * np.abs(np.rint(fi / tan_a))
+    else:
+        dy = ssin * np.abs(np.rint(fi * tan_a))
+        dx = m_scos * fi
+    dz = (ds * fi) * tanalt
+    return dx.astype(F32), dy.astype(F32), dz.astype(F32)
+
+
+def _executed(dx, dy, dz, amax, rows, cols):
+    """Number of executed steps: step k runs while the previous step still
+    satisfied ``amax >= dz and |dx| < rows and |dy| < cols`` (the first step
+    always sees the zero initial state)."""
+    ok = (F32(amax) >= dz) & (np.abs(dx) < rows) & (np.abs(dy) < cols)
+    if not (F32(amax) >= F32(0.)):
+        return 0
+    bad = np.flatnonzero(~ok)
+    return int(bad[0]) + 1 if bad.size else len(dz)
+
+
+def _trig(az, alt):
+    sin_a, cos_a, tan_a = torch.sin(az), torch.cos(az), torch.tan(az)
+    return (F32(torch.sign(sin_a).item()), F32(torch.sign(cos_a).item()), F32(tan_a.item()),
+            F32(torch.abs(1. / sin_a).item()), F32(torch.abs(1. / cos_a).item()))
+
+
+def svf_patch_table(azimuth_deg, altitude_deg, scale, amax, rows, cols):
+    """Executed steps of one SVF patch march (shadow.py:196-247)."""
+    degrees = torch.pi / 180.
+    az = torch.tensor(1e-12) if float(azimuth_deg) == 0.0 else torch.tensor(F32(azimuth_deg))
+    alt = torch.tensor(int(altitude_deg))
+    az = az * degrees
+    alt = alt * degrees
+    ssin, scos, tan_a, dssin, dscos = _trig(az, alt)
+    tanalt = F32((torch.tan(alt) / scale).item())
+    pb4 = torch.pi / 4.
+    branch_y = bool((pb4 <= az) & (az < 3. * pb4)) or bool((5. * pb4 <= az) & (az < 7. * pb4))
+    ds = dssin if branch_y else dscos
+    idx = np.arange(1, max(rows, cols) + 3)
+    dx, dy, dz = _march_steps(branch_y, ssin, scos, tan_a, ds, tanalt, idx)
+    n = _executed(dx, dy, dz, amax, rows, cols)
+    return dx[:n].astype(np.int32), dy[:n].astype(np.int32), dz[:n]
+
+
+def sun_table(azimuth, altitude, scale, amax, rows, cols):
+    """Executed steps of the sun march (solweig.py:1092-1149); returns the
+    steps and the float32 azimuth in radians used by the wall tail."""
+    degrees = torch.tensor(np.pi / 180.0)
+    az = torch.tensor(azimuth) * degrees
+    alt = torch.tensor(altitude) * degrees
+    ssin, scos, tan_a, dssin, dscos = _trig(az, alt)
+    tanalt = F32((torch.tan(alt) / scale).item())
+    pb4 = torch.tensor(np.pi / 4.0)
+    branch_y = bool((pb4 <= az) & (az < 3 * pb4)) or bool((5 * pb4 <= az) & (az < 7 * pb4))
+    ds = dssin if branch_y else dscos
+    idx = np.arange(0, max(rows, cols) + 3)
+    dx, dy, dz = _march_steps(branch_y, ssin, scos, tan_a, ds, tanalt, idx)
+    n = _executed(dx, dy, dz, amax, rows, cols)
+    return dx[:n].astype(np.int32), dy[:n].astype(np.int32), dz[:n], F32(az.item())
+
+
+def facesh_thresholds(az_rad_f32):
+    """Branch and float32 bounds of the wall-face test (solweig.py:1187-1196,
+    :239-248): mode 0 -> facesh = [aspect < lo or aspect >= hi] - wallbol + 1,
+    mode 1 -> facesh = 1 - [aspect > lo or aspect <= hi]."""
+    azt = torch.tensor(F32(az_rad_f32))
+    lo = azt - torch.pi / 2
+    hi = azt + torch.pi / 2
+    if lo >= 0 and hi < 2 * torch.pi:
+        return 0, F32(lo.item()), F32(hi.item())
+    if lo < 0 and hi <= 2 * torch.pi:
+        lo = lo + 2 * torch.pi
+    elif lo > 0 and hi >= 2 * torch.pi:
+        hi = hi - 2 * torch.pi
+    else:
+        raise ValueError(f"sun azimuth {az_rad_f32} outside the wall-face branches")
+    return 1, F32(lo.item()), F32(hi.item())
+
+
+@functools.lru_cache(maxsize=None)
+def gvf_table(second: int) -> np.ndarray:
+    """Walk offsets and face bounds of the 18 ground-view-factor azimuths."""
+    if second > N.MAX_GVF_STEPS:
+        raise ValueError(f"ground view factor walk of {second} steps exceeds {N.MAX_GVF_STEPS}")
+    tab = np.zeros(N.N_GVF_AZ, N.GVF_AZ_DTYPE)
+    azs = np.arange(5, 359, 20, dtype=np.float32)
+    for j, a in enumerate(azs):
+        az = torch.tensor(a) * (torch.pi / 180)
+        ssin, scos, tan_a, _, _ = _trig(az, az)
+        pb4 = torch.pi / 4
+        branch_y = bool((pb4 <= az) & (az < 3 * pb4)) or bool((5 * pb4 <= az) & (az < 7 * pb4))
+        dx, dy, _ = _march_steps(branch_y, ssin, scos, tan_a, F32(0), F32(0), np.arange(second))
+        tab["dx"][j, :second] = dx.astype(np.int8)
+        tab["dy"][j, :second] = dy.astype(np.int8)
+        mode, lo, hi = facesh_thresholds(F32(az.item()))
+        tab["facesh_mode"][j], tab["facesh_lo"][j], tab["facesh_hi"][j] = mode, lo, hi
+        flags = 0
+        if 0 <= a < 180:
+            flags |= 1
+        if 90 <= a < 270:
+            flags |= 2
+        if 180 <= a < 360:
+            flags |= 4
+        if 270 <= a or a < 90:
+            flags |= 8
+        tab["dir_flags"][j] = flags
+    return tab
+
+
+def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2):
+    """SVF plan record + concatenated step table + single-step patch mask."""
+    annulino, altint, _, nband = PATCH_LAYOUT[patch_option]
+    azs = sweep_azimuths(patch_option)
+    w_iso, w_an, count = ring_weights(patch_option)
+    plan = np.zeros(1, N.SVF_PLAN_DTYPE)
+    P = int(sum(nband))
+    plan["n_patches"] = P
+    plan["n_rings"] = len(altint)
+    plan["bush_any"] = int(bool(bush_any))
+    plan["ring_annuli"][0, :] = count
+    plan["w_iso"][0] = w_iso
+    plan["w_aniso"][0] = w_an
+    plan["tail"] = F32(3.0459e-004)
+    plan["trans"] = F32(0.03)
+    chunks = []
+    off = 0
+    single = np.zeros(N.CUBE_WORDS, np.uint32)
+    q = 0
+    for i in range(len(altint)):
+        for _ in range(nband[i]):
+            dx, dy, dz = svf_patch_table(azs[q], altint[i], scale, amax, rows, cols)
+            n = len(dz)
+            t = np.zeros(n, N.STEP_DTYPE)
+            t["dx"], t["dy"], t["dz"] = dx, dy, dz
+            chunks.append(t)
+            plan["step_offset"][0, q] = off
+            plan["step_count"][0, q] = n
+            plan["ring"][0, q] = i
+            a = float(azs[q])
+            plan["dir_flags"][0, q] = ((1 if 0 <= a < 180 else 0) | (2 if 90 <= a < 270 else 0) |
+                                       (4 if 180 <= a < 360 else 0) | (8 if (a >= 270 or a < 90) else 0))
+            if n <= 1:
+                single[q >> 5] |= np.uint32(1 << (q & 31))
+            off += n
+            q += 1
+    steps = np.concatenate(chunks) if chunks else np.zeros(0, N.STEP_DTYPE)
+    return plan, steps, single
+
+
+# ----------------------------------------------------- predicate bounds
+def _f32_to_key(x):
+    b = np.asarray(x, F32).view(np.int32).astype(np.int64)
+    return np.where(b >= 0, b, -(b & 0x7FFFFFFF))
+
+
+def _key_to_f32(k):
+    k = np.asarray(k, np.int64)
+    b = np.where(k >= 0, k, (-k) | 0x80000000).astype(np.uint32)
+    return b.view(F32)
+
+
+@functools.lru_cache(maxsize=None)
+def atan_degree_bounds(palt: float):
+    """Bounds on tan_delta for the shaded_or_sunlit predicate
+    (solweig.py:524-562): with g(x) = float32(atan(x) * (180 / pi)) evaluated
+    by torch's CPU kernel,  sunlit <=> x < lo  and  shaded <=> x > hi, where
+    lo = min{x : g(x) >= palt} and hi = max{x : g(x) <= palt}.  g is monotone;
+    both bounds are found by bisection over the ordered float32 values."""
+    palt = F32(palt)
+    rad2deg = 180.0 / torch.pi
+
+    def g(keys):
+        x = torch.from_numpy(_key_to_f32(keys).copy())
+        return (torch.atan(x) * rad2deg).numpy()
+
+    inf_key = int(_f32_to_key(F32(np.inf)))
+
+    def search(pred):  # smallest key with pred(g) true (monotone false -> true)
+        lo, hi = -inf_key, inf_key
+        if not pred(g(np.array([hi])))[0]:
+            return None
+        while hi - lo > 1:
+            mid = (lo + hi) // 2
+            if pred(g(np.array([mid])))[0]:
+                hi = mid
+            else:
+                lo = mid
+        return hi
+
+    k_lo = search(lambda v: v >= palt)
+    k_gt = search(lambda v: v > palt)
+    lo = F32(np.inf) if k_lo is None else _key_to_f32(np.array([k_lo]))[0]
+    hi = F32(np.inf) if k_gt is None else _key_to_f32(np.array([k_gt - 1]))[0]
+    return F32(lo), F32(hi)

@@ -1,0 +1,537 @@
+"""Per-step scalar chain of the time loop, packed into the kernel tables.
+
+Everything that does not vary across pixels is evaluated here, once per step,
+with 0-dim torch CPU tensors of the dtypes the reference uses (float64 met
+scalars, float32 sun geometry), so that every scalar the kernels read has the
+reference's float32/float64 bits:
+
+* sky emissivity, clearness index, diffuse fraction and the Perez sky
+  luminance per patch (``solweig_gpu/solweig.py:2038-2073, 851-983, 1227-1356``)
+* the ground temperature wave and CI_TgG (``solweig.py:2101-2122``)
+* wall temperature and the wall longwave terms (``solweig.py:118-121,
+  1594-1597``)
+* TsWaveDelay weights (``solweig.py:451-488``)
+* steradians, luminance shares and the sky longwave per patch
+  (``solweig.py:683-731, 1651-1760``)
+* the bounds of the shaded/sunlit patch predicate (``solweig.py:524-562``)
+* UTCI polynomial coefficients in (D_Tmrt, va) (``calculate_utci.py:24-330``)
+"""
+from __future__ import annotations
+
+import json
+import os
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _native as N
+from . import tables as T
+
+F32 = np.float32
+SBC = 5.67051e-8
+PKG = os.path.dirname(os.path.abspath(__file__))
+
+
+@dataclass
+class ModelParams:
+    """Model and receptor constants (utci_process.py:49-69) with the
+    override names run_utci_window accepts (utci_process.py:78-82)."""
+
+    albedo_b: float = 0.2
+    ewall: float = 0.9
+    absK: float = 0.7
+    absL: float = 0.95
+    Fside: float = 0.22
+    Fup: float = 0.06
+    Fcyl: float = 0.28
+    cyl: bool = True
+    elvis: float = 0
+    anisotropic_sky: int = 1
+    transVeg: float = 3. / 100.
+    height: float = 1.1
+    firstdayleaf: int = 97
+    lastdayleaf: int = 300
+
+
+PARAM_NAMES = frozenset(ModelParams.__dataclass_fields__)
+
+_G = ((10.0, (3.37, 2.85, 2.80, 2.64)), (20.0, (2.99, 3.02, 2.70, 2.93)), (30.0, (3.60, 3.00, 2.98, 2.93)),
+      (40.0, (3.04, 3.11, 2.92, 2.94)), (50.0, (2.70, 2.95, 2.77, 2.71)), (60.0, (2.52, 3.07, 2.67, 2.93)),
+      (70.0, (1.76, 2.69, 2.61, 2.61)), (80.0, (1.60, 1.67, 2.24, 2.63)), (90.0, (1.11, 1.44, 1.94, 2.02)))
+
+# Perez et al. (1993) coefficient sets, rows = clearness bins, columns = the
+# four terms of each of a..e (the published table, as solweig.py:1250-1269)
+_PEREZ = {
+    "a": ((1.3525, -0.2576, -0.2690, -1.4366), (-1.2219, -0.7730, 1.4148, 1.1016), (-1.1000, -0.2515, 0.8952, 0.0156),
+          (-0.5484, -0.6654, -0.2672, 0.7117), (-0.6000, -0.3566, -2.5000, 2.3250), (-1.0156, -0.3670, 1.0078, 1.4051),
+          (-1.0000, 0.0211, 0.5025, -0.5119), (-1.0500, 0.0289, 0.4260, 0.3590)),
+    "b": ((-0.7670, 0.0007, 1.2734, -0.1233), (-0.2054, 0.0367, -3.9128, 0.9156), (0.2782, -0.1812, -4.5000, 1.1766),
+          (0.7234, -0.6219, -5.6812, 2.6297), (0.2937, 0.0496, -5.6812, 1.8415), (0.2875, -0.5328, -3.8500, 3.3750),
+          (-0.3000, 0.1922, 0.7023, -1.6317), (-0.3250, 0.1156, 0.7781, 0.0025)),
+    "c": ((2.8000, 0.6004, 1.2375, 1.0000), (6.9750, 0.1774, 6.4477, -0.1239), (24.7219, -13.0812, -37.7000, 34.8438),
+          (33.3389, -18.3000, -62.2500, 52.0781), (21.0000, -4.7656, -21.5906, 7.2492), (14.0000, -0.9999, -7.1406, 7.5469),
+          (19.0000, -5.0000, 1.2438, -1.9094), (31.0625, -14.5000, -46.1148, 55.3750)),
+    "d": ((1.8734, 0.6297, 0.9738, 0.2809), (-1.5798, -0.5081, -1.7812, 0.1080), (-5.0000, 1.5218, 3.9229, -2.6204),
+          (-3.5000, 0.0016, 1.1477, 0.1062), (-3.5000, -0.1554, 1.4062, 0.3988), (-3.4000, -0.1078, -1.0750, 1.5702),
+          (-4.0000, 0.0250, 0.3844, 0.2656), (-7.2312, 0.4050, 13.3500, 0.6234)),
+    "e": ((0.0356, -0.1246, -0.5718, 0.9938), (0.2624, 0.0672, -0.2190, -0.4285), (-0.0156, 0.1597, 0.4199, -0.5562),
+          (0.4659, -0.3296, -0.0876, -0.0329), (0.0032, 0.0766, -0.0656, -0.1294), (-0.0672, 0.4016, 0.3017, -0.4844),
+          (1.0468, -0.3788, -2.4517, 1.4656), (1.5000, -0.6426, 1.8564, 0.5636)),
+}
+_CLEAR_BINS = (1.065, 1.230, 1.500, 1.950, 2.800, 4.500, 6.200)
+
+
+def _utci_terms():
+    with open(os.path.join(PKG, "data", "utci_terms.json")) as fh:
+        return [(float(F32(float(c))), a, b, d, e) for c, a, b, d, e in json.load(fh)["terms"]]
+
+
+_TERMS = _utci_terms()
+_ES_G = (-2.8365744E3, -6.028076559E3, 1.954263612E1, -2.737830188E-2, 1.6261698E-5, 7.0229056E-10,
+         -1.8680009E-13, 2.7150305)
+
+
+# --------------------------------------------------------------- scalars
+def _snup(jday_f32, lat_f32):
+    """Sunrise hour of daylen (solweig.py:47-73)."""
+    rad = torch.pi / 180.0
+    dec = -23.45 * torch.cos(2.0 * torch.pi * (jday_f32 + 10.0) / 365.0)
+    soc = torch.clamp(torch.tan(rad * dec) * torch.tan(rad * lat_f32), -1.0, 1.0)
+    return 12.0 - (12.0 + 24.0 * torch.arcsin(soc) / torch.pi) / 2.0
+
+
+def _clearness(zen, jday, Ta, RH, radG, latitude, P):
+    """clearnessindex_2013b (solweig.py:851-926) -> I0, CI, Kt."""
+    p = 1013.0 if P == -999.0 else P * 10.0
+    b = 2. * torch.pi * jday / 365.
+    D = torch.sqrt(1.00011 + 0.034221 * torch.cos(b) + 0.001280 * torch.sin(b) + 0.000719 * torch.cos(2. * b)
+                   + 0.000077 * torch.sin(2. * b))
+    cz = torch.cos(zen)
+    m = 35.0 * cz * ((1224.0 * (cz ** 2) + 1.0) ** (-1 / 2.0))
+    trpg = 1.021 - 0.084 * (m * (0.000949 * p + 0.051)) ** 0.5
+    G = next(g for hi, g in _G if latitude < hi)
+    if jday > 335 or jday <= 60:
+        G = G[0]
+    elif 60 < jday <= 152:
+        G = G[1]
+    elif 152 < jday <= 244:
+        G = G[2]
+    else:
+        G = G[3]
+    a2, b2 = torch.tensor(17.27), torch.tensor(237.7)
+    inner = ((a2 * Ta) / (b2 + Ta)) + torch.log(RH)
+    Td = (b2 * inner) / (a2 - inner)
+    Td = (Td * 1.8) + 32
+    u = torch.exp(0.1133 - torch.log(torch.tensor(G + 1.)) + 0.0393 * Td)
+    Tw = 1 - 0.077 * ((u * m) ** 0.3)
+    I0 = 1370.0 * torch.cos(zen) * trpg * Tw * D * (0.935 ** m)
+    I0 = torch.where(torch.abs(zen) > torch.pi / 2, torch.tensor(0.0), I0)
+    I0 = torch.where(torch.isnan(I0), torch.tensor(0.0), I0)
+    corr = 0.1473 * torch.log(90 - (zen / torch.pi * 180)) + 0.3454
+    return I0, radG / I0 + (1 - corr), radG / (1370.0 * torch.cos(zen) * D)
+
+
+def _diffuse(radG, altitude, Kt, Ta, RH):
+    """diffusefraction, Reindl et al. (1990) (solweig.py:928-983)."""
+    Ta = Ta if isinstance(Ta, torch.Tensor) else torch.tensor(Ta)
+    RH = RH if isinstance(RH, torch.Tensor) else torch.tensor(RH)
+    alfa = altitude * (torch.pi / 180.0)
+    alfa = alfa if isinstance(alfa, torch.Tensor) else torch.tensor(alfa)
+    if Ta <= -999.00 or RH <= -999.00 or torch.isnan(Ta) or torch.isnan(RH):
+        if Kt <= 0.3:
+            radD = radG * (1.020 - 0.248 * Kt)
+        elif 0.3 < Kt < 0.78:
+            radD = radG * (1.45 - 1.67 * Kt)
+        else:
+            radD = radG * 0.147
+    else:
+        RH = RH / 100
+        s = torch.sin(alfa)
+        if Kt <= 0.3:
+            radD = radG * (1 - 0.232 * Kt + 0.0239 * s - 0.000682 * Ta + 0.0195 * RH)
+        elif 0.3 < Kt < 0.78:
+            radD = radG * (1.329 - 1.716 * Kt + 0.267 * s - 0.00357 * Ta + 0.106 * RH)
+        else:
+            radD = radG * (0.426 * Kt - 0.256 * s + 0.00349 * Ta + 0.0734 * RH)
+    radI = (radG - radD) / torch.sin(alfa)
+    radI = torch.where(radI < 0, torch.tensor(0.0), radI)
+    radI = torch.where((altitude < 1) & (radI > radG), radG, radI)
+    radD = torch.where(radD > radG, radG, radD)
+    return radI, radD
+
+
+def _perez(zen_deg, azimuth_deg, radD, radI, jday):
+    """Perez_v3 with patchchoice 1 (solweig.py:1227-1356): (P, 3) float32."""
+    deg2rad = torch.tensor(np.pi / 180)
+    rad2deg = torch.tensor(180 / np.pi)
+    zen = torch.tensor(zen_deg) * deg2rad
+    azimuth = torch.tensor(azimuth_deg) * deg2rad
+    altitude = torch.tensor(90 - zen_deg) * deg2rad
+    z3 = 1.041 * torch.pow(zen, 3)
+    clearness = ((radD + radI) / (radD + z3)) / (1 + z3)
+    da = torch.tensor(jday * 2 * torch.pi / 365)
+    I0 = 1367 * (1.00011 + 0.034221 * torch.cos(da) + 0.00128 * torch.sin(da) + 0.000719 * torch.cos(2 * da)
+                 + 0.000077 * torch.sin(2 * da))
+    if altitude >= 10 * deg2rad:
+        airmass = 1 / torch.sin(altitude)
+    elif altitude < 0:
+        airmass = 1 / torch.sin(altitude) + 0.50572 * torch.pow(
+            180 * torch.complex(altitude, torch.tensor(0.)) / torch.pi + 6.07995, -1.6364)
+    else:
+        airmass = 1 / torch.sin(altitude) + 0.50572 * torch.pow(180 * altitude / torch.pi + 6.07995, -1.6364)
+    bright = (airmass * radD) / I0
+    if radD <= 10:
+        bright = torch.tensor(0.0)
+    ic = next((j for j, b in enumerate(_CLEAR_BINS) if clearness < b), 7)
+    co = {k: torch.tensor(v[ic]) for k, v in _PEREZ.items()}
+
+    def lin(c):
+        return c[0] + c[1] * zen + bright * (c[2] + c[3] * zen)
+
+    m_a, m_b, m_e = lin(co["a"]), lin(co["b"]), lin(co["e"])
+    if ic > 0:
+        m_c, m_d = lin(co["c"]), lin(co["d"])
+    else:
+        c, d = co["c"], co["d"]
+        m_c = torch.exp(torch.pow(bright * (c[0] + c[1] * zen), c[2])) - 1
+        m_d = -torch.exp(bright * (d[0] + d[1] * zen)) + d[2] + bright * d[3] * bright
+    alt_p, azi_p = (torch.from_numpy(v) for v in T.sky_patches(2))
+    skyzen = (90 - alt_p) * deg2rad
+    skyalt = alt_p * deg2rad
+    skyazi = azi_p * deg2rad
+    cs = torch.sin(skyalt) * torch.sin(altitude) + torch.cos(altitude) * torch.cos(skyalt) * \
+        torch.cos(torch.abs(skyazi - azimuth))
+    lv = (1 + m_a * torch.exp(m_b / torch.cos(skyzen))) * ((1 + m_c * torch.exp(m_d * torch.arccos(cs)) +
+                                                          m_e * cs * cs))
+    lv = lv / torch.sum(lv)
+    return torch.stack([skyalt * rad2deg, skyazi * rad2deg, lv], dim=1)
+
+
+def _steradians(palt):
+    """Solid angle of each patch (solweig.py:688-697, 1707-1718)."""
+    deg2rad = torch.tensor(np.pi / 180)
+    skyalt, cnt = torch.unique(palt, return_counts=True)
+    ster = torch.zeros(palt.shape[0])
+    for i in range(palt.shape[0]):
+        c = cnt[skyalt == palt[i]]
+        if c > 1:
+            ster[i] = ((360 / c) * deg2rad) * (torch.sin((palt[i] + palt[0]) * deg2rad)
+                                               - torch.sin((palt[i] - palt[0]) * deg2rad))
+        else:
+            ster[i] = ((360 / c) * deg2rad) * (torch.sin(palt[i] * deg2rad)
+                                               - torch.sin((palt[i - 1] + palt[0]) * deg2rad))
+    return ster
+
+
+def _lsky(esky, palt, Ta64):
+    """Sky longwave per patch on horizontal / vertical surfaces with the
+    Martin & Berdahl band emissivities (model2, solweig.py:1394-1413, 1725-1737)."""
+    deg2rad = torch.tensor(np.pi / 180)
+    sbc = torch.tensor(SBC)
+    u, _ = torch.unique(palt, return_counts=True)
+    band = 1 - (1 - esky) * torch.exp(0.308 * (1.7 - (1 / torch.cos((90 - u) * deg2rad))))
+    ster = _steradians(palt)
+    ld = torch.zeros(palt.shape[0])
+    ls = torch.zeros(palt.shape[0])
+    ta4 = (Ta64 + 273.15) ** 4
+    for alt in u:
+        msk = palt == alt
+        base = (band[u == alt] * sbc * ta4) / torch.tensor(np.pi)
+        ld[msk] = base * ster[msk] * torch.sin(alt * deg2rad)
+        ls[msk] = base * ster[msk] * torch.cos(alt * deg2rad)
+    return ld, ls, ster
+
+
+def _utci_coeffs(ta_mat: np.float32, rh32: np.float32) -> np.ndarray:
+    """Fold the 210-term regression for this step's Ta and Pa into a
+    polynomial in (D_Tmrt, va): c[d * 7 + v] (calculate_utci.py:24-330)."""
+    tk = torch.tensor([float(ta_mat)], dtype=torch.float32) + 273.15
+    g = torch.tensor(_ES_G, dtype=torch.float32)
+    es = g[7] * torch.log(tk)
+    for i in range(7):
+        es = es + g[i] * tk ** (i + 1 - 3.)
+    es = torch.exp(es) * 0.01
+    pa = float((es * torch.tensor([float(rh32)], dtype=torch.float32) / 100. / 10.0).item())
+    ta = float(ta_mat)
+    c = np.zeros(49, np.float64)
+    c[0] += ta
+    for coef, pt, pv, pd, pp in _TERMS:
+        c[pd * 7 + pv] += coef * ta ** pt * pa ** pp
+    return c
+
+
+# -------------------------------------------------------------- the series
+@dataclass
+class LandCoverProps:
+    """Per-pixel surface properties and the wall class (Tgmaps_v1.py:15-53)."""
+
+    tgk: np.ndarray
+    tstart: np.ndarray
+    alb: np.ndarray
+    emis: np.ndarray
+    tmaxlst: np.ndarray
+    tgk_wall: object
+    tstart_wall: object
+    tmaxlst_wall: object
+    landcover: int
+
+
+def landcover_props(lc_grid, lc_class, rows, cols) -> LandCoverProps:
+    """Cleaned land-cover codes -> property grids (utci_process.py:733-766)."""
+    if lc_grid is None:
+        z = np.zeros((rows, cols), F32)
+        return LandCoverProps(z + F32(0.37), z - F32(3.41), z + F32(0.15), z + F32(0.95), None, 0.37, -3.41, 15., 0)
+    lc = np.array(lc_grid, F32, copy=True)
+    lc[(lc < 1) | (lc > 7)] = 6
+    lc[(lc == 3) | (lc == 4)] = 5
+    ids = np.unique(lc)
+    out = {k: np.copy(lc) for k in ("tgk", "tstart", "alb", "emis", "tmax")}
+    cols_ = {"tstart": 4, "alb": 1, "emis": 2, "tmax": 5, "tgk": 3}
+    for v in ids:
+        row = lc_class[:, 0] == v
+        for k in ("tstart", "alb", "emis", "tmax", "tgk"):
+            arr = out[k]
+            arr[arr == v] = lc_class[row, cols_[k]]
+    wall = np.where(lc_class[:, 0] == 99)
+    return LandCoverProps(out["tgk"], out["tstart"], out["alb"], out["emis"], out["tmax"],
+                          np.asarray(lc_class[wall, 3], F32), np.asarray(lc_class[wall, 4], F32),
+                          np.asarray(lc_class[wall, 5], F32), 1)
+
+
+@dataclass
+class Series:
+    steps: np.ndarray         # TIME_STEP_DTYPE (n_t)
+    sun: np.ndarray           # SUN_STEP_DTYPE (n_day)
+    sun_table: np.ndarray     # STEP_DTYPE
+    patch: np.ndarray         # PATCH_STEP_DTYPE (n_t, P)
+    gvf: np.ndarray           # GVF_AZ_DTYPE (18)
+    final: dict               # carried scalars after the last step
+    class_idx: np.ndarray     # uint8 per pixel
+
+
+def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, scale, amax, rows, cols,
+                 props: LandCoverProps, params: ModelParams = None, time_start=0, time_stop=None,
+                 initial_scalars=None, patch_option=2) -> Series:
+    """Tables for steps [time_start, time_stop) of run_utci_window's loop
+    (utci_process.py:917-1067)."""
+    if params is None:
+        params = ModelParams()
+    if params.anisotropic_sky != 1 or not params.cyl:
+        raise NotImplementedError("only the reference defaults cyl=1, anisotropic_sky=1 are implemented")
+    if time_stop is None:
+        time_stop = met_file.shape[0]
+    n_t = time_stop - time_start
+    lat = location["latitude"]
+    Ta_all, RH_all, radG_all = met_file[:, 11], met_file[:, 10], met_file[:, 14]
+    P_all, Ws_all = met_file[:, 12], met_file[:, 9]
+    uhii_all = met_file[:, 24] if met_file.shape[1] > 24 else np.zeros(met_file.shape[0])
+    DOY = met_file[:, 1]
+    fdl, ldl = params.firstdayleaf, params.lastdayleaf
+    leaf = ((DOY > fdl) | (DOY < ldl)) if fdl > ldl else ((DOY > fdl) & (DOY < ldl))
+    psi = np.where(leaf, F32(1) * F32(params.transVeg), F32(0.5)).astype(F32)
+    height = torch.tensor(params.height)
+    first = torch.round(height)
+    if first == 0.:
+        first = torch.tensor(1.)
+    second = torch.round(height * 20.)
+    sc = torch.tensor(scale)
+    first_g = torch.round(first * sc)
+    first_g = torch.tensor(1.) if first_g < 1 else first_g
+    second_g = torch.round(second * sc)
+    first_f, second_f = F32(first_g.item()), F32(second_g.item())
+    timestepdec = 0 if met_file.shape[0] == 1 else dectime[1] - dectime[0]
+    if initial_scalars is None:
+        timeadd, firstdaytime, CI = 0., 1., 1.0
+    else:
+        timeadd = float(initial_scalars["timeadd"])
+        firstdaytime = float(initial_scalars["firstdaytime"])
+        CI = float(initial_scalars["CI"])
+
+    # pixel classes of the ground temperature wave
+    if props.landcover:
+        tvals, class_idx = np.unique(props.tmaxlst, return_inverse=True)
+        if len(tvals) > N.MAX_CLASSES:
+            raise ValueError(f"more than {N.MAX_CLASSES} distinct TmaxLST classes")
+        class_idx = class_idx.reshape(rows, cols).astype(np.uint8)
+    else:
+        tvals = np.array([15.], F32)
+        class_idx = np.zeros((rows, cols), np.uint8)
+
+    P = int(sum(T.PATCH_LAYOUT[patch_option][3]))
+    steps = np.zeros(n_t, N.TIME_STEP_DTYPE)
+    patch = np.zeros((n_t, P), N.PATCH_STEP_DTYPE)
+    sun_rows, tables = [], []
+    sun_off = 0
+    sbc_t = torch.tensor(SBC)
+    ewall_t = torch.tensor(params.ewall)
+    deg2rad_t = torch.tensor(np.pi / 180)
+    alt_n, azi_n = T.sky_patches(patch_option)
+    night_patches = torch.stack([torch.from_numpy(alt_n), torch.from_numpy(azi_n), torch.zeros(P)], dim=1)
+    diff_vals = np.array([F32(s) - (F32(1) - F32(v)) * F32(1 - params.transVeg) for s in (0, 1) for v in (0, 1)], F32)
+
+    for o, i in enumerate(range(time_start, time_stop)):
+        S = steps[o]
+        if (dectime[i] - np.floor(dectime[i])) == 0:
+            CI = 1.
+        alt64 = torch.tensor(altitude[0][i])
+        azi64 = torch.tensor(azimuth[0][i])
+        zen64 = torch.tensor(zen[0][i])
+        Ta64 = torch.tensor(Ta_all[i])
+        RH64 = torch.tensor(RH_all[i])
+        radG64 = torch.tensor(radG_all[i])
+        jd = jday[0][i]
+        ea = 6.107 * 10 ** ((7.5 * Ta64) / (237.3 + Ta64)) * (RH64 / 100.)
+        msteg = 46.5 * (ea / (Ta64 + 273.15))
+        esky = (1 - (1 + msteg) * torch.exp(-((1.2 + 3.0 * msteg) ** 0.5))) + params.elvis
+        ta32 = F32(Ta64.item())
+        S["ta32"] = ta32
+        S["ta4"] = F32(((Ta64 + 273.15) ** 4).item())
+        S["sbc"] = F32(SBC)
+        S["albedo_b"] = F32(params.albedo_b)
+        S["first"], S["second"] = first_f, second_f
+        S["refl_k"] = F32((1 - ewall_t).item())
+        S["absK"], S["absL"], S["Fside"], S["Fup"], S["Fcyl"] = (F32(v) for v in (
+            params.absK, params.absL, params.Fside, params.Fup, params.Fcyl))
+        S["absl_sbc"] = F32((params.absL * sbc_t).item())
+        S["rh32"] = F32(RH_all[i])
+        S["ws32"] = F32(Ws_all[i])
+        S["ta_mat"] = (F32(0) + F32(Ta_all[i])) + F32(uhii_all[i])
+        S["landcover"] = props.landcover
+        S["utci_c"] = _utci_coeffs(S["ta_mat"], S["rh32"])
+        S["night_lup_base"] = ((F32(0) + ta32) + F32(0)) + F32(273.15)
+        Q = patch[o]
+        if alt64 > 0:
+            S["is_day"] = 1
+            S["day_row"] = len(sun_rows)
+            SNUP = _snup(torch.tensor(jd.item()), torch.tensor(lat))
+            I0, CI, Kt = _clearness(torch.tensor(zen64.item()), torch.tensor(jd.item()), Ta64.item(),
+                                    torch.tensor(RH64.item()) / 100., torch.tensor(radG64.item()), lat,
+                                    torch.tensor(met_file[i, 12].item()))
+            CI = min(CI, 1.0)
+            radI, radD = _diffuse(torch.tensor(radG64.item()), torch.tensor(alt64.item()), Kt,
+                                  torch.tensor(Ta64.item()), torch.tensor(RH64.item()))
+            lv = _perez((zen64 * (180 / np.pi)).item(), azi64.item(), radD, radI, jd.item())
+            # sun march table and wall-face bounds
+            dx, dy, dz, az_f = T.sun_table(azi64.item(), alt64.item(), scale, float(amax), rows, cols)
+            t = np.zeros(len(dz), N.STEP_DTYPE)
+            t["dx"], t["dy"], t["dz"] = dx, dy, dz
+            tables.append(t)
+            srow = np.zeros(1, N.SUN_STEP_DTYPE)[0]
+            srow["step_offset"], srow["step_count"], srow["t"] = sun_off, len(dz), o
+            srow["facesh_mode"], srow["facesh_lo"], srow["facesh_hi"] = T.facesh_thresholds(az_f)
+            srow["psi_term"] = F32(1) - psi[i]
+            sun_rows.append(srow)
+            sun_off += len(dz)
+            # ground temperature wave (solweig.py:2101-2122)
+            dect = torch.tensor(dectime[i])
+            altmax64 = torch.tensor(altmax[0][i])
+            phase = (dect - torch.floor(dect)) - SNUP / 24
+            radI0, radD0 = _diffuse(I0, alt64.item(), 1., Ta64.item(), RH64.item())
+            corr = 0.1473 * torch.log(90 - (zen64 / np.pi * 180)) + 0.3454
+            CI_TgG = min((radG64 / (radI0 * (torch.sin(alt64 * (np.pi / 180))) + radD0)) + (1 - corr), 1.0)
+            S["cig"] = F32(float(CI_TgG))
+            S["altmax32"] = F32(altmax64.item())
+            if props.landcover:
+                tm = torch.from_numpy(np.asarray(tvals, F32))
+                # float64 phase / float32 class plane -> float32 (solweig.py:2103)
+                fac = torch.sin(((torch.tensor(F32(phase.item())) / (tm / 24 - SNUP / 24)) * np.pi) / 2)
+                tgk_w = torch.from_numpy(np.asarray(props.tgk_wall, F32))
+                tst_w = torch.from_numpy(np.asarray(props.tstart_wall, F32))
+                tmx_w = torch.from_numpy(np.asarray(props.tmaxlst_wall, F32))
+                tgwall = (tgk_w * altmax64 + tst_w) * torch.sin((phase / (tmx_w / 24 - SNUP / 24)) * np.pi / 2)
+            else:
+                fac = torch.tensor([float(F32(torch.sin((phase / (15. / 24 - SNUP / 24)) * np.pi / 2).item()))])
+                tgwall = (0.37 * altmax64 + -3.41) * torch.sin((phase / (15. / 24 - SNUP / 24)) * np.pi / 2)
+            S["tg_factor"][:len(tvals)] = fac.numpy().astype(F32)
+            tgwall = torch.maximum(tgwall, torch.tensor(0))
+            tgwall = tgwall * CI_TgG
+            lwall = sbc_t * ewall_t * (tgwall + Ta64 + 273.15) ** 4 - sbc_t * ewall_t * (Ta64 + 273.15) ** 4
+            S["lwall"] = F32(lwall.reshape(-1)[0].item())
+            # thermal lag weights (solweig.py:451-488), one timeadd for all six planes
+            S["tw_first"] = int(firstdaytime == 1)
+            if timeadd >= (59 / 1440):
+                w = torch.exp(-33.27 * torch.tensor(timeadd))
+                S["tw_mode"] = 1
+                timeadd = timestepdec if timestepdec > (59 / 1440) else 0
+            else:
+                timeadd = timeadd + timestepdec
+                w = torch.exp(-33.27 * torch.tensor(timeadd))
+                S["tw_mode"] = 0
+            S["tw_a"], S["tw_b"] = F32((1 - w).item()), F32(w.item())
+            firstdaytime = 0
+            # shortwave scalars
+            S["radI"], S["radD"], S["radG"] = F32(radI.item()), F32(radD.item()), F32(radG64.item())
+            S["sin_alt"] = F32(torch.sin(alt64 * (np.pi / 180)).item())
+            alt32 = torch.tensor(alt64.item())
+            S["cos_alt"] = F32(torch.cos(alt32 * torch.tensor(np.pi / 180.0)).item())
+            beta = torch.tensor(zen64.item(), dtype=torch.float32)
+            S["tan_beta"] = F32(torch.tan(beta).item())
+            S["qa"] = F32((torch.tan(beta) / 2).item())
+            # Kside per patch (solweig.py:683-724)
+            palt, pazi, plum = lv[:, 0], lv[:, 1], lv[:, 2]
+            ster = _steradians(palt)
+            radTot = torch.zeros(1)
+            for k in range(P):
+                radTot += (plum[k] * ster[k] * torch.sin(palt[k] * deg2rad_t))
+            lumChi = (plum * radD) / radTot
+            sun_k = ((params.albedo_b * (radI * torch.cos(alt32 * deg2rad_t)) + (radD * 0.5)) / torch.pi)
+            sh_k = ((params.albedo_b * radD * 0.5) / torch.pi)
+            cos_p = torch.cos(palt * deg2rad_t).numpy()
+            sin_p = torch.sin(palt * deg2rad_t).numpy()
+            ang = (torch.cos(palt * deg2rad_t) * torch.cos(torch.tensor(0.))).numpy()
+            ster_n = ster.numpy()
+            lum_n = lumChi.numpy()
+            lvz = plum.numpy()
+            for di in range(4):
+                Q["kside_d"][:, di] = ((diff_vals[di] * lum_n) * ang) * ster_n
+                Q["anilum"][:, di] = diff_vals[di] * lvz
+            Q["kref_veg"] = (F32(sh_k.item()) * ster_n) * cos_p
+            Q["kref_sun"] = (F32(sun_k.item()) * ster_n) * cos_p
+            Q["kref_sh"] = Q["kref_veg"]
+            yk = 2 * torch.cos(torch.abs(azi64.item() - pazi) * (torch.pi / 180.0)) * \
+                torch.tan(alt32 * (torch.pi / 180.0))
+            Q["yi_k"] = torch.where(yk > 0, 0.0, yk).numpy()
+            pz64 = pazi.double()
+            yl = 2 * torch.cos(torch.abs(azi64 - pz64) * (torch.pi / 180.0)) * torch.tan(alt64 * (torch.pi / 180.0))
+            Q["yi_l"] = torch.where(yl > 0, 0.0, yl).numpy().astype(F32)
+            azd = torch.abs(azi64 - pz64)
+            Q["flags"] = ((azd > 90) & (azd < 270)).numpy().astype(np.int32)
+            L_patches = lv
+            # sunlit wall surface of define_patch_characteristics (solweig.py:1596)
+            sun_surf = F32((((ewall_t * sbc_t) * ((Ta64 + tgwall + 273.15) ** 4)) /
+                            torch.tensor(np.pi)).reshape(-1)[0].item())
+        else:
+            S["is_day"] = 0
+            S["day_row"] = -1
+            S["tg_factor"][:] = 0
+            timeadd = 0
+            firstdaytime = 1
+            L_patches = night_patches
+            sun_surf = F32(0)
+        if CI < 0.95:
+            esky = CI * esky + (1 - CI) * 1.
+        # Lcyl per patch (solweig.py:1651-1760)
+        palt_l, pazi_l = L_patches[:, 0], L_patches[:, 1]
+        ld, ls, ster_l = _lsky(esky, palt_l, Ta64)
+        cos_l = torch.cos(palt_l * deg2rad_t)
+        sin_l = torch.sin(palt_l * deg2rad_t)
+        Q["ld_sky"] = ld.numpy()
+        Q["ls_sky"] = ls.numpy()
+        Q["ster"] = ster_l.numpy()
+        Q["cos_alt"] = cos_l.numpy()
+        Q["sin_alt"] = sin_l.numpy()
+        surf = ((ewall_t * sbc_t * ((Ta64 + 273.15) ** 4)) / torch.tensor(np.pi))  # float64
+        s64 = ster_l.double()
+        Q["veg_cos"] = ((surf * s64) * cos_l.double()).numpy()
+        Q["veg_sin"] = ((surf * s64) * sin_l.double()).numpy()
+        Q["sh_cos"] = Q["veg_cos"]
+        Q["sh_sin"] = Q["veg_sin"]
+        Q["sun_cos"] = (sun_surf * ster_l.numpy()) * cos_l.numpy()
+        Q["sun_sin"] = (sun_surf * ster_l.numpy()) * sin_l.numpy()
+        for k, pa in enumerate(palt_l.numpy()):
+            Q["thr_sun"][k], Q["thr_shd"][k] = T.atan_degree_bounds(float(pa))
+    sun = np.array(sun_rows, N.SUN_STEP_DTYPE) if sun_rows else np.zeros(0, N.SUN_STEP_DTYPE)
+    table = np.concatenate(tables) if tables else np.zeros(0, N.STEP_DTYPE)
+    final = {"CI": float(CI), "firstdaytime": float(firstdaytime), "timeadd": float(timeadd)}
+    return Series(steps, sun, table, patch, T.gvf_table(int(second_f)), final, class_idx)

@@ -1,0 +1,344 @@
+"""Throughput of the exact SOLWEIG chain (SVF sweep + sun march + fluxes +
+Tmrt + UTCI) on B200, in pixel x timesteps per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload exact500|tile4096]
+
+One step = one pass of the whole chain over one site: the 153-patch SVF sweep
+and the 24 hourly steps of the time loop (sun march of the daytime steps,
+ground view factors, K/L fluxes, Tmrt, UTCI).  Inputs are the seeded
+synthetic city of the workload (500 x 500 px at 1 m by default).
+
+* ``value``: device throughput with the rasters and tables resident in HBM
+  (CUDA events on the launching stream, L2 flushed before every timed step).
+* ``e2e``: the same metric through the public entry point
+  (:func:`solweig_project_b200.api.run_exact_chain` from host rasters in
+  pinned memory), host->device inputs and device->host UTCI/Tmrt included.
+* With torchrun (N > 1) every rank runs its own site (weak scaling, no
+  collective on the data path); the time is the max over ranks.
+* ``--impl reference`` times the CPU oracle (the reference's algorithm
+  restated on the host cores) on a bounded crop of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+METRIC = "px*steps/s shadow->Tmrt->UTCI (exact chain incl. SVF sweep)"
+UNIT = "px*steps/s"
+N_STEPS_DAY = 24
+WORKLOADS = {
+    # name: (side, h_max, description)
+    "exact500": (500, 40.0, "500x500 px @1 m, 24 hourly steps, SVF sweep + shadows + fluxes + Tmrt + UTCI"),
+    "tile4096": (4096, 120.0, "4096x4096 px @1 m, buildings up to 120 m, 24 hourly steps, full exact chain"),
+}
+FLUX_BYTES_PER_PX_STEP = 190      # compulsory HBM bytes per pixel and step of the flux stage
+SVF_GATHER_BYTES_PER_STEP = 12    # 3 float32 gathers per march step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="exact500")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name, rank):
+    from solweig_project_b200 import synthetic
+    side, hmax, _ = WORKLOADS[name]
+    city = synthetic.make_city(side, side, seed=1234 + rank, h_max=hmax)
+    met = synthetic.make_met(1234)
+    geo = synthetic.load_sun_geometry("single")
+    return city, met, geo, synthetic.default_lc_class()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("clocks.sm", "clocks.max.sm", "clocks_event_reasons.active", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        try:
+            rows = [[c.strip() for c in line.split(",")] for line in open(self.path) if line.strip()]
+        except OSError:
+            rows = []
+        sm = [float(r[0]) for r in rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def cpu_baseline(city, met, geo, lc_class, crop=64):
+    """The CPU oracle on a bounded crop (crop x crop px, all 24 steps, SVF
+    sweep included), single thread."""
+    import torch
+    torch.set_num_threads(1)
+    from oracle import svf as osvf, window as ow
+    sl = (slice(0, crop), slice(0, crop))
+    dsm, trees, dem = city.dsm[sl], city.trees[sl], city.dem[sl]
+    t0 = time.perf_counter()
+    vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(dsm, trees, dem)
+    bundle = osvf.svf_calculator(2, amax, dsm, vegdsm, vegdsm2, bush, city.scale)
+    ow.run_utci_window(a=dsm, temp1=trees, temp2=dem, walls=city.walls[sl], dirwalls=city.aspect[sl],
+                       svf_bundle=bundle, met_file=met, location={"latitude": 30.3, "longitude": -97.7,
+                                                                  "altitude": 3.0}, scale=city.scale,
+                       landcover_grid=city.landcover[sl], lc_class=lc_class, requested_variables=("utci", "tmrt"),
+                       **geo)
+    dt = time.perf_counter() - t0
+    return {"value": crop * crop * N_STEPS_DAY / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{crop}x{crop} px crop of the workload, 24 steps, SVF sweep included, {dt:.2f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU oracle with all host threads on a bounded crop."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    from oracle import svf as osvf, window as ow
+    city, met, geo, lc_class = make_workload(args.workload, 0)
+    crop = 96
+    sl = (slice(0, crop), slice(0, crop))
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        dsm, trees, dem = city.dsm[sl], city.trees[sl], city.dem[sl]
+        vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(dsm, trees, dem)
+        bundle = osvf.svf_calculator(2, amax, dsm, vegdsm, vegdsm2, bush, city.scale)
+        ow.run_utci_window(a=dsm, temp1=trees, temp2=dem, walls=city.walls[sl], dirwalls=city.aspect[sl],
+                           svf_bundle=bundle, met_file=met,
+                           location={"latitude": 30.3, "longitude": -97.7, "altitude": 3.0}, scale=city.scale,
+                           landcover_grid=city.landcover[sl], lc_class=lc_class,
+                           requested_variables=("utci", "tmrt"), **geo)
+        if it >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    value = crop * crop * N_STEPS_DAY / t
+    side = WORKLOADS[args.workload][0]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded city, 24 h forcing)",
+        "config": {"workload": args.workload, "rows": side, "cols": side, "timesteps": N_STEPS_DAY,
+                   "sample": f"{crop}x{crop} px crop"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{crop}x{crop} px crop of the {side}x{side} workload, 24 steps, SVF included, "
+                                   f"CPU oracle with {cores} torch threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from solweig_project_b200 import _native as N
+    from solweig_project_b200 import api, build
+    from solweig_project_b200.engine import DeviceSite
+    build.build()
+    city, met, geo, lc_class = make_workload(args.workload, rank)
+    rows, cols = city.shape
+    npix = rows * cols
+    loc = {"latitude": 30.3, "longitude": -97.7, "altitude": 3.0}
+
+    site = DeviceSite(city.dsm, city.trees, city.dem, city.walls, city.aspect, city.scale,
+                      landcover=city.landcover, lc_class=lc_class)
+    res = site.run_svf()
+    ser = site.build_series(met, geo["altitude"], geo["azimuth"], geo["zen"], geo["jday"], geo["dectime"],
+                            geo["altmax"], loc)
+    series, series_dev = site.upload_series(ser)
+    n_day = series.n_day
+    dev = site.device
+    planes, bits = res.planes, res.bits
+    gsrc = torch.empty((max(1, n_day), rows, cols, 4), dtype=torch.float32, device=dev)
+    outputs = torch.empty((2, N_STEPS_DAY, rows, cols), dtype=torch.float32, device=dev)
+    mask = N.OUT_UTCI | N.OUT_TMRT
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        site.launch_svf(planes, bits)
+        if ev is not None:
+            ev[1].record(stream)
+        site.launch_sun_march(series, gsrc)
+        if ev is not None:
+            ev[2].record(stream)
+        site.state.zero_()
+        site.launch_flux_loop(series, gsrc, mask, outputs)
+        if ev is not None:
+            ev[3].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    launches0 = N.launch_count()
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(float(k))          # evict L2 between timed steps (not timed)
+            step(events[k])
+        torch.cuda.synchronize()
+    launches = N.launch_count() - launches0
+    svf_ms = [e[0].elapsed_time(e[1]) for e in events]
+    march_ms = [e[1].elapsed_time(e[2]) for e in events]
+    loop_ms = [e[2].elapsed_time(e[3]) for e in events]
+    step_ms = sum(e[0].elapsed_time(e[3]) for e in events) / args.steps
+    t_max = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    step_ms = float(t_max.item())
+    value = world * npix * N_STEPS_DAY / (step_ms / 1e3)
+
+    # ---------------------------------------------------------------- e2e
+    e2e = None
+    if not args.no_e2e:
+        pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in (
+            ("dsm", city.dsm), ("trees", city.trees), ("dem", city.dem), ("walls", city.walls),
+            ("aspect", city.aspect), ("landcover", city.landcover))}
+        from solweig_project_b200 import engine as E
+        e2e_times = []
+        moved = []
+        for it in range(2 + max(1, min(args.steps, 3))):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            E.TRANSFER.update(h2d=0, d2h=0)
+            e0.record(stream)
+            out = api.run_exact_chain(dsm=pinned["dsm"].numpy(), trees=pinned["trees"].numpy(),
+                                      dem=pinned["dem"].numpy(), walls=pinned["walls"].numpy(),
+                                      aspect=pinned["aspect"].numpy(), scale=city.scale, met_file=met,
+                                      location=loc, landcover=pinned["landcover"].numpy(), lc_class=lc_class,
+                                      requested=("utci", "tmrt"), **geo)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if it >= 2:
+                e2e_times.append(e0.elapsed_time(e1))
+                moved.append(dict(E.TRANSFER))
+        h2d, d2h = moved[-1]["h2d"], moved[-1]["d2h"]
+        e2e_ms = torch.tensor([sum(e2e_times) / len(e2e_times)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * npix * N_STEPS_DAY / (float(e2e_ms.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": float(e2e_ms.item())}
+
+    if rank == 0:
+        svf_steps = int(site.svf_tables(2)[2])
+        loop_t = sum(loop_ms) / len(loop_ms)
+        svf_t = sum(svf_ms) / len(svf_ms)
+        march_t = sum(march_ms) / len(march_ms)
+        from solweig_project_b200.synthetic import DEFAULT_LOCATION  # noqa: F401
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        stages = {
+            "svf_sweep": {"ms": svf_t, "gbs_gather": SVF_GATHER_BYTES_PER_STEP * svf_steps * npix / (svf_t * 1e6)},
+            "sun_march": {"ms": march_t},
+            "flux_loop": {"ms": loop_t,
+                          "gbs_compulsory": FLUX_BYTES_PER_PX_STEP * npix * N_STEPS_DAY / (loop_t * 1e6)},
+        }
+        dom = max(stages, key=lambda k: stages[k]["ms"])
+        if dom == "svf_sweep":
+            achieved = stages[dom]["gbs_gather"]
+            roof_note = "march gather bytes (12 B x executed steps per pixel) / launch time"
+        elif dom == "flux_loop":
+            achieved = stages[dom]["gbs_compulsory"]
+            roof_note = "compulsory 190 B per pixel-step / launch time"
+        else:
+            achieved = None
+            roof_note = ""
+        clk = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded city + 24 h forcing, random geometry)",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][2], "rows": rows,
+                       "cols": cols, "timesteps": N_STEPS_DAY, "daytime_steps": int(n_day),
+                       "svf_march_steps_per_px": svf_steps, "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": f"site-per-rank x{world}"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback",
+                         "definition": roof_note},
+            "stages": stages,
+            "gpu_launches": int(launches),
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        }
+        if e2e is not None:
+            line["e2e"] = e2e
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(city, met, geo, lc_class)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -55,7 +55,7 @@ extern "C" {
 #define SW100_MAX_CLASSES 8     /* land-cover property classes */
 #define SW100_N_GVF_AZ 18       /* ground view factor search azimuths */
 #define SW100_MAX_GVF_STEPS 64  /* bound on the `second` walk length */
-#define SW100_SVF_PLANES 16     /* 15 SVF planes + SVFtotal */
+#define SW100_SVF_PLANES 19     /* 15 SVF planes, SVFtotal, 3 time-loop statics */
 
 /* status codes beyond CUDA's */
 #define SW100_E_ARG 1001         /* invalid argument */
@@ -115,17 +115,31 @@ typedef struct {
   float w_aniso[SW100_MAX_RINGS][SW100_MAX_ANNULI];
   float tail;                                 /* 3.0459e-4 (shadow.py:587) */
   float trans;                                /* 0.03 (shadow.py:612) */
+  float trans_veg;                            /* transVeg of the time loop (utci_process.py:864) */
 } sw100_svf_plan;
 
-/* out_planes: SW100_SVF_PLANES * npix floats in the reference's 19-tuple
- * order without the cubes, then SVFtotal: svf, svfaveg, svfE, svfEaveg,
+/* out_planes: SW100_SVF_PLANES * npix floats: the reference's 19-tuple
+ * order without the cubes, then SVFtotal (svf, svfaveg, svfE, svfEaveg,
  * svfEveg, svfN, svfNaveg, svfNveg, svfS, svfSaveg, svfSveg, svfveg, svfW,
- * svfWaveg, svfWveg, svftotal.  out_bits: 3 cubes (sh, vegsh, vbshvegsh).
- * plan and steps are device copies of the host tables. */
+ * svfWaveg, svfWveg, svftotal), then three per-pixel statics of the time
+ * loop derived from them: svfbuveg = svf - (1 - svfveg) * (1 - transVeg),
+ * tan(acos(sqrt(svf))) and tan(asin(exp(log(1 - tmp) / 2))) with
+ * tmp = max(svf + svfveg - 1, 0) (utci_process.py:864-897), each
+ * transcendental rounded to float32 once per reference operation.
+ * out_bits: 3 cubes (sh, vegsh, vbshvegsh).  plan and steps are device
+ * copies of the host tables. */
 int sw100_svf_workspace_bytes(int rows, int cols, int n_steps, int64_t* bytes);
 int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
                     const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
                     void* workspace, int64_t workspace_bytes, void* stream);
+
+/* Pack dense patch cubes (rows, cols, n_patches) float32, as the reference
+ * returns and caches them (shadow.py:625, utci_process.py:347-394), into the
+ * 3 bit cubes the time loop reads.  `single_step` (host, SW100_CUBE_WORDS
+ * words) marks patches whose SVF march ran at most one step: their
+ * vbshvegsh bit records "== 1", every other bit "!= 0". */
+int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbshvegshmat, int rows, int cols,
+                     int n_patches, const uint32_t* single_step, uint32_t* out_bits, void* stream);
 
 /* ------------------------------------------------------ time series -- */
 typedef struct {
@@ -253,6 +267,13 @@ int sw100_time_loop_workspace_bytes(int rows, int cols, int n_day, int64_t* byte
 int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
                     float* state, uint32_t out_mask, float* outputs, void* workspace,
                     int64_t workspace_bytes, void* stream);
+
+/* The fused loop kernel of sw100_time_loop alone, reading sun-march records
+ * from a previous sw100_sun_march call on the same series (gsrc as written
+ * there, n_day * npix * 4 floats).  Lets a caller time or overlap the two
+ * launches separately; no workspace. */
+int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
+                    const float* gsrc, float* state, uint32_t out_mask, float* outputs, void* stream);
 
 /* ---------------------------------------------------------------- UTCI -- */
 /* utci_calculator over n float32 elements: saturation vapour pressure from

@@ -22,15 +22,15 @@ MAX_ANNULI = 16
 MAX_CLASSES = 8
 N_GVF_AZ = 18
 MAX_GVF_STEPS = 64
-SVF_PLANES = 16
+SVF_PLANES = 19
 
 OUT_UTCI, OUT_TMRT, OUT_KUP, OUT_KDOWN, OUT_LUP, OUT_LDOWN, OUT_SHADOW = (1 << i for i in range(7))
 OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDOWN, "lup": OUT_LUP,
             "ldown": OUT_LDOWN, "shadow": OUT_SHADOW}
 
 # Exported symbols (checked by the CPU tests against include/solweig_b200.h)
-SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_sun_march_workspace_bytes",
-           "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop", "sw100_utci",
+SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_pack_cubes", "sw100_sun_march_workspace_bytes",
+           "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop", "sw100_flux_loop", "sw100_utci",
            "sw100_abi_version", "sw100_last_error", "sw100_launch_count")
 
 
@@ -56,7 +56,7 @@ SVF_PLAN_DTYPE = np.dtype([
     ("ring", "<i4", (MAX_PATCHES,)), ("dir_flags", "<i4", (MAX_PATCHES,)),
     ("ring_annuli", "<i4", (MAX_RINGS,)),
     ("w_iso", "<f4", (MAX_RINGS, MAX_ANNULI)), ("w_aniso", "<f4", (MAX_RINGS, MAX_ANNULI)),
-    ("tail", "<f4"), ("trans", "<f4"),
+    ("tail", "<f4"), ("trans", "<f4"), ("trans_veg", "<f4"),
 ], align=True)
 
 SUN_STEP_DTYPE = np.dtype([
@@ -88,7 +88,7 @@ TIME_STEP_DTYPE = np.dtype([
     ("tg_factor", "<f4", (MAX_CLASSES,)), ("pad1", "<i4"), ("utci_c", "<f8", (49,)),
 ], align=True)
 
-EXPECTED_SIZES = {"sw100_step": 16, "sw100_svf_plan": 4696, "sw100_sun_step": 32,
+EXPECTED_SIZES = {"sw100_step": 16, "sw100_svf_plan": 4700, "sw100_sun_step": 32,
                   "sw100_gvf_azimuth": 144, "sw100_patch_step": 128, "sw100_time_step": 568}
 DTYPES = {"sw100_step": STEP_DTYPE, "sw100_svf_plan": SVF_PLAN_DTYPE, "sw100_sun_step": SUN_STEP_DTYPE,
           "sw100_gvf_azimuth": GVF_AZ_DTYPE, "sw100_patch_step": PATCH_STEP_DTYPE,
@@ -138,12 +138,15 @@ def load(path: str = LIB_PATH):
         "sw100_svf_workspace_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, i64p]),
         "sw100_svf_sweep": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp,
                                       C.c_int64, vp]),
+        "sw100_pack_cubes": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32), vp, vp]),
         "sw100_sun_march_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
         "sw100_sun_march": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, vp,
                                       C.c_int64, vp]),
         "sw100_time_loop_workspace_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, i64p]),
         "sw100_time_loop": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, C.c_uint32,
                                       vp, vp, C.c_int64, vp]),
+        "sw100_flux_loop": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, C.c_uint32,
+                                      vp, vp]),
         "sw100_utci": (C.c_int, [vp, vp, vp, vp, C.c_int64, vp, vp]),
     }
     for name, (res, args) in sig.items():

@@ -28,6 +28,8 @@ __global__ void time_loop_kernel(SitePlanes site, int rows, int cols, const sw10
                                  const sw100_patch_step* patch_steps, int n_patches,
                                  const sw100_gvf_azimuth* gvf_az, const float4* gsrc, float* state,
                                  uint32_t out_mask, float* outputs);
+__global__ void pack_cubes_kernel(const float* sh, const float* veg, const float* vb, size_t npix, int n_patches,
+                                  Single5 single, uint32_t* bits);
 __global__ void utci_kernel(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n,
                             float* out);
 }  // namespace sw100
@@ -185,6 +187,25 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
   return check_launch("svf_sweep_kernel");
 }
 
+int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbshvegshmat, int rows, int cols,
+                     int n_patches, const uint32_t* single_step, uint32_t* out_bits, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(shmat, "shmat")) || (rc = check_ptr(vegshmat, "vegshmat")) ||
+      (rc = check_ptr(vbshvegshmat, "vbshvegshmat")) || (rc = check_ptr(out_bits, "out_bits")))
+    return rc;
+  if (n_patches <= 0 || n_patches > 32 * SW100_CUBE_WORDS) return fail(SW100_E_SIZE, "n_patches out of range");
+  Single5 single = {};
+  if (single_step)
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) single.w[w] = single_step[w];
+  const size_t n = (size_t)rows * cols;
+  const int threads = 256;
+  const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 16);
+  pack_cubes_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(shmat, vegshmat, vbshvegshmat, n,
+                                                                                n_patches, single, out_bits);
+  return check_launch("pack_cubes_kernel");
+}
+
 int sw100_sun_march_workspace_bytes(int rows, int cols, int64_t* bytes) {
   int rc;
   if ((rc = check_grid(rows, cols))) return rc;
@@ -241,6 +262,24 @@ int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw1
   dim3 grid((cols + 31) / 32, (rows + 3) / 4);
   time_loop_kernel<<<grid, block, 0, st>>>(make_site(*site), rows, cols, series->steps, series->n_t, series->patch,
                                            series->n_patches, series->gvf, gsrc, state, out_mask, outputs);
+  return check_launch("time_loop_kernel");
+}
+
+int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw100_series* series, const float* gsrc,
+                    float* state, uint32_t out_mask, float* outputs, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_loop(site))) return rc;
+  if ((rc = validate_series(series))) return rc;
+  if ((rc = check_ptr(state, "state"))) return rc;
+  if (series->n_day > 0 && (rc = check_ptr(gsrc, "gsrc"))) return rc;
+  if (out_mask & ~0x7Fu) return fail(SW100_E_ARG, "unknown output bits 0x%x", out_mask);
+  if (out_mask && !outputs) return fail(SW100_E_ARG, "outputs must not be NULL");
+  dim3 block(32, 4);
+  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  time_loop_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
+      make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
+      reinterpret_cast<const float4*>(gsrc), state, out_mask, outputs);
   return check_launch("time_loop_kernel");
 }
 

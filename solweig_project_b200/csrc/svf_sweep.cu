@@ -13,6 +13,8 @@
 // (patch-major, annulus-minor), so the sums are bit-identical; the three
 // patch masks are packed into 5-word bit cubes per pixel (60 B/px instead of
 // the reference's 1836 B/px of float cubes).
+#include <cmath>
+
 #include "sw_common.cuh"
 
 namespace sw100 {
@@ -174,7 +176,19 @@ __global__ void __launch_bounds__(128) svf_sweep_kernel(
   const float vals[SW100_SVF_PLANES] = {A.svf,  A.aveg,  A.svfE, A.avegE, A.vegE, A.svfN, A.avegN, A.vegN,
                                         A.svfS, A.avegS, A.vegS, A.veg,   A.svfW, A.avegW, A.vegW, total};
 #pragma unroll
-  for (int k = 0; k < SW100_SVF_PLANES; ++k) out[k * npix + p] = vals[k];
+  for (int k = 0; k < 16; ++k) out[k * npix + p] = vals[k];
+  // time-loop statics (utci_process.py:864-897): every float32 operation of
+  // the reference rounded once; transcendentals evaluated in double
+  out[16 * npix + p] = A.svf - (1.f - A.veg) * (1.f - plan.trans_veg);
+  const float s = (float)sqrt((double)A.svf);
+  const float asvf = (float)acos((double)s);
+  out[17 * npix + p] = (float)tan((double)asvf);
+  float tmp = A.svf + A.veg - 1.f;
+  if (tmp < 0.f) tmp = 0.f;
+  const float lg = (float)log((double)(1.f - tmp));
+  const float ex = (float)exp((double)(lg / 2.f));
+  const float alfa = (float)asin((double)ex);
+  out[18 * npix + p] = (float)tan((double)alfa);
 #pragma unroll
   for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
     bits[(0 * SW100_CUBE_WORDS + w) * npix + p] = wsh[w];
@@ -203,6 +217,30 @@ __global__ void svf_bush_flags_kernel(const float4* __restrict__ src4, int rows,
       float tv = 0.f;
       if (in_grid(sr, sc, rows, cols)) tv = __fsub_rn(src4[(size_t)sr * cols + sc].y, st.dz);
       if (tv > a && flags[off + k] == 0u) atomicExch(&flags[off + k], 1u);
+    }
+  }
+}
+
+// Dense (rows, cols, P) float cubes -> word-planar bit cubes.
+__global__ void pack_cubes_kernel(const float* __restrict__ sh, const float* __restrict__ veg,
+                                  const float* __restrict__ vb, size_t npix, int n_patches, Single5 single,
+                                  uint32_t* __restrict__ bits) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npix; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t w0[SW100_CUBE_WORDS] = {}, w1[SW100_CUBE_WORDS] = {}, w2[SW100_CUBE_WORDS] = {};
+    const float* a = sh + i * n_patches;
+    const float* b = veg + i * n_patches;
+    const float* c = vb + i * n_patches;
+    for (int q = 0; q < n_patches; ++q) {
+      const uint32_t bit = 1u << (q & 31);
+      const bool one_step = single.w[q >> 5] & bit;
+      if (a[q] != 0.f) w0[q >> 5] |= bit;
+      if (b[q] != 0.f) w1[q >> 5] |= bit;
+      if (one_step ? (c[q] == 1.f) : (c[q] != 0.f)) w2[q >> 5] |= bit;
+    }
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+      bits[(0 * SW100_CUBE_WORDS + w) * npix + i] = w0[w];
+      bits[(1 * SW100_CUBE_WORDS + w) * npix + i] = w1[w];
+      bits[(2 * SW100_CUBE_WORDS + w) * npix + i] = w2[w];
     }
   }
 }

@@ -36,6 +36,10 @@ __device__ __forceinline__ float pow4f(float x) {
 // plane into a float32 plane: add in double, round once.
 __device__ __forceinline__ float add64(float acc, double term) { return (float)((double)acc + term); }
 
+struct Single5 {
+  uint32_t w[SW100_CUBE_WORDS];
+};
+
 // Read-only cached load of one march step (16 bytes).
 __device__ __forceinline__ sw100_step load_step(const sw100_step* p) {
   const int4 v = __ldg(reinterpret_cast<const int4*>(p));

@@ -26,7 +26,7 @@ from . import timeseries as TS
 
 F32 = np.float32
 SVF_NAMES = ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg", "svfNveg", "svfS", "svfSaveg",
-             "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg", "svftotal")
+             "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg", "svftotal", "svfbuveg", "hsvf", "tan_alfa")
 STATE_NAMES = ("Tgmap1", "Tgmap1E", "Tgmap1S", "Tgmap1W", "Tgmap1N", "TgOut1")
 
 
@@ -36,8 +36,18 @@ def require_cuda():
     N.load()
 
 
+# host <-> device bytes moved by this module (inputs, tables, results)
+TRANSFER = {"h2d": 0, "d2h": 0}
+
+
+def _upload(host: torch.Tensor, device) -> torch.Tensor:
+    """Host tensor -> device through a pinned staging buffer."""
+    TRANSFER["h2d"] += host.numel() * host.element_size()
+    return host.pin_memory().to(device, non_blocking=True)
+
+
 def _dev(x, device, dtype=torch.float32):
-    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).to(device, non_blocking=True)
+    return _upload(torch.as_tensor(np.ascontiguousarray(x), dtype=dtype), device)
 
 
 def _table(arr: np.ndarray, device) -> torch.Tensor:
@@ -45,7 +55,12 @@ def _table(arr: np.ndarray, device) -> torch.Tensor:
     raw = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
     if raw.size == 0:
         raw = np.zeros(16, np.uint8)
-    return torch.from_numpy(raw.copy()).to(device, non_blocking=True)
+    return _upload(torch.from_numpy(raw.copy()), device)
+
+
+def to_host(t: torch.Tensor) -> np.ndarray:
+    TRANSFER["d2h"] += t.numel() * t.element_size()
+    return t.cpu().numpy()
 
 
 def _ptr(t):
@@ -79,7 +94,7 @@ def march_inputs(dsm, trees, dem):
 
 @dataclass
 class SvfResult:
-    planes: torch.Tensor      # (16, rows, cols) float32, SVF_NAMES order
+    planes: torch.Tensor      # (19, rows, cols) float32, SVF_NAMES order
     bits: torch.Tensor        # (3, 5, rows, cols) int32 words (sh, vegsh, vbshvegsh)
     single_step: np.ndarray   # uint32[5] patches with <= 1 march step
 
@@ -134,6 +149,34 @@ class DeviceSite:
         self.svf_result: SvfResult | None = None
         self.state = torch.zeros((6, self.rows, self.cols), dtype=torch.float32, device=d)
         self._keep = []
+        self._cache = {}
+
+    @classmethod
+    def from_march_rasters(cls, a, vegdsm, vegdsm2, bush, amaxvalue, scale, device="cuda"):
+        """A site that only runs the SVF sweep, from the march rasters the
+        reference's svf_calculator takes (DSM, canopy top, trunk top, bush)."""
+        require_cuda()
+        self = cls.__new__(cls)
+        self.device = torch.device(device)
+        self.params = TS.ModelParams()
+        a = np.asarray(a, F32)
+        self.rows, self.cols = a.shape
+        vegdsm = np.asarray(vegdsm, F32)
+        vegdsm2 = np.asarray(vegdsm2, F32)
+        bush = np.asarray(bush, F32)
+        self.amax = F32(amaxvalue)
+        self.bush_any = bool(bush.max() > 0)
+        self.vmax = F32(max(a.max(), vegdsm.max(), vegdsm2.max()))
+        self.scale = float(scale)
+        d = self.device
+        self.t = {"dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
+                  "bush": _dev(bush, d) if self.bush_any else None}
+        self.props = None
+        self.svf_result = None
+        self.state = None
+        self._keep = []
+        self._cache = {}
+        return self
 
     # --------------------------------------------------------------- SVF
     def site_struct(self) -> N.SitePlanes:
@@ -152,46 +195,63 @@ class DeviceSite:
                 s.single_step[w] = int(self.svf_result.single_step[w])
         return s
 
-    def run_svf(self, patch_option=2) -> SvfResult:
-        plan, steps, single = T.svf_plan(self.rows, self.cols, self.scale, self.amax, self.bush_any, patch_option)
+    def svf_tables(self, patch_option=2):
+        """Plan and step tables of the SVF sweep, built and uploaded once."""
+        key = ("svf", patch_option)
+        if key not in self._cache:
+            plan, steps, single = T.svf_plan(self.rows, self.cols, self.scale, self.amax, self.bush_any,
+                                             patch_option, trans_veg=self.params.transVeg)
+            d = self.device
+            ws_bytes = N.workspace_bytes("sw100_svf_workspace_bytes", self.rows, self.cols, len(steps))
+            self._cache[key] = (_table(plan, d), _table(steps, d), len(steps), single,
+                                torch.empty(ws_bytes, dtype=torch.uint8, device=d))
+        return self._cache[key]
+
+    def launch_svf(self, planes, bits, patch_option=2):
+        """The sweep alone into caller buffers (no host work once the tables
+        are cached)."""
+        plan_d, steps_d, n_steps, _, ws = self.svf_tables(patch_option)
+        site = self.site_struct()
+        N.call("sw100_svf_sweep", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), n_steps,
+               _ptr(planes), _ptr(bits), _ptr(ws), ws.numel(), _stream())
+
+    def run_svf(self, patch_option=2, exact_statics=False) -> SvfResult:
         d = self.device
-        plan_d, steps_d = _table(plan, d), _table(steps, d)
         planes = torch.empty((N.SVF_PLANES, self.rows, self.cols), dtype=torch.float32, device=d)
         bits = torch.empty((3, N.CUBE_WORDS, self.rows, self.cols), dtype=torch.int32, device=d)
-        ws_bytes = N.workspace_bytes("sw100_svf_workspace_bytes", self.rows, self.cols, len(steps))
-        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=d)
-        site = self.site_struct()
-        N.call("sw100_svf_sweep", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), len(steps),
-               _ptr(planes), _ptr(bits), _ptr(ws), ws_bytes, _stream())
-        self._keep = [plan_d, steps_d, ws]
-        self.svf_result = SvfResult(planes, bits, single)
-        self._prepare_loop_statics()
+        self.launch_svf(planes, bits, patch_option)
+        self.svf_result = SvfResult(planes, bits, self.svf_tables(patch_option)[3])
+        self._prepare_loop_statics(exact_statics)
         return self.svf_result
 
-    def set_svf(self, planes16, bits, single_step):
-        """Install an SVF result computed earlier (cached bundle)."""
-        self.svf_result = SvfResult(planes16, bits, np.asarray(single_step, np.uint32))
-        self._prepare_loop_statics()
+    def set_svf(self, planes, bits, single_step, exact_statics=False):
+        """Install an SVF result computed earlier (a cached bundle)."""
+        self.svf_result = SvfResult(planes, bits, np.asarray(single_step, np.uint32))
+        self._prepare_loop_statics(exact_statics)
 
-    def _prepare_loop_statics(self):
+    def _prepare_loop_statics(self, exact=False):
         """Per-pixel statics of the time loop derived from the SVF planes:
-        svfbuveg (utci_process.py:864), hsvf = tan(asvf) with asvf =
-        acos(sqrt(svf)) (utci_process.py:865, solweig.py:550) and
-        tan(svfalfa) (utci_process.py:892-897).  The two transcendental planes
-        are evaluated with torch's CPU kernels, the reference's rounding."""
-        svf = self.svf_result.plane("svf").detach().to("cpu")
-        svfveg = self.svf_result.plane("svfveg").detach().to("cpu")
-        tv = self.params.transVeg
-        svfbuveg = svf - (1.0 - svfveg) * (1.0 - tv)
+        svfbuveg (utci_process.py:864), tan(asvf) with asvf = acos(sqrt(svf))
+        (utci_process.py:865, solweig.py:550) and tan(svfalfa)
+        (utci_process.py:892-897).  The sweep kernel writes all three (each
+        transcendental rounded once from double); with ``exact`` the two
+        transcendental planes are re-evaluated by torch's CPU kernels, whose
+        rounding is the reference's own."""
+        r = self.svf_result
+        self.t["svfbuveg"] = r.plane("svfbuveg")
+        self.t["bits"] = r.bits
+        if not exact:
+            self.t["hsvf"] = r.plane("hsvf")
+            self.t["tan_alfa"] = r.plane("tan_alfa")
+            return
+        svf = r.plane("svf").detach().to("cpu")
+        svfveg = r.plane("svfveg").detach().to("cpu")
         hsvf = torch.tan(torch.acos(torch.sqrt(svf)))
         tmp = svf + svfveg - 1.0
         tmp[tmp < 0.0] = 0.0
         tan_alfa = torch.tan(torch.asin(torch.exp(torch.log(1.0 - tmp) / 2.0)))
-        d = self.device
-        self.t["svfbuveg"] = svfbuveg.to(d)
-        self.t["hsvf"] = hsvf.to(d)
-        self.t["tan_alfa"] = tan_alfa.to(d)
-        self.t["bits"] = self.svf_result.bits
+        self.t["hsvf"] = hsvf.to(self.device)
+        self.t["tan_alfa"] = tan_alfa.to(self.device)
 
     # ---------------------------------------------------------- time loop
     def build_series(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, time_start=0,
@@ -201,7 +261,7 @@ class DeviceSite:
                               amax=self.amax, rows=self.rows, cols=self.cols, props=self.props,
                               params=self.params, time_start=time_start, time_stop=time_stop,
                               initial_scalars=initial_scalars)
-        self.t["class_idx"] = torch.from_numpy(ser.class_idx).to(self.device)
+        self.t["class_idx"] = _upload(torch.from_numpy(ser.class_idx), self.device)
         return ser
 
     def upload_series(self, ser: TS.Series):
@@ -244,13 +304,24 @@ class DeviceSite:
         n_day = max(1, s.n_day)
         gsrc = torch.empty((n_day, self.rows, self.cols, 4), dtype=torch.float32, device=d)
         dbg = torch.empty((n_day, 8, self.rows, self.cols), dtype=torch.float32, device=d)
-        ws_bytes = N.workspace_bytes("sw100_sun_march_workspace_bytes", self.rows, self.cols)
-        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=d)
-        site = self.site_struct()
-        N.call("sw100_sun_march", C.byref(site), self.rows, self.cols, C.byref(s), _ptr(gsrc), _ptr(dbg), _ptr(ws),
-               ws_bytes, _stream())
-        self._keep = [dev, ws]
+        self.launch_sun_march(s, gsrc, dbg)
+        self._keep = [dev]
         return gsrc[:s.n_day], dbg[:s.n_day]
+
+    def launch_sun_march(self, series: N.Series, gsrc, debug8=None):
+        key = "sun_ws"
+        ws_bytes = N.workspace_bytes("sw100_sun_march_workspace_bytes", self.rows, self.cols)
+        if key not in self._cache:
+            self._cache[key] = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
+        ws = self._cache[key]
+        site = self.site_struct()
+        N.call("sw100_sun_march", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc), _ptr(debug8),
+               _ptr(ws), ws_bytes, _stream())
+
+    def launch_flux_loop(self, series: N.Series, gsrc, out_mask, outputs):
+        site = self.site_struct()
+        N.call("sw100_flux_loop", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc),
+               _ptr(self.state), out_mask, _ptr(outputs), _stream())
 
     def load_state(self, state: dict):
         for k, name in enumerate(STATE_NAMES):

@@ -175,3 +175,38 @@ def make_met(seed: int = 1234, year: int = DEFAULT_YEAR, doy: int = DEFAULT_DOY,
     met[:, 23] = -999.0
     met[:, 24] = uhii
     return met
+
+
+def multi_site_specs(n_sites: int = 64, seed: int = 2024):
+    """Seeded specs of the batched workload: square sides log-uniform in
+    [128, 1024] px, building density U(10, 45) %, canopy cover U(0, 30) %,
+    latitude U(0, 60) N (longitude -97.7, UTC-5)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_sites):
+        side = int(round(math.exp(rng.uniform(math.log(128), math.log(1024)))))
+        specs.append({"seed": int(seed * 1000 + i), "side": side, "density": float(rng.uniform(0.10, 0.45)),
+                      "canopy": float(rng.uniform(0.0, 0.30)), "latitude": float(rng.uniform(0.0, 60.0)),
+                      "longitude": DEFAULT_LOCATION["longitude"]})
+    return specs
+
+
+def default_lc_class() -> np.ndarray:
+    """Land-cover class table (code, albedo, emissivity, TgK, Tstart, TmaxLST)
+    as the reference loads landcoverclasses_2016a.txt (utci_process.py:1310-1316)."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "landcover_classes.json")
+    with open(path) as fh:
+        rows = json.load(fh)["classes"]
+    return np.array([r[1:] for r in rows], np.float64)
+
+
+def load_sun_geometry(prefix: str, path: str | None = None):
+    """Sun geometry arrays (float64, (1, 24)) recorded for a workload."""
+    import os
+    if path is None:
+        path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden",
+                            "sun_geometry.npz")
+    with np.load(path) as z:
+        return {k: z[f"{prefix}_{k}"] for k in ("altitude", "azimuth", "zen", "jday", "dectime", "altmax")}

@@ -213,7 +213,7 @@ def gvf_table(second: int) -> np.ndarray:
     return tab
 
 
-def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2):
+def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03):
     """SVF plan record + concatenated step table + single-step patch mask."""
     annulino, altint, _, nband = PATCH_LAYOUT[patch_option]
     azs = sweep_azimuths(patch_option)
@@ -228,6 +228,7 @@ def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2):
     plan["w_aniso"][0] = w_an
     plan["tail"] = F32(3.0459e-004)
     plan["trans"] = F32(0.03)
+    plan["trans_veg"] = F32(trans_veg)
     chunks = []
     off = 0
     single = np.zeros(N.CUBE_WORDS, np.uint32)

@@ -141,6 +141,35 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
 int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbshvegshmat, int rows, int cols,
                      int n_patches, const uint32_t* single_step, uint32_t* out_bits, void* stream);
 
+/* SVF sweep that allocates nothing and takes no workspace.
+ *
+ * This entry point has no counterpart in the reference.  It serves callers
+ * that cannot call cudaMalloc themselves: code embedded in a host framework
+ * that owns every device allocation through its own pool and forbids direct
+ * allocations, or latency-bound loops that cannot afford cudaMalloc /
+ * cudaFree (both may synchronise the device).  Such callers still pass
+ * their inputs and outputs; the scratch space of the sweep (the packed
+ * march source and the bush step flags) lives in a file-scope static
+ * device array of SW100_SVF_NOALLOC_SCRATCH_BYTES bytes, which every GPU
+ * that loads this library holds until the process exits.
+ *
+ * Limits: the grid must satisfy
+ *   align256(rows * cols * 16) + align256(n_steps * 4) <= SW100_SVF_NOALLOC_SCRATCH_BYTES
+ * (up to 1024 x 1024 pixels with 65536 table steps); larger requests are
+ * refused with SW100_E_SIZE before anything is launched.
+ *
+ * The first call on each device looks up the array's device address with
+ * that device current (cudaGetSymbolAddress) and caches it; make that first
+ * call before any stream capture on the device.  All calls share the one
+ * array, which keeps the last call's contents (the bush flags are cleared
+ * on every call): calls that overlap on the GPU, on different streams or
+ * from different threads, race on it and must be serialised by the
+ * caller.  Results are identical to sw100_svf_sweep. */
+#define SW100_SVF_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024 + 256 * 1024)
+int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                            const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
+                            void* stream);
+
 /* ------------------------------------------------------ time series -- */
 typedef struct {
   int32_t step_offset;     /* into the sun step table */

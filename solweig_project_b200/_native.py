@@ -23,13 +23,14 @@ MAX_CLASSES = 8
 N_GVF_AZ = 18
 MAX_GVF_STEPS = 64
 SVF_PLANES = 19
+SVF_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024 + 256 * 1024
 
 OUT_UTCI, OUT_TMRT, OUT_KUP, OUT_KDOWN, OUT_LUP, OUT_LDOWN, OUT_SHADOW = (1 << i for i in range(7))
 OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDOWN, "lup": OUT_LUP,
             "ldown": OUT_LDOWN, "shadow": OUT_SHADOW}
 
 # Exported symbols (checked by the CPU tests against include/solweig_b200.h)
-SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_pack_cubes", "sw100_sun_march_workspace_bytes",
+SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noalloc", "sw100_pack_cubes", "sw100_sun_march_workspace_bytes",
            "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop", "sw100_flux_loop", "sw100_utci",
            "sw100_abi_version", "sw100_last_error", "sw100_launch_count")
 
@@ -138,6 +139,8 @@ def load(path: str = LIB_PATH):
         "sw100_svf_workspace_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, i64p]),
         "sw100_svf_sweep": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp,
                                       C.c_int64, vp]),
+        "sw100_svf_sweep_noalloc": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp,
+                                              vp]),
         "sw100_pack_cubes": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32), vp, vp]),
         "sw100_sun_march_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
         "sw100_sun_march": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, vp,

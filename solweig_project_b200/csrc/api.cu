@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "sw_common.cuh"
@@ -298,3 +299,68 @@ int sw100_utci(const float* ta, const float* rh, const float* tmrt, const float*
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- allocation-free variant
+// Scratch of sw100_svf_sweep_noalloc: a file-scope device array, one per
+// device that loads the library.  Host code must not use its name as a
+// device address; the address is looked up per device below.
+namespace {
+__device__ __align__(256) unsigned char g_svf_noalloc_scratch[SW100_SVF_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 128;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up once
+// per device, with that device current).
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail((int)e, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return fail(SW100_E_ARG, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_svf_noalloc_scratch);
+    if (e != cudaSuccess) return fail((int)e, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+}  // namespace
+
+extern "C" int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                                       const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
+                                       void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_march(site))) return rc;
+  if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(out_planes, "out_planes")) ||
+      (rc = check_ptr(out_bits, "out_bits")))
+    return rc;
+  int64_t need = 0;
+  if ((rc = sw100_svf_workspace_bytes(rows, cols, n_steps, &need))) return rc;
+  if (need > (int64_t)SW100_SVF_NOALLOC_SCRATCH_BYTES)
+    return fail(SW100_E_SIZE,
+                "grid %d x %d with %d steps needs %lld scratch bytes; the allocation-free sweep has %lld "
+                "(at most 1024 x 1024 pixels)",
+                rows, cols, n_steps, (long long)need, (long long)SW100_SVF_NOALLOC_SCRATCH_BYTES);
+  void* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* src4 = static_cast<float4*>(scratch);
+  uint32_t* flags = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + align_up((int64_t)rows * cols * 16));
+  if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
+  dim3 block(32, 4);
+  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  if (site->bush_any) {
+    cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)n_steps * 4, st);
+    if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+    svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags);
+    if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
+  }
+  svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
+                                           site->vmax, out_planes, out_bits);
+  return check_launch("svf_sweep_kernel");
+}

@@ -55,14 +55,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="exact500")
+    ap.add_argument("--side", type=int, default=None, help="override the workload's square side (px)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
-def make_workload(name, rank):
+def make_workload(name, rank, side=None):
     from solweig_project_b200 import synthetic
-    side, hmax, _ = WORKLOADS[name]
+    side0, hmax, _ = WORKLOADS[name]
+    side = side or side0
     city = synthetic.make_city(side, side, seed=1234 + rank, h_max=hmax)
     met = synthetic.make_met(1234)
     geo = synthetic.load_sun_geometry("single")
@@ -143,7 +145,7 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     torch.set_num_threads(cores)
     from oracle import svf as osvf, window as ow
-    city, met, geo, lc_class = make_workload(args.workload, 0)
+    city, met, geo, lc_class = make_workload(args.workload, 0, args.side)
     crop = 96
     sl = (slice(0, crop), slice(0, crop))
     times = []
@@ -194,7 +196,7 @@ def main():
     from solweig_project_b200 import api, build
     from solweig_project_b200.engine import DeviceSite
     build.build()
-    city, met, geo, lc_class = make_workload(args.workload, rank)
+    city, met, geo, lc_class = make_workload(args.workload, rank, args.side)
     rows, cols = city.shape
     npix = rows * cols
     loc = {"latitude": 30.3, "longitude": -97.7, "altitude": 3.0}
@@ -318,7 +320,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded city + 24 h forcing, random geometry)",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][2], "rows": rows,
+            "config": {"workload": args.workload if args.side is None else f"{args.workload}@{rows}",
+                       "description": WORKLOADS[args.workload][2], "rows": rows,
                        "cols": cols, "timesteps": N_STEPS_DAY, "daytime_steps": int(n_day),
                        "svf_march_steps_per_px": svf_steps, "l2": "flushed (256 MiB write) before every timed step",
                        "parallelism": f"site-per-rank x{world}"},

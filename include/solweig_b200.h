@@ -54,6 +54,7 @@ extern "C" {
 #define SW100_CUBE_WORDS 5      /* ceil(153 / 32) */
 #define SW100_MAX_CLASSES 8     /* land-cover property classes */
 #define SW100_N_GVF_AZ 18       /* ground view factor search azimuths */
+#define SW100_UTCI_TERMS 210   /* terms of the UTCI regression */
 #define SW100_MAX_GVF_STEPS 64  /* bound on the `second` walk length */
 #define SW100_SVF_PLANES 19     /* 15 SVF planes, SVFtotal, 3 time-loop statics */
 
@@ -105,7 +106,7 @@ typedef struct {
   int32_t n_patches;                          /* 153 */
   int32_t n_rings;                            /* 8 */
   int32_t bush_any;                           /* bush.max() > 0 */
-  int32_t pad0;
+  int32_t all_finite;                         /* no NaN / inf in dsm, vegdsm, vegdsm2 */
   int32_t step_offset[SW100_MAX_PATCHES];     /* into the step table */
   int32_t step_count[SW100_MAX_PATCHES];
   int32_t ring[SW100_MAX_PATCHES];            /* altitude band of the patch */
@@ -247,11 +248,13 @@ typedef struct {
   float ta_mat;             /* float32(Ta) + float32(uhii) */
   int32_t landcover;        /* Tg = max(Tg, 0) when land cover is used */
   float tg_factor[SW100_MAX_CLASSES]; /* sin(...) of the Tg wave per TmaxLST class */
-  int32_t pad1;
-  /* UTCI polynomial of this step in (D = Tmrt - Ta, va):
-   * utci = sum_i D^i sum_j utci_c[i * 7 + j] va^j, coefficients folded from
-   * the 210-term regression with this step's Ta and Pa */
-  double utci_c[49];
+  /* UTCI of this step (calculate_utci.py:259-330, float32 as the reference
+   * evaluates it): Pa^1..Pa^6 of this step's vapour pressure, and per
+   * regression term j the float32 product c_j * Ta^pt_j (c_j when pt_j == 0);
+   * the kernel multiplies in va, D = Tmrt - Ta and Pa and sums in order */
+  float utci_pa[6];
+  float utci_k[SW100_UTCI_TERMS];
+  int32_t pad1[2];
 } sw100_time_step;
 
 /* All tables of one site's time loop (device pointers). */

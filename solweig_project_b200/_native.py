@@ -21,6 +21,7 @@ MAX_RINGS = 16
 MAX_ANNULI = 16
 MAX_CLASSES = 8
 N_GVF_AZ = 18
+UTCI_TERMS = 210
 MAX_GVF_STEPS = 64
 SVF_PLANES = 19
 SVF_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024 + 256 * 1024
@@ -52,7 +53,7 @@ class NativeError(RuntimeError):
 STEP_DTYPE = np.dtype([("dx", "<i4"), ("dy", "<i4"), ("dz", "<f4"), ("pad", "<i4")], align=True)
 
 SVF_PLAN_DTYPE = np.dtype([
-    ("n_patches", "<i4"), ("n_rings", "<i4"), ("bush_any", "<i4"), ("pad0", "<i4"),
+    ("n_patches", "<i4"), ("n_rings", "<i4"), ("bush_any", "<i4"), ("all_finite", "<i4"),
     ("step_offset", "<i4", (MAX_PATCHES,)), ("step_count", "<i4", (MAX_PATCHES,)),
     ("ring", "<i4", (MAX_PATCHES,)), ("dir_flags", "<i4", (MAX_PATCHES,)),
     ("ring_annuli", "<i4", (MAX_RINGS,)),
@@ -86,11 +87,12 @@ TIME_STEP_DTYPE = np.dtype([
     ("second", "<f4"), ("tan_beta", "<f4"), ("qa", "<f4"), ("refl_k", "<f4"), ("night_lup_base", "<f4"),
     ("absK", "<f4"), ("absL", "<f4"), ("Fside", "<f4"), ("Fup", "<f4"), ("Fcyl", "<f4"),
     ("absl_sbc", "<f4"), ("rh32", "<f4"), ("ws32", "<f4"), ("ta_mat", "<f4"), ("landcover", "<i4"),
-    ("tg_factor", "<f4", (MAX_CLASSES,)), ("pad1", "<i4"), ("utci_c", "<f8", (49,)),
+    ("tg_factor", "<f4", (MAX_CLASSES,)), ("utci_pa", "<f4", (6,)), ("utci_k", "<f4", (UTCI_TERMS,)),
+    ("pad1", "<i4", (2,)),
 ], align=True)
 
 EXPECTED_SIZES = {"sw100_step": 16, "sw100_svf_plan": 4700, "sw100_sun_step": 32,
-                  "sw100_gvf_azimuth": 144, "sw100_patch_step": 128, "sw100_time_step": 568}
+                  "sw100_gvf_azimuth": 144, "sw100_patch_step": 128, "sw100_time_step": 1040}
 DTYPES = {"sw100_step": STEP_DTYPE, "sw100_svf_plan": SVF_PLAN_DTYPE, "sw100_sun_step": SUN_STEP_DTYPE,
           "sw100_gvf_azimuth": GVF_AZ_DTYPE, "sw100_patch_step": PATCH_STEP_DTYPE,
           "sw100_time_step": TIME_STEP_DTYPE}

@@ -36,12 +36,17 @@ def nvcc() -> str:
 
 
 def write_utci_include() -> str:
-    """Generate csrc/utci_terms.inc from data/utci_terms.json."""
+    """Generate csrc/utci_series.inc from data/utci_terms.json: one
+    SW_UTCI_TERM(j, pt, pv, pd, pp, c) line per regression term, in the
+    reference's summation order, with c rounded to float32 (written as an
+    exact hexadecimal literal)."""
+    import numpy as np
     with open(os.path.join(PKG, "data", "utci_terms.json")) as fh:
         terms = json.load(fh)["terms"]
-    lines = [f"{{{c}, {a}, {b}, {d}, {e}}}," for c, a, b, d, e in terms]
+    lines = [f"SW_UTCI_TERM({j}, {a}, {b}, {d}, {e}, {float(np.float32(float(c))).hex()}f)"
+             for j, (c, a, b, d, e) in enumerate(terms)]
     text = "// generated from solweig_project_b200/data/utci_terms.json\n" + "\n".join(lines) + "\n"
-    path = os.path.join(CSRC, "utci_terms.inc")
+    path = os.path.join(CSRC, "utci_series.inc")
     old = open(path).read() if os.path.exists(path) else None
     if old != text:
         with open(path, "w") as fh:

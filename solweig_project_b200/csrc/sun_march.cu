@@ -33,7 +33,8 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
     const int sr = r + st.dx, sc = c + st.dy;
     const float dz = st.dz;
     float temp = 0.f, tv = 0.f, tv2 = 0.f, tlf = 0.f, tlg = 0.f;
-    if (in_grid(sr, sc, rows, cols)) {
+    const bool inb = in_grid(sr, sc, rows, cols);
+    if (inb) {
       const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
       temp = __fsub_rn(v.x, dz);
       tv = __fsub_rn(v.y, dz);
@@ -51,12 +52,13 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
     vegsh = tmax(vegsh, vegsh2);
     if (vegsh * sh > 0.f) vegsh = 0.f;
     vbsh = vbsh + vegsh;
-    // Nothing above this pixel can be reached any more: every later source
-    // height minus a larger drop stays at or below the pixel, its running
-    // building maximum and its running vegetation maximum (out-of-grid reads
-    // are 0, covered by a >= 0 and shvoveg >= 0).
+    // Nothing above this pixel can be reached any more: the ray has left the
+    // grid (it stays out and reads zeros), or every later source height
+    // minus a larger drop stays at or below the pixel, its running building
+    // maximum and its running vegetation maximum.  Zeros are covered by
+    // a >= 0 and shvoveg >= 0.
     const float top = __fsub_rn(vmax, dz);
-    if (a >= 0.f && shvoveg >= 0.f && top <= a && top <= shvoveg) break;
+    if (a >= 0.f && shvoveg >= 0.f && (!inb || (top <= a && top <= shvoveg))) break;
   }
   MarchOut o;
   float facesh;

@@ -44,7 +44,8 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
     const int sr = r + st.dx, sc = c + st.dy;
     const float dz = st.dz;
     float temp = 0.f, tv = 0.f, tv2 = 0.f, tb = 0.f;
-    if (in_grid(sr, sc, rows, cols)) {
+    const bool inb = in_grid(sr, sc, rows, cols);
+    if (inb) {
       const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
       temp = __fsub_rn(v.x, dz);
       tv = __fsub_rn(v.y, dz);
@@ -73,9 +74,11 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
     }
     if (may_exit && k >= 1) {
       // nothing later can change sh / vegsh / vbsh>0: building shadow is
-      // final, or no source can rise above this pixel any more
-      // (out-of-grid reads are 0, so the height test needs a >= 0)
-      const bool done = (sh == 1.f) || (a >= 0.f && __fsub_rn(vmax, dz) <= a);
+      // final, or no source can rise above this pixel any more -- the ray
+      // has left the grid (shifts grow monotonically, so it stays out and
+      // reads zeros) or even the highest source minus the growing drop stays
+      // at or below the pixel.  Both need a >= 0 (zeros never exceed it).
+      const bool done = (sh == 1.f) || (a >= 0.f && (!inb || __fsub_rn(vmax, dz) <= a));
       if (done) {
         if (vegsh > 0.f && vbsh == 0 && k + 1 < n) vbsh = 1;
         break;
@@ -100,6 +103,59 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
   vb_out = vb;
 }
 
+// The same march for a pixel that grows no bush shadow, on finite inputs.
+// There the running maximum f only matters through "f > a", which turns on
+// at the first source with height - dz > a and stays on; building shadow
+// then zeroes the vegetation state for good, so the march ends there.
+// vegsh and the "vbshvegsh ever counted" flag are booleans.  Returns final
+// (sh, vegsh, vbshvegsh) with values as march_patch.
+__device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4, int rows, int cols, int r, int c,
+                                                 float a, float veg2_p, const sw100_step* __restrict__ steps, int n,
+                                                 float vmax, float& sh_out, float& veg_out, float& vb_out) {
+  bool sh = false, vegsh = false, vb_any = false;
+  if (n > 0) {
+    // first step (index 1 of shadow.py): the trunk-zone rule of :288-293
+    const sw100_step st = load_step(&steps[0]);
+    const int sr = r + st.dx, sc = c + st.dy;
+    float temp = 0.f, tv = 0.f, tv2 = 0.f;
+    if (in_grid(sr, sc, rows, cols)) {
+      const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
+      temp = __fsub_rn(v.x, st.dz);
+      tv = __fsub_rn(v.y, st.dz);
+      tv2 = __fsub_rn(v.z, st.dz);
+    }
+    sh = temp > a;
+    vegsh = (tv > a) && !(tv2 > a) && !sh;
+    float first = __fsub_rn(tv, temp);
+    if (first <= 0.f) first = 1000.f;
+    if (first < st.dz) vegsh = true;
+    vegsh = vegsh && (veg2_p > a);
+    if (sh) {
+      if (n > 1) vegsh = false;  // the next step zeroes it under building shadow
+    } else {
+      for (int k = 1; k < n; ++k) {
+        const sw100_step sk = load_step(&steps[k]);
+        const int rr = r + sk.dx, cc = c + sk.dy;
+        if (!in_grid(rr, cc, rows, cols)) {
+          // zeros from here on: shadow only for a pixel below 0
+          if (0.f > a) { sh = true; vegsh = false; }
+          else vb_any = vb_any || vegsh;
+          break;
+        }
+        const float4 v = __ldg(&src4[(size_t)rr * cols + cc]);
+        if (__fsub_rn(v.x, sk.dz) > a) { sh = true; vegsh = false; break; }
+        vegsh = vegsh || ((__fsub_rn(v.y, sk.dz) > a) && !(__fsub_rn(v.z, sk.dz) > a));
+        vb_any = vb_any || vegsh;
+        if (a >= 0.f && __fsub_rn(vmax, sk.dz) <= a) break;
+      }
+    }
+  }
+  const float vegf = vegsh ? 1.f : 0.f;
+  sh_out = sh ? 0.f : 1.f;
+  veg_out = 1.f - vegf;
+  vb_out = 1.f - ((vb_any ? 1.f : 0.f) - vegf);
+}
+
 __global__ void __launch_bounds__(128) svf_sweep_kernel(
     const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
     const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
@@ -120,6 +176,7 @@ __global__ void __launch_bounds__(128) svf_sweep_kernel(
   const float4 self = src4[p];
   const float a = self.x, veg2_p = self.z, bush_p = self.w;
   const bool bush_any = plan.bush_any != 0;
+  const bool fast = plan.all_finite != 0 && !(bush_any && bush_p > 1.f);
 
   SvfAcc A = {};
   uint32_t wsh[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
@@ -129,8 +186,11 @@ __global__ void __launch_bounds__(128) svf_sweep_kernel(
   for (int q = 0; q < plan.n_patches; ++q) {
     const int off = plan.step_offset[q];
     float sh, veg, vb;
-    march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, plan.step_count[q],
-                bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);
+    if (fast)
+      march_patch_fast(src4, rows, cols, r, c, a, veg2_p, steps + off, plan.step_count[q], vmax, sh, veg, vb);
+    else
+      march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, plan.step_count[q],
+                  bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);
     const uint32_t bit = 1u << (q & 31);
     if (sh != 0.f) wsh[q >> 5] |= bit;
     if (veg != 0.f) wveg[q >> 5] |= bit;

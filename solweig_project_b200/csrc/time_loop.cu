@@ -25,6 +25,7 @@
 
 #include "sw_common.cuh"
 #include "sw_internal.cuh"
+#include "utci_series.cuh"
 
 namespace sw100 {
 
@@ -71,18 +72,57 @@ __device__ __forceinline__ float cylindric_wedge(float ta, float tb, float qa) {
   return fsh;
 }
 
-// UTCI polynomial in (D_Tmrt, va) for this step: sum_i D^i sum_j c[i][j] va^j
-__device__ __forceinline__ float utci_poly(const double* c, float d, float va) {
-  const double D = d, V = va;
-  double acc = 0.0;
-#pragma unroll
-  for (int i = 6; i >= 0; --i) {
-    double q = 0.0;
-#pragma unroll
-    for (int j = 6 - i; j >= 0; --j) q = q * V + c[i * 7 + j];
-    acc = acc * D + q;
+// Running state of one ground-view-factor search direction
+// (sunonsurface_2018a, solweig.py:155-213).  Building flags, the running
+// minimum f and the wall indicators are 0/1, so min / or become products /
+// maxima (exact on those values).
+struct GvfWalk {
+  float f;
+  float tbu = 0.f, tsh = 0.f, tlup = 0.f, talb = 0.f, talbsh = 0.f, twall = 0.f;
+  float wsh = 0.f, wLupsh = 0.f, walbsh = 0.f, walbnosh = 0.f;
+  float wLwall = 0.f, walbwall = 0.f, wwall = 0.f, walbwallnosh = 0.f;
+  float tempbub = 0.f, tempbubwall = 0.f;
+  float s_wall = 0.f, s_Lwall = 0.f, s_Lupsh = 0.f, s_albwall = 0.f, s_albsh = 0.f, s_albwallnosh = 0.f,
+        s_albnosh = 0.f;
+  __device__ __forceinline__ void snapshot() {
+    s_wall = wwall; s_Lwall = wLwall; s_Lupsh = wLupsh; s_albwall = walbwall; s_albsh = walbsh;
+    s_albwallnosh = walbwallnosh; s_albnosh = walbnosh;
   }
-  return (float)acc;
+};
+
+// Steps [n0, n1) of one walk.  A source outside the grid keeps the previous
+// sample (the reference's temporaries are never cleared).
+template <bool CHECKED>
+__device__ __forceinline__ void gvf_walk(GvfWalk& W, const float4* __restrict__ G, int r, int c, int rows, int cols,
+                                         const int8_t* dx, const int8_t* dy, int n0, int n1, float lwall,
+                                         float albedo_b) {
+  for (int n = n0; n < n1; ++n) {
+    const int sr = r + dx[n], sc = c + dy[n];
+    if (!CHECKED || in_grid(sr, sc, rows, cols)) {
+      const float4 g = G[(size_t)sr * cols + sc];
+      const uint32_t fl = __float_as_uint(g.w);
+      W.tbu = (fl & 1u) ? 1.f : 0.f;
+      W.tsh = g.x;
+      W.tlup = g.y;
+      W.talb = g.z;
+      W.talbsh = g.z * g.x;
+      W.twall = (fl & 2u) ? 1.f : 0.f;
+    }
+    const float f = W.f * W.tbu;  // torch.min of 0/1 values
+    W.f = f;
+    W.wsh = W.wsh + W.tsh * f;
+    W.wLupsh = W.wLupsh + W.tlup * f;
+    W.walbsh = W.walbsh + W.talbsh * f;
+    W.walbnosh = W.walbnosh + W.talb * f;
+    const float tempb = W.twall * f;
+    const float tempbwall = 1.f - f;  // f * -1 + 1
+    W.tempbub = fmaxf(tempb, W.tempbub);              // (tempb + tempbub) > 0 on 0/1 values
+    W.tempbubwall = fmaxf(tempbwall, W.tempbubwall);
+    W.wLwall = W.wLwall + W.tempbub * lwall;
+    W.walbwall = W.walbwall + W.tempbub * albedo_b;
+    W.wwall = W.wwall + W.tempbub;
+    W.walbwallnosh = W.walbwallnosh + W.tempbubwall * albedo_b;
+  }
 }
 
 struct GvfSums {
@@ -90,7 +130,7 @@ struct GvfSums {
   float LupE, albE, albnoshE, LupS, albS, albnoshS, LupW, albW, albnoshW, LupN, albN, albnoshN;
 };
 
-__global__ void __launch_bounds__(128) time_loop_kernel(
+__global__ void __launch_bounds__(128, 5) time_loop_kernel(
     SitePlanes site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, float* __restrict__ state,
@@ -162,7 +202,7 @@ __global__ void __launch_bounds__(128) time_loop_kernel(
 
     float shadow = 0.f, Lup, LupE, LupS, LupW, LupN;
     float Kdown = 0.f, Kup = 0.f, KupE = 0.f, KupS = 0.f, KupW = 0.f, KupN = 0.f;
-    float Kside = 0.f;
+    float Kside = 0.f, ksideI = 0.f, albF_day = 0.f;
     if (P.is_day) {
       const float4* G = gsrc + (size_t)P.day_row * npix;
       const float4 own = G[p];
@@ -174,44 +214,30 @@ __global__ void __launch_bounds__(128) time_loop_kernel(
       const int second_i = (int)P.second;
       const float first = P.first, second = P.second;
       const float f1 = first + 1.f, s1 = second + 1.f;
+      // a pixel at least `second - 1` pixels from every edge never walks out
+      // of the grid: its walk needs no bounds test
+      const int reach = second_i - 1;
+      const bool interior = r >= reach && r < rows - reach && c >= reach && c < cols - reach;
+      const int first_i = (int)first;
+      const int snap_n = min(first_i, second_i);  // snapshot after this many steps
       for (int az = 0; az < SW100_N_GVF_AZ; ++az) {
-        float f = bld;
-        float tbu = 0.f, tsh = 0.f, tlup = 0.f, talb = 0.f, talbsh = 0.f, twall = 0.f;
-        float wsh_ = 0.f, wLupsh = 0.f, walbsh = 0.f, walbnosh = 0.f;
-        float wLwall = 0.f, walbwall = 0.f, wwall = 0.f, walbwallnosh = 0.f;
-        float tempbub = 0.f, tempbubwall = 0.f;
-        float s_wall = 0.f, s_Lwall = 0.f, s_Lupsh = 0.f, s_albwall = 0.f, s_albsh = 0.f, s_albwallnosh = 0.f,
-              s_albnosh = 0.f;
-        for (int n = 0; n < second_i; ++n) {
-          const int sr = r + AZ[az].dx[n], sc = c + AZ[az].dy[n];
-          if (in_grid(sr, sc, rows, cols)) {
-            const float4 g = G[(size_t)sr * cols + sc];
-            const uint32_t fl = __float_as_uint(g.w);
-            tbu = (fl & 1u) ? 1.f : 0.f;
-            tsh = g.x;
-            tlup = g.y;
-            talb = g.z;
-            talbsh = g.z * g.x;
-            twall = (fl & 2u) ? 1.f : 0.f;
-          }
-          f = tmin(f, tbu);
-          wsh_ = wsh_ + tsh * f;
-          wLupsh = wLupsh + tlup * f;
-          walbsh = walbsh + talbsh * f;
-          walbnosh = walbnosh + talb * f;
-          const float tempb = twall * f;
-          const float tempbwall = f * -1.f + 1.f;
-          tempbub = (tempb + tempbub) > 0.f ? 1.f : 0.f;
-          tempbubwall = (tempbwall + tempbubwall) > 0.f ? 1.f : 0.f;
-          wLwall = wLwall + tempbub * P.lwall;
-          walbwall = walbwall + tempbub * P.albedo_b;
-          wwall = wwall + tempbub;
-          walbwallnosh = walbwallnosh + tempbubwall * P.albedo_b;
-          if ((float)(n + 1) <= first) {
-            s_wall = wwall; s_Lwall = wLwall; s_Lupsh = wLupsh; s_albwall = walbwall; s_albsh = walbsh;
-            s_albwallnosh = walbwallnosh; s_albnosh = walbnosh;
-          }
+        GvfWalk W;
+        W.f = bld;
+        if (interior) {
+          gvf_walk<false>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, 0, snap_n, P.lwall, P.albedo_b);
+          W.snapshot();
+          gvf_walk<false>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, snap_n, second_i, P.lwall, P.albedo_b);
+        } else {
+          gvf_walk<true>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, 0, snap_n, P.lwall, P.albedo_b);
+          W.snapshot();
+          gvf_walk<true>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, snap_n, second_i, P.lwall, P.albedo_b);
         }
+        const float wsh_ = W.wsh, wLupsh = W.wLupsh, walbsh = W.walbsh, walbnosh = W.walbnosh;
+        float wLwall = W.wLwall, walbwall = W.walbwall;
+        const float wwall = W.wwall, walbwallnosh = W.walbwallnosh;
+        const float s_wall = W.s_wall, s_Lwall = W.s_Lwall, s_Lupsh = W.s_Lupsh, s_albwall = W.s_albwall,
+                    s_albsh = W.s_albsh, s_albwallnosh = W.s_albwallnosh, s_albnosh = W.s_albnosh;
+        (void)wsh_;
         const float wsi_f = s_wall > 0.f ? 1.f : 0.f;
         const float wi_f = s_albwallnosh > 0.f ? 1.f : 0.f;
         const float wsi_s = wwall > 0.f ? 1.f : 0.f;
@@ -268,66 +294,77 @@ __global__ void __launch_bounds__(128) time_loop_kernel(
       KupS = (gvfalbS * P.radI) * P.sin_alt + kup_b * ganS;
       KupW = (gvfalbW * P.radI) * P.sin_alt + kup_b * ganW;
       KupN = (gvfalbN * P.radI) * P.sin_alt + kup_b * ganN;
-      const float ksideI = (shadow * P.radI) * P.cos_alt;
-      float ksideD = 0.f, kref_sun = 0.f, kref_sh = 0.f, kref_veg = 0.f, anilum = 0.f;
-      for (int q = 0; q < n_patches; ++q) {
-        const sw100_patch_step& Q = PP[q];
-        const uint32_t b = 1u << (q & 31);
-        const int w = q >> 5;
-        const bool sh = wsh[w] & b, veg = wveg[w] & b;
-        const bool vb1 = wvb[w] & b;
-        const bool vb0 = !vb1 && !(site.single_step[w] & b);
-        const int di = (sh ? 2 : 0) + (veg ? 1 : 0);
-        ksideD = ksideD + Q.kside_d[di];
-        anilum = anilum + Q.anilum[di];
-        if (!veg || vb0) kref_veg = kref_veg + Q.kref_veg;
-        if (!sh && vb1) {
-          const float td = hsvf + Q.yi_k;
-          if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
-          if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
-        }
-      }
-      Kside = (((ksideI + ksideD) + kref_sun) + kref_sh) + kref_veg;
-      const float dRad = anilum * P.radD;
-      Kdown = ((P.radI * shadow) * P.sin_alt + dRad) + albF;
+      ksideI = (shadow * P.radI) * P.cos_alt;
+      albF_day = albF;
     } else {
       Lup = (P.sbc * emis) * pow4f(P.night_lup_base);
       LupE = LupS = LupW = LupN = Lup;
     }
-    // ---------------- longwave (Lcyl_v2022a / define_patch_characteristics)
+    // ---------------- 153-patch sums: Kside (day) and Lcyl pass 1
+    // (solweig.py:683-724 and 1514-1611).  The patch masks come from the bit
+    // cubes one 32-patch word at a time (the word loop is unrolled so the
+    // words stay in registers).
+    float ksideD = 0.f, kref_sun = 0.f, kref_sh = 0.f, kref_veg = 0.f, anilum = 0.f;
     float ld_sky = 0.f, ld_veg = 0.f, ld_sh = 0.f, ld_sun = 0.f, ld_ref = 0.f;
     float ls_sky = 0.f, ls_veg = 0.f, ls_sh = 0.f, ls_sun = 0.f, ls_ref = 0.f;
-    for (int q = 0; q < n_patches; ++q) {
-      const sw100_patch_step& Q = PP[q];
-      const uint32_t b = 1u << (q & 31);
-      const int w = q >> 5;
-      const bool sh = wsh[w] & b, veg = wveg[w] & b;
-      const bool vb1 = wvb[w] & b;
-      const bool vb0 = !vb1 && !(site.single_step[w] & b);
-      if (sh && veg) { ld_sky = ld_sky + Q.ld_sky; ls_sky = ls_sky + Q.ls_sky; }
-      if (!veg || vb0) { ls_veg = add64(ls_veg, Q.veg_cos); ld_veg = add64(ld_veg, Q.veg_sin); }
-      const bool tsh = !sh && vb1;
-      if (Q.flags & 1) {
-        if (tsh) {
-          const float td = hsvf + Q.yi_l;
-          if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
-          if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
+    const bool day = P.is_day != 0;
+#pragma unroll
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+      const int q0 = w * 32;
+      const int nq = min(32, n_patches - q0);
+      const uint32_t sw = wsh[w], vw = wveg[w], bw = wvb[w], sgl = site.single_step[w];
+      for (int j = 0; j < nq; ++j) {
+        const sw100_patch_step& Q = PP[q0 + j];
+        const bool sh = (sw >> j) & 1u, veg = (vw >> j) & 1u;
+        const bool vb1 = (bw >> j) & 1u;                      // vbshvegsh == 1
+        const bool vb0 = !vb1 && !((sgl >> j) & 1u);          // vbshvegsh == 0
+        const bool tsh = !sh && vb1;                           // (1 - sh) * vb == 1
+        const bool tveg = !veg || vb0;
+        if (day) {
+          const int di = (sh ? 2 : 0) + (veg ? 1 : 0);
+          ksideD = ksideD + Q.kside_d[di];
+          anilum = anilum + Q.anilum[di];
+          if (tveg) kref_veg = kref_veg + Q.kref_veg;
+          if (tsh) {
+            const float td = hsvf + Q.yi_k;
+            if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
+            if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
+          }
         }
-      } else if (tsh) {
-        ls_sh = add64(ls_sh, Q.sh_cos);
-        ld_sh = add64(ld_sh, Q.sh_sin);
+        if (sh && veg) { ld_sky = ld_sky + Q.ld_sky; ls_sky = ls_sky + Q.ls_sky; }
+        if (tveg) { ls_veg = add64(ls_veg, Q.veg_cos); ld_veg = add64(ld_veg, Q.veg_sin); }
+        if (tsh) {
+          if (Q.flags & 1) {
+            const float td = hsvf + Q.yi_l;
+            if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
+            if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
+          } else {
+            ls_sh = add64(ls_sh, Q.sh_cos);
+            ld_sh = add64(ld_sh, Q.sh_sin);
+          }
+        }
       }
     }
+    if (day) {
+      Kside = (((ksideI + ksideD) + kref_sun) + kref_sh) + kref_veg;
+      const float dRad = anilum * P.radD;
+      Kdown = ((P.radI * shadow) * P.sin_alt + dRad) + albF_day;
+    }
+    // ---------------- Lcyl pass 2: reflected longwave (solweig.py:1613-1633)
     const float refl = (((ld_sky + Lup) * P.refl_k) * 0.5f) / 3.14159274101257324f;
-    for (int q = 0; q < n_patches; ++q) {
-      const sw100_patch_step& Q = PP[q];
-      const uint32_t b = 1u << (q & 31);
-      const int w = q >> 5;
-      const bool vb0 = !(wvb[w] & b) && !(site.single_step[w] & b);
-      if (!(wsh[w] & b) || !(wveg[w] & b) || vb0) {
-        const float rs = refl * Q.ster;
-        ls_ref = ls_ref + rs * Q.cos_alt;
-        ld_ref = ld_ref + rs * Q.sin_alt;
+#pragma unroll
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+      const int q0 = w * 32;
+      const int nq = min(32, n_patches - q0);
+      // temp_sh = (sh == 0) | (vegsh == 0) | (vbshvegsh == 0)
+      const uint32_t any0 = ~wsh[w] | ~wveg[w] | (~wvb[w] & ~site.single_step[w]);
+      for (int j = 0; j < nq; ++j) {
+        if ((any0 >> j) & 1u) {
+          const sw100_patch_step& Q = PP[q0 + j];
+          const float rs = refl * Q.ster;
+          ls_ref = ls_ref + rs * Q.cos_alt;
+          ld_ref = ld_ref + rs * Q.sin_alt;
+        }
       }
     }
     const float Lside = (((ls_sky + ls_veg) + ls_sh) + ls_sun) + ls_ref;
@@ -350,7 +387,7 @@ __global__ void __launch_bounds__(128) time_loop_kernel(
         float va = wind * P.ws32;
         va = (va < 0.15f) ? 0.15f : va;
         if (P.ta_mat <= -999.f || P.rh32 <= -999.f || va <= -999.f || tmrt <= -999.f) u = -999.f;
-        else u = utci_poly(P.utci_c, tmrt - P.ta_mat, va);
+        else u = utci_series_step(P.utci_k, P.utci_pa, P.ta_mat, va, tmrt - P.ta_mat);
       }
       o[slot++ * blk] = u;
     }

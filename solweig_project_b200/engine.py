@@ -133,6 +133,7 @@ class DeviceSite:
         self.amax = F32(amaxvalue) if amaxvalue is not None else amax
         self.bush_any = bool(bush.max() > 0)
         self.vmax = F32(max(a.max(), vegdsm.max(), vegdsm2.max()))
+        self.all_finite = bool(np.isfinite(a).all() and np.isfinite(vegdsm).all() and np.isfinite(vegdsm2).all())
         self.scale = float(scale)
         d = self.device
         self.t = {
@@ -167,6 +168,7 @@ class DeviceSite:
         self.amax = F32(amaxvalue)
         self.bush_any = bool(bush.max() > 0)
         self.vmax = F32(max(a.max(), vegdsm.max(), vegdsm2.max()))
+        self.all_finite = bool(np.isfinite(a).all() and np.isfinite(vegdsm).all() and np.isfinite(vegdsm2).all())
         self.scale = float(scale)
         d = self.device
         self.t = {"dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
@@ -200,7 +202,8 @@ class DeviceSite:
         key = ("svf", patch_option)
         if key not in self._cache:
             plan, steps, single = T.svf_plan(self.rows, self.cols, self.scale, self.amax, self.bush_any,
-                                             patch_option, trans_veg=self.params.transVeg)
+                                             patch_option, trans_veg=self.params.transVeg,
+                                             all_finite=self.all_finite)
             d = self.device
             ws_bytes = N.workspace_bytes("sw100_svf_workspace_bytes", self.rows, self.cols, len(steps))
             self._cache[key] = (_table(plan, d), _table(steps, d), len(steps), single,
@@ -325,7 +328,10 @@ class DeviceSite:
 
     def load_state(self, state: dict):
         for k, name in enumerate(STATE_NAMES):
-            self.state[k].copy_(torch.as_tensor(np.asarray(state[name], F32)))
+            v = state[name]
+            if not isinstance(v, torch.Tensor):
+                v = torch.as_tensor(np.asarray(v, F32))
+            self.state[k].copy_(v.to(dtype=torch.float32))
 
     def state_dict(self):
         return {name: self.state[k].clone() for k, name in enumerate(STATE_NAMES)}

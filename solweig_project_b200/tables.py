@@ -130,18 +130,25 @@ def _trig(az, alt):
             F32(torch.abs(1. / sin_a).item()), F32(torch.abs(1. / cos_a).item()))
 
 
-def svf_patch_table(azimuth_deg, altitude_deg, scale, amax, rows, cols):
-    """Executed steps of one SVF patch march (shadow.py:196-247)."""
+@functools.lru_cache(maxsize=1024)
+def _svf_patch_trig(azimuth_deg: float, altitude_deg: int):
+    """Site-independent part of a patch march: float32 trigonometry and the
+    step-direction branch (shadow.py:196-226)."""
     degrees = torch.pi / 180.
     az = torch.tensor(1e-12) if float(azimuth_deg) == 0.0 else torch.tensor(F32(azimuth_deg))
     alt = torch.tensor(int(altitude_deg))
     az = az * degrees
     alt = alt * degrees
     ssin, scos, tan_a, dssin, dscos = _trig(az, alt)
-    tanalt = F32((torch.tan(alt) / scale).item())
     pb4 = torch.pi / 4.
     branch_y = bool((pb4 <= az) & (az < 3. * pb4)) or bool((5. * pb4 <= az) & (az < 7. * pb4))
-    ds = dssin if branch_y else dscos
+    return branch_y, ssin, scos, tan_a, (dssin if branch_y else dscos), F32(torch.tan(alt).item())
+
+
+def svf_patch_table(azimuth_deg, altitude_deg, scale, amax, rows, cols):
+    """Executed steps of one SVF patch march (shadow.py:196-247)."""
+    branch_y, ssin, scos, tan_a, ds, tan_alt = _svf_patch_trig(float(azimuth_deg), int(altitude_deg))
+    tanalt = F32(tan_alt / F32(scale))  # float32 tensor / python float
     idx = np.arange(1, max(rows, cols) + 3)
     dx, dy, dz = _march_steps(branch_y, ssin, scos, tan_a, ds, tanalt, idx)
     n = _executed(dx, dy, dz, amax, rows, cols)
@@ -213,7 +220,7 @@ def gvf_table(second: int) -> np.ndarray:
     return tab
 
 
-def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03):
+def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03, all_finite=False):
     """SVF plan record + concatenated step table + single-step patch mask."""
     annulino, altint, _, nband = PATCH_LAYOUT[patch_option]
     azs = sweep_azimuths(patch_option)
@@ -223,6 +230,7 @@ def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03):
     plan["n_patches"] = P
     plan["n_rings"] = len(altint)
     plan["bush_any"] = int(bool(bush_any))
+    plan["all_finite"] = int(bool(all_finite))
     plan["ring_annuli"][0, :] = count
     plan["w_iso"][0] = w_iso
     plan["w_aniso"][0] = w_an

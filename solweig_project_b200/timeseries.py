@@ -208,8 +208,20 @@ def _perez(zen_deg, azimuth_deg, radD, radI, jday):
     return torch.stack([skyalt * rad2deg, skyazi * rad2deg, lv], dim=1)
 
 
+_STER_CACHE: dict = {}
+
+
 def _steradians(palt):
-    """Solid angle of each patch (solweig.py:688-697, 1707-1718)."""
+    """Solid angle of each patch (solweig.py:688-697, 1707-1718); a pure
+    function of the patch altitudes, which repeat from step to step."""
+    key = palt.numpy().tobytes()
+    hit = _STER_CACHE.get(key)
+    if hit is None:
+        hit = _STER_CACHE.setdefault(key, _steradians_uncached(palt))
+    return hit.clone()
+
+
+def _steradians_uncached(palt):
     deg2rad = torch.tensor(np.pi / 180)
     skyalt, cnt = torch.unique(palt, return_counts=True)
     ster = torch.zeros(palt.shape[0])
@@ -243,22 +255,49 @@ def _lsky(esky, palt, Ta64):
     return ld, ls, ster
 
 
-def _utci_coeffs(ta_mat: np.float32, rh32: np.float32) -> np.ndarray:
-    """Fold the 210-term regression for this step's Ta and Pa into a
-    polynomial in (D_Tmrt, va): c[d * 7 + v] (calculate_utci.py:24-330)."""
-    tk = torch.tensor([float(ta_mat)], dtype=torch.float32) + 273.15
-    g = torch.tensor(_ES_G, dtype=torch.float32)
-    es = g[7] * torch.log(tk)
-    for i in range(7):
-        es = es + g[i] * tk ** (i + 1 - 3.)
-    es = torch.exp(es) * 0.01
-    pa = float((es * torch.tensor([float(rh32)], dtype=torch.float32) / 100. / 10.0).item())
-    ta = float(ta_mat)
-    c = np.zeros(49, np.float64)
-    c[0] += ta
-    for coef, pt, pv, pd, pp in _TERMS:
-        c[pd * 7 + pv] += coef * ta ** pt * pa ** pp
-    return c
+def utci_pow(x, p: int) -> np.float32:
+    """x ** p of a float32 value as torch evaluates a float32 tensor ** int:
+    float32 products for p <= 3, the correctly rounded power for p = 4..6
+    (a float64 product chain rounded once); the device uses the same
+    arithmetic (csrc/utci_series.cuh)."""
+    x = F32(x)
+    if p == 1:
+        return x
+    if p == 2:
+        return x * x
+    if p == 3:
+        return (x * x) * x
+    d = np.float64(x)
+    d2 = d * d
+    d4 = d2 * d2
+    return F32(d4 if p == 4 else (d4 * d if p == 5 else d4 * d2))
+
+
+def utci_vapour_pressure(ta, rh) -> np.float32:
+    """Pa (kPa) of calculate_utci.py:273-282 in float32, log / exp rounded
+    once from float64."""
+    g = [F32(v) for v in _ES_G]
+    tk = F32(ta) + F32(273.15)
+    es = g[7] * F32(np.log(np.float64(tk)))
+    es = es + g[0] * (F32(1) / (tk * tk))
+    es = es + g[1] * (F32(1) / tk)
+    es = es + g[2] * F32(1)
+    es = es + g[3] * tk
+    es = es + g[4] * (tk * tk)
+    es = es + g[5] * ((tk * tk) * tk)
+    es = es + g[6] * utci_pow(tk, 4)
+    es = F32(np.exp(np.float64(es))) * F32(0.01)
+    return ((es * F32(rh)) / F32(100.0)) / F32(10.0)
+
+
+def _utci_table(ta_mat: np.float32, rh32: np.float32):
+    """Per-step UTCI table (calculate_utci.py:259-330): Pa^1..Pa^6 and, per
+    regression term, the float32 product c * Ta^pt that starts the term."""
+    pa = utci_vapour_pressure(ta_mat, rh32)
+    pa_pows = np.array([utci_pow(pa, p) for p in range(1, 7)], F32)
+    ta_pows = [F32(1)] + [utci_pow(ta_mat, p) for p in range(1, 7)]
+    k = np.array([F32(c) * ta_pows[pt] if pt else F32(c) for c, pt, _, _, _ in _TERMS], F32)
+    return pa_pows, k
 
 
 # -------------------------------------------------------------- the series
@@ -398,7 +437,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         S["ws32"] = F32(Ws_all[i])
         S["ta_mat"] = (F32(0) + F32(Ta_all[i])) + F32(uhii_all[i])
         S["landcover"] = props.landcover
-        S["utci_c"] = _utci_coeffs(S["ta_mat"], S["rh32"])
+        S["utci_pa"], S["utci_k"] = _utci_table(S["ta_mat"], S["rh32"])
         S["night_lup_base"] = ((F32(0) + ta32) + F32(0)) + F32(273.15)
         Q = patch[o]
         if alt64 > 0:
@@ -471,9 +510,9 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             # Kside per patch (solweig.py:683-724)
             palt, pazi, plum = lv[:, 0], lv[:, 1], lv[:, 2]
             ster = _steradians(palt)
-            radTot = torch.zeros(1)
-            for k in range(P):
-                radTot += (plum[k] * ster[k] * torch.sin(palt[k] * deg2rad_t))
+            # radTot += lum * ster * sin(alt), one float32 add per patch in order
+            terms = (plum * ster * torch.sin(palt * deg2rad_t)).numpy()
+            radTot = torch.tensor([np.add.accumulate(terms, dtype=F32)[-1]])
             lumChi = (plum * radD) / radTot
             sun_k = ((params.albedo_b * (radI * torch.cos(alt32 * deg2rad_t)) + (radD * 0.5)) / torch.pi)
             sh_k = ((params.albedo_b * radD * 0.5) / torch.pi)

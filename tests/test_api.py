@@ -1,0 +1,185 @@
+"""Drop-in API and the solweig_core-style seam.
+
+CPU tests cover argument validation and dispatch (they raise before any GPU
+work); GPU tests run the drop-ins against the reference goldens."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from conftest import golden_location, load_golden
+from golden_util import assert_bits_equal, max_abs
+
+from solweig_project_b200 import api
+from solweig_project_b200.core import (ArrayView, DispatchBlockedError, PhysicalWindow, RefusalReason,
+                                       RequestValidationError, SolveRequestView, StaleBufferError, TimeCoverage)
+from solweig_project_b200.core.dispatch import BACKEND_EXACT_CHAIN, resolve
+
+
+def _request(**kw):
+    base = dict(logical_domain_id="site", rows=10, cols=12, origin_x_m=0.0, origin_y_m=0.0, pixel_size_m=1.0,
+                read_window=PhysicalWindow(0, 10, 0, 12), write_window=PhysicalWindow(2, 8, 3, 9),
+                time=TimeCoverage(0, 24, 24), profile_id="b200")
+    base.update(kw)
+    return SolveRequestView(**base)
+
+
+def test_cuda_request_resolves_to_the_exact_chain():
+    res = resolve(_request())
+    assert res.ready and res.plan.backend == BACKEND_EXACT_CHAIN and res.plan.device == "cuda"
+
+
+def test_cpu_request_is_refused_not_retargeted():
+    res = resolve(_request(device="cpu"))
+    assert not res.ready and res.plan is None
+    assert res.refusal.reason is RefusalReason.UNSUPPORTED_DEVICE
+    with pytest.raises(DispatchBlockedError):
+        res.raise_if_blocked()
+
+
+def test_unknown_backend_preference_is_refused():
+    res = resolve(_request(), prefer_backend="numba-full-solve")
+    assert res.refusal.reason is RefusalReason.UNKNOWN_BACKEND
+
+
+@pytest.mark.parametrize("bad", [
+    dict(write_window=PhysicalWindow(0, 11, 0, 12)),
+    dict(read_window=PhysicalWindow(3, 8, 3, 9), write_window=PhysicalWindow(2, 8, 3, 9)),
+    dict(time=TimeCoverage(5, 30, 24)),
+    dict(rows=0),
+    dict(profile_id=""),
+    dict(device="tpu"),
+])
+def test_request_validation_refuses(bad):
+    with pytest.raises(RequestValidationError) as err:
+        _request(**bad).validate()
+    assert err.value.refusal.reason is RefusalReason.REQUEST_INVALID
+
+
+def test_frozen_view_detects_mutation():
+    a = np.zeros((4, 4), np.float32)
+    v = ArrayView.from_numpy(a, freeze=True, logical_domain_id="site")
+    v.assert_not_mutated()
+    a[1, 1] = 2
+    with pytest.raises(StaleBufferError):
+        v.assert_not_mutated()
+
+
+def test_run_utci_window_validates_before_gpu_work():
+    d = load_golden("city36")
+    common = dict(a=d["dsm"], temp1=d["trees"].copy(), temp2=d["dem"], walls=d["walls_ref"],
+                  dirwalls=d["aspect_ref"], svf_bundle=(), met_file=d["met"], altitude=d["altitude"],
+                  azimuth=d["azimuth"], zen=d["zen"], jday=d["jday"], dectime=d["dectime"], altmax=d["altmax"],
+                  location=golden_location(d), scale=1.0)
+    with pytest.raises(ValueError, match="unknown requested variables"):
+        api.run_utci_window(**common, requested_variables=("utci", "wbgt"))
+    with pytest.raises(ValueError, match="invalid time range"):
+        api.run_utci_window(**common, time_start=4, time_stop=2)
+    with pytest.raises(ValueError, match="out_window"):
+        api.run_utci_window(**common, out_window=(0, 99, 0, 5))
+    with pytest.raises(ValueError, match="requires out_window"):
+        api.run_utci_window(**common, svf_bundle_cubes_cropped=True)
+    with pytest.raises(ValueError, match="unknown model parameters"):
+        api.run_utci_window(**common, model_parameters={"albedo": 0.3})
+
+
+def test_svf_calculator_requires_its_inputs():
+    with pytest.raises(ValueError, match="must be provided"):
+        api.svf_calculator(2, amaxvalue=10.0, a=np.zeros((4, 4), np.float32))
+
+
+@pytest.mark.gpu
+def test_dropins_against_reference(cuda):
+    d = load_golden("city36")
+    import torch
+    from oracle.svf import scene_from_rasters
+    vegdsm, vegdsm2, bush, amax = scene_from_rasters(d["dsm"], d["trees"], d["dem"])
+    bundle = api.svf_calculator(2, amax, d["dsm"], vegdsm, vegdsm2, bush, 1.0)
+    names = ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg", "svfNveg", "svfS", "svfSaveg",
+             "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg", "vegshmat", "vbshvegshmat", "shmat", "svftotal")
+    for name, v in zip(names, bundle):
+        assert isinstance(v, torch.Tensor) and v.is_cuda
+        assert_bits_equal(v.cpu().numpy(), d["svf_" + name].astype(np.float32), name)
+    kw = dict(a=d["dsm"], temp1=d["trees"].copy(), temp2=d["dem"], walls=d["walls_ref"], dirwalls=d["aspect_ref"],
+              met_file=d["met"], altitude=d["altitude"], azimuth=d["azimuth"], zen=d["zen"], jday=d["jday"],
+              dectime=d["dectime"], altmax=d["altmax"], location=golden_location(d), scale=1.0,
+              amaxvalue=d["amaxvalue"], landcover_grid=d["landcover"], lc_class=d["lc_class"],
+              requested_variables=("utci", "tmrt", "shadow", "ta", "wind"))
+    # the dense 19-tuple, as the reference returns it
+    out, final = api.run_utci_window(svf_bundle=bundle, return_final_state=True, **kw)
+    assert_bits_equal(out["shadow"], d["out_shadow"], "shadow")
+    assert_bits_equal(out["ta"], d["out_ta"], "ta")
+    assert_bits_equal(out["wind"], d["out_wind"], "wind")
+    assert max_abs(out["tmrt"], d["out_tmrt"]) <= 1e-3
+    assert max_abs(out["utci"], d["out_utci"]) <= 1e-3
+    assert final["CI"] == float(d["final_CI"]) and final["next_step"] == 24
+    # the packed form gives the same numbers
+    packed = api.svf_calculator(2, amax, d["dsm"], vegdsm, vegdsm2, bush, 1.0, packed=True)
+    out2 = api.run_utci_window(svf_bundle=packed, **dict(kw, temp1=d["trees"].copy()))
+    assert_bits_equal(out2["shadow"], out["shadow"], "packed shadow")
+    assert max_abs(out2["tmrt"], out["tmrt"]) <= 1e-4
+    # warm start at step 10 resumes the cold trajectory
+    first, state = api.run_utci_window(svf_bundle=packed, time_stop=10, return_final_state=True,
+                                       **dict(kw, temp1=d["trees"].copy()))
+    rest = api.run_utci_window(svf_bundle=packed, time_start=10, initial_state=state,
+                               **dict(kw, temp1=d["trees"].copy()))
+    assert max_abs(rest["tmrt"], out2["tmrt"][10:]) <= 1e-4
+    with pytest.raises(ValueError, match="next_step"):
+        api.run_utci_window(svf_bundle=packed, time_start=11, initial_state=state,
+                            **dict(kw, temp1=d["trees"].copy()))
+    # out_window crops the full-window result
+    win = api.run_utci_window(svf_bundle=packed, out_window=(5, 30, 2, 20), **dict(kw, temp1=d["trees"].copy()))
+    assert_bits_equal(win["shadow"], out["shadow"][:, 5:30, 2:20], "window shadow")
+
+
+def _utci_f64(ta, rh, tmrt, va):
+    """UTCI of calculate_utci.py:259-330 re-evaluated in float64 (the float32
+    regression coefficients, every other operation in double), with the
+    largest magnitude the running sum `Ta + t_0 + ... + t_j` reaches."""
+    from oracle.radiation import _utci_terms
+    ta, rh, tmrt, va = (np.asarray(x, np.float64) for x in (ta, rh, tmrt, va))
+    g = [-2.8365744E3, -6.028076559E3, 1.954263612E1, -2.737830188E-2, 1.6261698E-5, 7.0229056E-10,
+         -1.8680009E-13, 2.7150305]
+    tk = ta + 273.15
+    es = g[7] * np.log(tk) + sum(g[i] * tk ** (i - 2.0) for i in range(7))
+    pa = np.exp(es) * 0.01 * rh / 100.0 / 10.0
+    d = tmrt - ta
+    acc = ta.copy()
+    peak = np.abs(acc)
+    for c, pt, pv, pd, pp in _utci_terms():
+        acc = acc + float(c) * ta ** pt * va ** pv * d ** pd * pa ** pp
+        peak = np.maximum(peak, np.abs(acc))
+    return acc, peak
+
+
+@pytest.mark.gpu
+def test_utci_calculator_against_oracle(cuda):
+    """The standalone UTCI against the oracle's float32 evaluation.
+
+    The 210-term sum is ill-conditioned for windy, hot inputs: its running
+    sum reaches ~1e4 while the result is ~10-50, so a one-ulp difference in
+    one float32 power (torch's vectorised pow is not correctly rounded)
+    moves the result by ulp(running sum).  Each value must be within 1e-3 C
+    of the oracle or within 4 ulp of its largest running sum, and the
+    device's error against a float64 re-evaluation may not exceed the
+    oracle's own by more than that bound."""
+    from oracle.radiation import utci_calculator as oracle_utci
+    rng = np.random.default_rng(0)
+    n = 20000
+    ta = rng.uniform(-20, 45, n).astype(np.float32)
+    rh = rng.uniform(5, 100, n).astype(np.float32)
+    tmrt = (ta + rng.uniform(-10, 40, n)).astype(np.float32)
+    va = rng.uniform(0.5, 15, n).astype(np.float32)
+    ta[:5] = -999.0
+    got = api.utci_calculator(ta, rh, tmrt, va).cpu().numpy()
+    want = oracle_utci(ta, rh, tmrt, va)
+    assert (got[:5] == -999).all()
+    got, want = got[5:].astype(np.float64), want[5:].astype(np.float64)
+    exact, peak = _utci_f64(ta[5:], rh[5:], tmrt[5:], va[5:])
+    bound = np.maximum(1e-3, 4 * np.spacing(peak.astype(np.float32)).astype(np.float64))
+    diff = np.abs(got - want)
+    assert (diff <= bound).all(), f"worst excess {float((diff - bound).max())}"
+    assert (np.abs(got - exact) <= np.abs(want - exact) + bound).all()
+    # calm, mild conditions (the chain's usual range) stay within 1e-3 C
+    calm = (va[5:] <= 4) & (ta[5:] <= 35)
+    assert diff[calm].max() <= 1e-3

@@ -114,21 +114,55 @@ def test_struct_layouts_match_c_header(tmp_path):
     assert sizes[len(names) + 1] == ctypes.sizeof(N.Series)
 
 
-def test_utci_coefficients_reproduce_polynomial():
-    """Folding Ta and Pa into a (D_Tmrt, va) polynomial is the same function."""
+def _series_step(pa_pows, k, ta, va, d):
+    """The device's per-step UTCI sum (csrc/utci_series.cuh utci_series_step)
+    restated in numpy float32."""
+    from oracle.radiation import _utci_terms
+    vp = [None] + [np.array([TS.utci_pow(x, p) for x in va], np.float32) for p in range(1, 7)]
+    dp = [None] + [np.array([TS.utci_pow(x, p) for x in d], np.float32) for p in range(1, 7)]
+    acc = np.full(va.shape, ta, np.float32)
+    for j, (_, pt, pv, pd, pp) in enumerate(_utci_terms()):
+        t = np.full(va.shape, k[j], np.float32)
+        if pv:
+            t = t * vp[pv]
+        if pd:
+            t = t * dp[pd]
+        if pp:
+            t = t * pa_pows[pp - 1]
+        acc = acc + t
+    return acc
+
+
+def test_utci_step_table_reproduces_the_reference_sum():
+    """The per-step table (Pa powers, c * Ta^pt per term) gives the
+    reference's float32 running sum: bit-equal on most pixels, and within
+    1e-3 C everywhere at the chain's wind speeds."""
     from oracle.radiation import utci_calculator
     rng = np.random.default_rng(3)
-    ta = np.float32(31.7)
-    rh = np.float32(48.0)
-    c = TS._utci_coeffs(np.float32(ta), np.float32(rh))
-    tmrt = rng.uniform(15, 75, 5000).astype(np.float32)
-    va = rng.uniform(0.5, 6, 5000).astype(np.float32)
-    want = utci_calculator(np.full(5000, ta, np.float32), np.full(5000, rh, np.float32), tmrt, va)
-    D = (tmrt - ta).astype(np.float64)
-    got = np.zeros(5000)
-    for i in range(6, -1, -1):
-        q = np.zeros(5000)
-        for j in range(6 - i, -1, -1):
-            q = q * va + c[i * 7 + j]
-        got = got * D + q
-    assert np.abs(got - want).max() < 2e-4
+    for ta, rh in ((np.float32(31.7), np.float32(48.0)), (np.float32(24.25), np.float32(70.0)),
+                   (np.float32(36.0), np.float32(35.0))):
+        pa_pows, k = TS._utci_table(ta, rh)
+        assert pa_pows.dtype == np.float32 and k.shape == (210,)
+        tmrt = rng.uniform(15, 75, 3000).astype(np.float32)
+        va = rng.uniform(0.15, 6, 3000).astype(np.float32)
+        want = utci_calculator(np.full(3000, ta, np.float32), np.full(3000, rh, np.float32), tmrt, va)
+        got = _series_step(pa_pows, k, ta, va, (tmrt - ta).astype(np.float32))
+        assert np.abs(got.astype(np.float64) - want).max() <= 1e-3
+        assert (got == want).mean() >= 0.9
+
+
+def test_utci_vapour_pressure_matches_the_reference_chain():
+    """Pa of calculate_utci.py:273-282: float32, log / exp rounded once."""
+    import torch
+    ta = np.linspace(-30, 50, 4001).astype(np.float32)
+    rh = np.float32(55.0)
+    tk = torch.from_numpy(ta + np.float32(273.15))
+    g = torch.tensor([-2.8365744E3, -6.028076559E3, 1.954263612E1, -2.737830188E-2,
+                      1.6261698E-5, 7.0229056E-10, -1.8680009E-13, 2.7150305], dtype=torch.float32)
+    es = g[7] * torch.log(tk)
+    for i in range(0, 7):
+        es = es + g[i] * tk ** (i + 1 - 3.)
+    want = ((torch.exp(es) * 0.01) * float(rh) / 100. / 10.0).numpy()
+    got = np.array([TS.utci_vapour_pressure(t, rh) for t in ta], np.float32)
+    rel = np.abs(got.astype(np.float64) - want) / np.abs(want)
+    assert rel.max() <= 4e-7 and (got == want).mean() >= 0.95

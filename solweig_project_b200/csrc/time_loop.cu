@@ -72,57 +72,87 @@ __device__ __forceinline__ float cylindric_wedge(float ta, float tb, float qa) {
   return fsh;
 }
 
-// Running state of one ground-view-factor search direction
-// (sunonsurface_2018a, solweig.py:155-213).  Building flags, the running
-// minimum f and the wall indicators are 0/1, so min / or become products /
-// maxima (exact on those values).
+// One ground-view-factor search direction (sunonsurface_2018a,
+// solweig.py:155-213) for one pixel.  The reference's running minimum f is
+// 0/1: it is 1 until the walk first meets a building sample and 0 from then
+// on.  While f == 1 the shadow / Lup / albedo sums grow by the sample and
+// tempbub is the running OR of the sunlit-wall samples; once f == 0 those
+// sums add exact zeros, tempbub is frozen and tempbubwall is 1.  The wall
+// sums only ever add 0 or one constant (Lwall, albedo_b), so each equals
+// that constant added k times in float32, k counted here and the value
+// looked up in a per-step table.  The walk therefore stops at the first
+// building, and every sum is the reference's own float32 sequence.
 struct GvfWalk {
-  float f;
-  float tbu = 0.f, tsh = 0.f, tlup = 0.f, talb = 0.f, talbsh = 0.f, twall = 0.f;
-  float wsh = 0.f, wLupsh = 0.f, walbsh = 0.f, walbnosh = 0.f;
-  float wLwall = 0.f, walbwall = 0.f, wwall = 0.f, walbwallnosh = 0.f;
-  float tempbub = 0.f, tempbubwall = 0.f;
-  float s_wall = 0.f, s_Lwall = 0.f, s_Lupsh = 0.f, s_albwall = 0.f, s_albsh = 0.f, s_albwallnosh = 0.f,
-        s_albnosh = 0.f;
-  __device__ __forceinline__ void snapshot() {
-    s_wall = wwall; s_Lwall = wLwall; s_Lupsh = wLupsh; s_albwall = walbwall; s_albsh = walbsh;
-    s_albwallnosh = walbwallnosh; s_albnosh = walbnosh;
-  }
+  float sLup, sAlb, sNosh;   // weightsum{Lupsh, albsh, albnosh} after `second` steps
+  float qLup, qAlb, qNosh;   // the same after the `first` snapshot
+  int m, m2;                 // steps with tempbub == 1 / tempbubwall == 1 (all steps)
+  int qm, qm2;               // the same at the snapshot
 };
 
-// Steps [n0, n1) of one walk.  A source outside the grid keeps the previous
-// sample (the reference's temporaries are never cleared).
 template <bool CHECKED>
-__device__ __forceinline__ void gvf_walk(GvfWalk& W, const float4* __restrict__ G, int r, int c, int rows, int cols,
-                                         const int8_t* dx, const int8_t* dy, int n0, int n1, float lwall,
-                                         float albedo_b) {
-  for (int n = n0; n < n1; ++n) {
-    const int sr = r + dx[n], sc = c + dy[n];
-    if (!CHECKED || in_grid(sr, sc, rows, cols)) {
-      const float4 g = G[(size_t)sr * cols + sc];
-      const uint32_t fl = __float_as_uint(g.w);
-      W.tbu = (fl & 1u) ? 1.f : 0.f;
-      W.tsh = g.x;
-      W.tlup = g.y;
-      W.talb = g.z;
-      W.talbsh = g.z * g.x;
-      W.twall = (fl & 2u) ? 1.f : 0.f;
+__device__ __forceinline__ GvfWalk gvf_walk(const float4* __restrict__ G, size_t p, int r, int c, int rows,
+                                            int cols, const int8_t* dx, const int8_t* dy, const int* off,
+                                            float bld, int second_i, int snap_n) {
+  float sLup = 0.f, sAlb = 0.f, sNosh = 0.f, qLup = 0.f, qAlb = 0.f, qNosh = 0.f;
+  int tb = 0, m = 0, n0 = second_i, qm = -1;
+  if (bld == 0.f) {
+    n0 = 0;  // f = min(buildings, .) is 0 from the first step
+  } else {
+    // the sample of the last in-grid step (the reference never clears its
+    // temporaries); step 0 has no shift, so it is always in the grid
+    uint32_t fl = 0u;
+    float tlup = 0.f, talb = 0.f, talbsh = 0.f;
+    for (int n = 0; n < second_i; ++n) {
+      bool load = true;
+      size_t src = 0;
+      if (CHECKED) {
+        const int sr = r + dx[n], sc = c + dy[n];
+        load = in_grid(sr, sc, rows, cols);
+        src = (size_t)sr * cols + sc;
+      } else {
+        src = (size_t)((long long)p + off[n]);
+      }
+      if (load) {
+        const float4 g = G[src];
+        fl = __float_as_uint(g.w);
+        tlup = g.y;
+        talb = g.z;
+        talbsh = g.z * g.x;  // albshadow = alb * shadow
+      }
+      if (!(fl & 1u)) {  // a building sample: f becomes 0
+        n0 = n;
+        break;
+      }
+      sLup = sLup + tlup;
+      sAlb = sAlb + talbsh;
+      sNosh = sNosh + talb;
+      tb |= (int)((fl >> 1) & 1u);
+      m += tb;
+      if (n + 1 == snap_n) { qLup = sLup; qAlb = sAlb; qNosh = sNosh; qm = m; }
     }
-    const float f = W.f * W.tbu;  // torch.min of 0/1 values
-    W.f = f;
-    W.wsh = W.wsh + W.tsh * f;
-    W.wLupsh = W.wLupsh + W.tlup * f;
-    W.walbsh = W.walbsh + W.talbsh * f;
-    W.walbnosh = W.walbnosh + W.talb * f;
-    const float tempb = W.twall * f;
-    const float tempbwall = 1.f - f;  // f * -1 + 1
-    W.tempbub = fmaxf(tempb, W.tempbub);              // (tempb + tempbub) > 0 on 0/1 values
-    W.tempbubwall = fmaxf(tempbwall, W.tempbubwall);
-    W.wLwall = W.wLwall + W.tempbub * lwall;
-    W.walbwall = W.walbwall + W.tempbub * albedo_b;
-    W.wwall = W.wwall + W.tempbub;
-    W.walbwallnosh = W.walbwallnosh + W.tempbubwall * albedo_b;
   }
+  GvfWalk W;
+  W.sLup = sLup; W.sAlb = sAlb; W.sNosh = sNosh;
+  const int rest = second_i - n0;  // steps with f == 0
+  W.m = m + tb * rest;
+  W.m2 = rest;
+  if (qm < 0) {  // the snapshot lies at or after the first building
+    W.qLup = sLup; W.qAlb = sAlb; W.qNosh = sNosh;
+    W.qm = m + tb * (snap_n - n0);
+    W.qm2 = snap_n - n0;
+  } else {
+    W.qLup = qLup; W.qAlb = qAlb; W.qNosh = qNosh;
+    W.qm = qm;
+    W.qm2 = 0;
+  }
+  return W;
+}
+
+// `x / d * sel + y / e * (1 - sel)` of the reference with sel in {0, 1}:
+// one of the two products is an exact zero, so only one quotient is needed
+// (the zero is still added, keeping the float32 result identical)
+__device__ __forceinline__ float pick_div(bool sel, float x, float d, float y, float e) {
+  return sel ? (x / d + 0.f) : (0.f + y / e);
 }
 
 struct GvfSums {
@@ -140,12 +170,16 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
   __shared__ __align__(16) sw100_time_step P;
   __shared__ __align__(16) sw100_patch_step PP[kMaxPatchSmem];
   __shared__ GvfAzSmem AZ[SW100_N_GVF_AZ];
+  __shared__ int AZOFF[SW100_N_GVF_AZ][SW100_MAX_GVF_STEPS];  // dx * cols + dy
+  // Lwall / albedo_b added k times in float32, k = 0..second (this step)
+  __shared__ float REP_L[SW100_MAX_GVF_STEPS + 1], REP_A[SW100_MAX_GVF_STEPS + 1];
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int nthr = blockDim.x * blockDim.y;
   for (int i = tid; i < SW100_N_GVF_AZ * SW100_MAX_GVF_STEPS; i += nthr) {
     const int a = i / SW100_MAX_GVF_STEPS, n = i % SW100_MAX_GVF_STEPS;
     AZ[a].dx[n] = gvf_az[a].dx[n];
     AZ[a].dy[n] = gvf_az[a].dy[n];
+    AZOFF[a][n] = (int)gvf_az[a].dx[n] * cols + (int)gvf_az[a].dy[n];
   }
   if (tid < SW100_N_GVF_AZ) {
     AZ[tid].facesh_mode = gvf_az[tid].facesh_mode;
@@ -196,6 +230,15 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
       int4* pd = reinterpret_cast<int4*>(PP);
       const int n16 = n_patches * (int)(sizeof(sw100_patch_step) / 16);
       for (int i = tid; i < n16; i += nthr) pd[i] = ps[i];
+      if (tsteps[t].is_day) {
+        const float lw = tsteps[t].lwall, ab = tsteps[t].albedo_b;
+        for (int i = tid; i <= SW100_MAX_GVF_STEPS; i += nthr) {
+          float sl = 0.f, sa = 0.f;
+          for (int k = 0; k < i; ++k) { sl = sl + lw; sa = sa + ab; }
+          REP_L[i] = sl;
+          REP_A[i] = sa;
+        }
+      }
     }
     __syncthreads();
     if (!live) continue;
@@ -221,39 +264,28 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
       const int first_i = (int)first;
       const int snap_n = min(first_i, second_i);  // snapshot after this many steps
       for (int az = 0; az < SW100_N_GVF_AZ; ++az) {
-        GvfWalk W;
-        W.f = bld;
-        if (interior) {
-          gvf_walk<false>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, 0, snap_n, P.lwall, P.albedo_b);
-          W.snapshot();
-          gvf_walk<false>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, snap_n, second_i, P.lwall, P.albedo_b);
-        } else {
-          gvf_walk<true>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, 0, snap_n, P.lwall, P.albedo_b);
-          W.snapshot();
-          gvf_walk<true>(W, G, r, c, rows, cols, AZ[az].dx, AZ[az].dy, snap_n, second_i, P.lwall, P.albedo_b);
-        }
-        const float wsh_ = W.wsh, wLupsh = W.wLupsh, walbsh = W.walbsh, walbnosh = W.walbnosh;
-        float wLwall = W.wLwall, walbwall = W.walbwall;
-        const float wwall = W.wwall, walbwallnosh = W.walbwallnosh;
-        const float s_wall = W.s_wall, s_Lwall = W.s_Lwall, s_Lupsh = W.s_Lupsh, s_albwall = W.s_albwall,
-                    s_albsh = W.s_albsh, s_albwallnosh = W.s_albwallnosh, s_albnosh = W.s_albnosh;
-        (void)wsh_;
-        const float wsi_f = s_wall > 0.f ? 1.f : 0.f;
-        const float wi_f = s_albwallnosh > 0.f ? 1.f : 0.f;
-        const float wsi_s = wwall > 0.f ? 1.f : 0.f;
-        const float wi_s = walbwallnosh > 0.f ? 1.f : 0.f;
+        const GvfWalk W = interior
+            ? gvf_walk<false>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], bld, second_i, snap_n)
+            : gvf_walk<true>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], bld, second_i, snap_n);
+        // the reference's weight sums
+        const float wwall = (float)W.m;
+        float wLwall = REP_L[W.m], walbwall = REP_A[W.m];
+        const float walbwallnosh = REP_A[W.m2];
+        const float s_wall = (float)W.qm, s_Lwall = REP_L[W.qm], s_albwall = REP_A[W.qm];
+        const float s_albwallnosh = REP_A[W.qm2];
+        const bool wsi_f = s_wall > 0.f, wi_f = s_albwallnosh > 0.f;
+        const bool wsi_s = wwall > 0.f, wi_s = walbwallnosh > 0.f;
         const float facesh = facesh_value(AZ[az].facesh_mode, AZ[az].facesh_lo, AZ[az].facesh_hi, aspect, wallbol);
         float keep = ((wwall == second) ? 1.f : 0.f) - facesh;
         if (keep == -1.f) keep = 0.f;
         const bool kz = keep == 1.f;
-        const float gLup1 = ((s_Lwall + s_Lupsh) / f1) * wsi_f + (s_Lupsh / first) * (1.f - wsi_f);
-        if (kz) wLwall = 0.f;
-        const float gLup2 = ((wLwall + wLupsh) / s1) * wsi_s + (wLupsh / second) * (1.f - wsi_s);
-        const float galb1 = ((s_albwall + s_albsh) / f1) * wsi_f + (s_albsh / first) * (1.f - wsi_f);
-        if (kz) walbwall = 0.f;
-        const float galb2 = ((walbwall + walbsh) / s1) * wsi_s + (walbsh / second) * (1.f - wsi_s);
-        const float gan1 = ((s_albwallnosh + s_albnosh) / f1) * wi_f + (s_albnosh / first) * (1.f - wi_f);
-        const float gan2 = ((walbwallnosh + walbnosh) / second) * wi_s + (walbnosh / second) * (1.f - wi_s);
+        if (kz) { wLwall = 0.f; walbwall = 0.f; }
+        const float gLup1 = pick_div(wsi_f, s_Lwall + W.qLup, f1, W.qLup, first);
+        const float gLup2 = pick_div(wsi_s, wLwall + W.sLup, s1, W.sLup, second);
+        const float galb1 = pick_div(wsi_f, s_albwall + W.qAlb, f1, W.qAlb, first);
+        const float galb2 = pick_div(wsi_s, walbwall + W.sAlb, s1, W.sAlb, second);
+        const float gan1 = pick_div(wi_f, s_albwallnosh + W.qNosh, f1, W.qNosh, first);
+        const float gan2 = pick_div(wi_s, walbwallnosh + W.sNosh, second, W.sNosh, second);
         const float gLup = (gLup1 * 0.5f + gLup2 * 0.4f) / 0.9f + lup_own * nb;
         const float galb = (galb1 * 0.5f + galb2 * 0.4f) / 0.9f + (alb * nb) * shadow;
         const float gan = ((gan1 * 0.5f + gan2 * 0.4f) / 0.9f) * bld + alb * nb;

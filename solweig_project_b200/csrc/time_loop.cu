@@ -148,12 +148,41 @@ __device__ __forceinline__ GvfWalk gvf_walk(const float4* __restrict__ G, size_t
   return W;
 }
 
+// x / d for a divisor shared by every pixel of a step, given rd, the
+// correctly rounded float32 reciprocal of d.  Markstein's theorem (IBM J.
+// Res. Dev. 34(1), 1990; Muller et al., Handbook of Floating-Point
+// Arithmetic, ch. 5): q = x * rd is within one ulp of x / d, the remainder
+// x - q * d is exact in one FMA, and q + r * rd rounded once is the
+// correctly rounded quotient -- the IEEE float32 x / d -- for operands in the
+// normal range.  Three instructions instead of a full division.
+__device__ __forceinline__ float div_by(float x, float d, float rd) {
+  const float q = __fmul_rn(x, rd);
+  const float r = __fmaf_rn(-q, d, x);
+  return __fmaf_rn(r, rd, q);
+}
+
+// Bits of the patches q0 .. q0 + 31 that exist (n_patches of them in all).
+__device__ __forceinline__ uint32_t patch_word_mask(int n_patches, int q0) {
+  const int n = n_patches - q0;
+  return n >= 32 ? 0xffffffffu : (n <= 0 ? 0u : ((1u << n) - 1u));
+}
+
+// Divisors of the walk epilogue, with their reciprocals.
+struct StepDiv {
+  float first, f1, second, s1, rfirst, rf1, rsecond, rs1;
+};
+
 // `x / d * sel + y / e * (1 - sel)` of the reference with sel in {0, 1}:
 // one of the two products is an exact zero, so only one quotient is needed
 // (the zero is still added, keeping the float32 result identical)
-__device__ __forceinline__ float pick_div(bool sel, float x, float d, float y, float e) {
-  return sel ? (x / d + 0.f) : (0.f + y / e);
+__device__ __forceinline__ float pick_div(bool sel, float x, float d, float rd, float y, float e, float re) {
+  return sel ? (div_by(x, d, rd) + 0.f) : (0.f + div_by(y, e, re));
 }
+
+// correctly rounded float32 reciprocals of 0.9f, 18 and 9
+constexpr float kR09 = 0x1.1c71c8p+0f;
+constexpr float kR18 = 0x1.c71c72p-5f;
+constexpr float kR9 = 0x1.c71c72p-4f;
 
 struct GvfSums {
   float Lup, alb, albnosh;
@@ -255,13 +284,21 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
       // ---------------- ground view factors (18 azimuths)
       GvfSums S = {};
       const int second_i = (int)P.second;
-      const float first = P.first, second = P.second;
-      const float f1 = first + 1.f, s1 = second + 1.f;
+      const float second = P.second;
+      StepDiv D;
+      D.first = P.first;
+      D.second = second;
+      D.f1 = P.first + 1.f;
+      D.s1 = second + 1.f;
+      D.rfirst = __frcp_rn(D.first);
+      D.rf1 = __frcp_rn(D.f1);
+      D.rsecond = __frcp_rn(D.second);
+      D.rs1 = __frcp_rn(D.s1);
       // a pixel at least `second - 1` pixels from every edge never walks out
       // of the grid: its walk needs no bounds test
       const int reach = second_i - 1;
       const bool interior = r >= reach && r < rows - reach && c >= reach && c < cols - reach;
-      const int first_i = (int)first;
+      const int first_i = (int)P.first;
       const int snap_n = min(first_i, second_i);  // snapshot after this many steps
       for (int az = 0; az < SW100_N_GVF_AZ; ++az) {
         const GvfWalk W = interior
@@ -280,15 +317,15 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
         if (keep == -1.f) keep = 0.f;
         const bool kz = keep == 1.f;
         if (kz) { wLwall = 0.f; walbwall = 0.f; }
-        const float gLup1 = pick_div(wsi_f, s_Lwall + W.qLup, f1, W.qLup, first);
-        const float gLup2 = pick_div(wsi_s, wLwall + W.sLup, s1, W.sLup, second);
-        const float galb1 = pick_div(wsi_f, s_albwall + W.qAlb, f1, W.qAlb, first);
-        const float galb2 = pick_div(wsi_s, walbwall + W.sAlb, s1, W.sAlb, second);
-        const float gan1 = pick_div(wi_f, s_albwallnosh + W.qNosh, f1, W.qNosh, first);
-        const float gan2 = pick_div(wi_s, walbwallnosh + W.sNosh, second, W.sNosh, second);
-        const float gLup = (gLup1 * 0.5f + gLup2 * 0.4f) / 0.9f + lup_own * nb;
-        const float galb = (galb1 * 0.5f + galb2 * 0.4f) / 0.9f + (alb * nb) * shadow;
-        const float gan = ((gan1 * 0.5f + gan2 * 0.4f) / 0.9f) * bld + alb * nb;
+        const float gLup1 = pick_div(wsi_f, s_Lwall + W.qLup, D.f1, D.rf1, W.qLup, D.first, D.rfirst);
+        const float gLup2 = pick_div(wsi_s, wLwall + W.sLup, D.s1, D.rs1, W.sLup, D.second, D.rsecond);
+        const float galb1 = pick_div(wsi_f, s_albwall + W.qAlb, D.f1, D.rf1, W.qAlb, D.first, D.rfirst);
+        const float galb2 = pick_div(wsi_s, walbwall + W.sAlb, D.s1, D.rs1, W.sAlb, D.second, D.rsecond);
+        const float gan1 = pick_div(wi_f, s_albwallnosh + W.qNosh, D.f1, D.rf1, W.qNosh, D.first, D.rfirst);
+        const float gan2 = pick_div(wi_s, walbwallnosh + W.sNosh, D.second, D.rsecond, W.sNosh, D.second, D.rsecond);
+        const float gLup = div_by(gLup1 * 0.5f + gLup2 * 0.4f, 0.9f, kR09) + lup_own * nb;
+        const float galb = div_by(galb1 * 0.5f + galb2 * 0.4f, 0.9f, kR09) + (alb * nb) * shadow;
+        const float gan = div_by(gan1 * 0.5f + gan2 * 0.4f, 0.9f, kR09) * bld + alb * nb;
         S.Lup = S.Lup + gLup;
         S.alb = S.alb + galb;
         S.albnosh = S.albnosh + gan;
@@ -299,12 +336,14 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
         if (df & 8) { S.LupN = S.LupN + gLup; S.albN = S.albN + galb; S.albnoshN = S.albnoshN + gan; }
       }
       const float lup_air = (P.sbc * emis) * P.ta4;
-      const float gvfLup = S.Lup / 18.f + lup_air;
-      const float gvfalb = S.alb / 18.f, gvfalbnosh = S.albnosh / 18.f;
-      const float gvfLupE = S.LupE / 9.f + lup_air, gvfLupS = S.LupS / 9.f + lup_air;
-      const float gvfLupW = S.LupW / 9.f + lup_air, gvfLupN = S.LupN / 9.f + lup_air;
-      const float gvfalbE = S.albE / 9.f, gvfalbS = S.albS / 9.f, gvfalbW = S.albW / 9.f, gvfalbN = S.albN / 9.f;
-      const float ganE = S.albnoshE / 9.f, ganS = S.albnoshS / 9.f, ganW = S.albnoshW / 9.f, ganN = S.albnoshN / 9.f;
+      const float gvfLup = div_by(S.Lup, 18.f, kR18) + lup_air;
+      const float gvfalb = div_by(S.alb, 18.f, kR18), gvfalbnosh = div_by(S.albnosh, 18.f, kR18);
+      const float gvfLupE = div_by(S.LupE, 9.f, kR9) + lup_air, gvfLupS = div_by(S.LupS, 9.f, kR9) + lup_air;
+      const float gvfLupW = div_by(S.LupW, 9.f, kR9) + lup_air, gvfLupN = div_by(S.LupN, 9.f, kR9) + lup_air;
+      const float gvfalbE = div_by(S.albE, 9.f, kR9), gvfalbS = div_by(S.albS, 9.f, kR9);
+      const float gvfalbW = div_by(S.albW, 9.f, kR9), gvfalbN = div_by(S.albN, 9.f, kR9);
+      const float ganE = div_by(S.albnoshE, 9.f, kR9), ganS = div_by(S.albnoshS, 9.f, kR9);
+      const float ganW = div_by(S.albnoshW, 9.f, kR9), ganN = div_by(S.albnoshN, 9.f, kR9);
       // ---------------- thermal lag (state in registers)
       const float tgtemp = tg * shadow + P.ta32;
       const float g0[6] = {gvfLup, gvfLupE, gvfLupS, gvfLupW, gvfLupN, tgtemp};
@@ -332,48 +371,79 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
       Lup = (P.sbc * emis) * pow4f(P.night_lup_base);
       LupE = LupS = LupW = LupN = Lup;
     }
-    // ---------------- 153-patch sums: Kside (day) and Lcyl pass 1
-    // (solweig.py:683-724 and 1514-1611).  The patch masks come from the bit
-    // cubes one 32-patch word at a time (the word loop is unrolled so the
-    // words stay in registers).
+    // ---------------- 153-patch sums: Kside (day) and Lcyl
+    // (solweig.py:683-724, 1514-1633).  Every sum is its own accumulator fed
+    // in patch order, so the patches are visited per sum: one dense pass for
+    // the sums that take (almost) every patch, and ascending set-bit walks
+    // of a per-pixel mask for the sums that take few.
     float ksideD = 0.f, kref_sun = 0.f, kref_sh = 0.f, kref_veg = 0.f, anilum = 0.f;
     float ld_sky = 0.f, ld_veg = 0.f, ld_sh = 0.f, ld_sun = 0.f, ld_ref = 0.f;
     float ls_sky = 0.f, ls_veg = 0.f, ls_sh = 0.f, ls_sun = 0.f, ls_ref = 0.f;
     const bool day = P.is_day != 0;
+    // dense: sky-visible longwave (sh == 1 & vegsh == 1); by day the diffuse
+    // Kside term and the anisotropic luminance, indexed by (sh, vegsh)
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
       const int nq = min(32, n_patches - q0);
-      const uint32_t sw = wsh[w], vw = wveg[w], bw = wvb[w], sgl = site.single_step[w];
-      for (int j = 0; j < nq; ++j) {
-        const sw100_patch_step& Q = PP[q0 + j];
-        const bool sh = (sw >> j) & 1u, veg = (vw >> j) & 1u;
-        const bool vb1 = (bw >> j) & 1u;                      // vbshvegsh == 1
-        const bool vb0 = !vb1 && !((sgl >> j) & 1u);          // vbshvegsh == 0
-        const bool tsh = !sh && vb1;                           // (1 - sh) * vb == 1
-        const bool tveg = !veg || vb0;
-        if (day) {
-          const int di = (sh ? 2 : 0) + (veg ? 1 : 0);
-          ksideD = ksideD + Q.kside_d[di];
-          anilum = anilum + Q.anilum[di];
-          if (tveg) kref_veg = kref_veg + Q.kref_veg;
-          if (tsh) {
-            const float td = hsvf + Q.yi_k;
-            if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
-            if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
+      const uint32_t sw = wsh[w], vw = wveg[w];
+      if (day) {
+        for (int j = 0; j < nq; ++j) {
+          const sw100_patch_step& Q = PP[q0 + j];
+          const bool sh = (sw >> j) & 1u, veg = (vw >> j) & 1u;
+          const float4 kd = *reinterpret_cast<const float4*>(Q.kside_d);
+          const float4 an = *reinterpret_cast<const float4*>(Q.anilum);
+          ksideD = ksideD + (sh ? (veg ? kd.w : kd.z) : (veg ? kd.y : kd.x));
+          anilum = anilum + (sh ? (veg ? an.w : an.z) : (veg ? an.y : an.x));
+          if (sh && veg) { ld_sky = ld_sky + Q.ld_sky; ls_sky = ls_sky + Q.ls_sky; }
+        }
+      } else {
+        for (int j = 0; j < nq; ++j) {
+          if ((sw >> j) & (vw >> j) & 1u) {
+            const sw100_patch_step& Q = PP[q0 + j];
+            ld_sky = ld_sky + Q.ld_sky;
+            ls_sky = ls_sky + Q.ls_sky;
           }
         }
-        if (sh && veg) { ld_sky = ld_sky + Q.ld_sky; ls_sky = ls_sky + Q.ls_sky; }
-        if (tveg) { ls_veg = add64(ls_veg, Q.veg_cos); ld_veg = add64(ld_veg, Q.veg_sin); }
-        if (tsh) {
-          if (Q.flags & 1) {
-            const float td = hsvf + Q.yi_l;
-            if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
-            if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
-          } else {
-            ls_sh = add64(ls_sh, Q.sh_cos);
-            ld_sh = add64(ld_sh, Q.sh_sin);
-          }
+      }
+    }
+    // vegetation-facing patches (vegsh == 0 or vbshvegsh == 0): vegetation
+    // longwave (float64 adds) and by day the vegetation-reflected Kside
+#pragma unroll
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+      const int q0 = w * 32;
+      uint32_t m = (~wveg[w] | (~wvb[w] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
+      while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1u;
+        const sw100_patch_step& Q = PP[q0 + j];
+        ls_veg = add64(ls_veg, Q.veg_cos);
+        ld_veg = add64(ld_veg, Q.veg_sin);
+        if (day) kref_veg = kref_veg + Q.kref_veg;
+      }
+    }
+    // wall-facing patches ((1 - sh) * vbshvegsh == 1): sunlit / shaded wall
+    // terms, split by the shaded_or_sunlit predicate
+#pragma unroll
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+      const int q0 = w * 32;
+      uint32_t m = ~wsh[w] & wvb[w] & patch_word_mask(n_patches, q0);
+      while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1u;
+        const sw100_patch_step& Q = PP[q0 + j];
+        if (day) {
+          const float td = hsvf + Q.yi_k;
+          if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
+          if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
+        }
+        if (Q.flags & 1) {
+          const float td = hsvf + Q.yi_l;
+          if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
+          if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
+        } else {
+          ls_sh = add64(ls_sh, Q.sh_cos);
+          ld_sh = add64(ld_sh, Q.sh_sin);
         }
       }
     }
@@ -383,20 +453,19 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
       Kdown = ((P.radI * shadow) * P.sin_alt + dRad) + albF_day;
     }
     // ---------------- Lcyl pass 2: reflected longwave (solweig.py:1613-1633)
+    // over temp_sh = (sh == 0) | (vegsh == 0) | (vbshvegsh == 0)
     const float refl = (((ld_sky + Lup) * P.refl_k) * 0.5f) / 3.14159274101257324f;
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
-      const int nq = min(32, n_patches - q0);
-      // temp_sh = (sh == 0) | (vegsh == 0) | (vbshvegsh == 0)
-      const uint32_t any0 = ~wsh[w] | ~wveg[w] | (~wvb[w] & ~site.single_step[w]);
-      for (int j = 0; j < nq; ++j) {
-        if ((any0 >> j) & 1u) {
-          const sw100_patch_step& Q = PP[q0 + j];
-          const float rs = refl * Q.ster;
-          ls_ref = ls_ref + rs * Q.cos_alt;
-          ld_ref = ld_ref + rs * Q.sin_alt;
-        }
+      uint32_t m = (~wsh[w] | ~wveg[w] | (~wvb[w] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
+      while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1u;
+        const sw100_patch_step& Q = PP[q0 + j];
+        const float rs = refl * Q.ster;
+        ls_ref = ls_ref + rs * Q.cos_alt;
+        ld_ref = ld_ref + rs * Q.sin_alt;
       }
     }
     const float Lside = (((ls_sky + ls_veg) + ls_sh) + ls_sun) + ls_ref;

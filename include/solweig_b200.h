@@ -134,6 +134,55 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
                     const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
                     void* workspace, int64_t workspace_bytes, void* stream);
 
+/* ------------------------------------------- windowed SVF recompute -- */
+/* Corridor descriptor of one patch for sw100_svf_window (one int32 per
+ * patch, built by the host from the step table): bits 0-1 the axis of the
+ * patch's major shift (0 = rows / dx, 1 = cols / dy), which is
+ * +-(k + 1) at step k, with the minor shift moving by at most one cell per
+ * step in one direction; bit 2 set when the major shift is negative.
+ * SW100_CORRIDOR_LOCAL marks a patch whose result does not depend on the
+ * heights it reads (every step drops the source by more than twice the
+ * largest |height|): only pixels inside the edit re-march it.
+ * SW100_CORRIDOR_ALWAYS marks a patch whose table has neither form: every
+ * window pixel re-marches it. */
+#define SW100_CORRIDOR_LOCAL 2
+#define SW100_CORRIDOR_ALWAYS 3
+
+/* Exact SVF recompute of a window after an edit of the march rasters.
+ *
+ * Replaces the corridor-closure work of the reference's incremental exact
+ * march (solweig_core/sparse_work.py:633-781 build_sparse_work: per patch,
+ * D_p = C u {t : t + d in C} over the executed step offsets d) for one
+ * edited rectangle.  `site` holds the edited (post) rasters; `planes` and
+ * `bits` hold the sweep result of the rasters before the edit and are
+ * updated in place.  rect = {r0, r1, c0, c1} (inclusive) bounds every
+ * changed cell; window = {r0, r1, c0, c1} (inclusive, inside the grid) must
+ * contain every pixel within the patches' largest shift of the rectangle
+ * (pixels outside it cannot reach the rectangle).  Each window pixel
+ * re-marches the patches whose march reads the rectangle, keeps the stored
+ * bits of the others and re-accumulates its 19 planes in the sweep's
+ * order, so the result equals sw100_svf_sweep on the edited rasters bit for
+ * bit.  The plan and step tables must be those of the edited rasters and
+ * identical to the tables of the stored result (same rows, cols, scale and
+ * amaxvalue); rasters with bush (plan bush flag set, before or after the
+ * edit) are refused with SW100_E_ARG: their whole-grid step flags change
+ * with any edit.  Workspace: sw100_svf_window_workspace_bytes. */
+int sw100_svf_window_workspace_bytes(int rows, int cols, int64_t* bytes);
+int sw100_svf_window(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                     const sw100_step* steps, int n_steps, const int32_t* corridor, const int32_t rect[4],
+                     const int32_t window[4], float* planes, uint32_t* bits, void* workspace,
+                     int64_t workspace_bytes, void* stream);
+
+/* Bounding box of the cells whose march rasters (dsm, vegdsm, vegdsm2,
+ * bush) differ between two sites of the same grid, bit for bit (the
+ * composed-source diff C of solweig_core/sparse_work.py:199-251).  Writes
+ * {rmin, rmax, cmin, cmax} to the 4 int32 of device memory `box`;
+ * rmax = -1 when nothing differs.  Workspace:
+ * sw100_diff_bbox_workspace_bytes. */
+int sw100_diff_bbox_workspace_bytes(int rows, int cols, int64_t* bytes);
+int sw100_diff_bbox(const sw100_site_planes* before, const sw100_site_planes* after, int rows, int cols,
+                    int32_t* box, void* workspace, int64_t workspace_bytes, void* stream);
+
 /* Pack dense patch cubes (rows, cols, n_patches) float32, as the reference
  * returns and caches them (shadow.py:625, utci_process.py:347-394), into the
  * 3 bit cubes the time loop reads.  `single_step` (host, SW100_CUBE_WORDS

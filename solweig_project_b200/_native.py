@@ -33,7 +33,10 @@ OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDO
 # Exported symbols (checked by the CPU tests against include/solweig_b200.h)
 SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noalloc", "sw100_pack_cubes", "sw100_sun_march_workspace_bytes",
            "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop", "sw100_flux_loop", "sw100_utci",
-           "sw100_abi_version", "sw100_last_error", "sw100_launch_count")
+           "sw100_abi_version", "sw100_last_error", "sw100_launch_count", "sw100_svf_window_workspace_bytes",
+           "sw100_svf_window", "sw100_diff_bbox_workspace_bytes", "sw100_diff_bbox")
+CORRIDOR_LOCAL = 2
+CORRIDOR_ALWAYS = 3
 
 
 class NativeUnavailable(RuntimeError):
@@ -153,6 +156,12 @@ def load(path: str = LIB_PATH):
         "sw100_flux_loop": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, C.c_uint32,
                                       vp, vp]),
         "sw100_utci": (C.c_int, [vp, vp, vp, vp, C.c_int64, vp, vp]),
+        "sw100_svf_window_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
+        "sw100_svf_window": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp,
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_int32), vp, vp, vp, C.c_int64, vp]),
+        "sw100_diff_bbox_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
+        "sw100_diff_bbox": (C.c_int, [C.POINTER(SitePlanes), C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp,
+                                      C.c_int64, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

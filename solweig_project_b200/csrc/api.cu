@@ -5,6 +5,7 @@
 // allocates: every scratch buffer comes from the caller's workspace, so the
 // entry points can be captured in CUDA graphs and driven from any allocator.
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -20,6 +21,11 @@ __global__ void pack4_kernel(const float* a, const float* b, const float* c, con
 __global__ void svf_sweep_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                  const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
                                  uint32_t* bits);
+__global__ void svf_window_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
+                                  const sw100_step* steps, const int32_t* corridor, float vmax, int4 rect, int4 win,
+                                  float* out, uint32_t* bits);
+__global__ void diff_bbox_kernel(const float4* a, const float4* b, int rows, int cols, int* box);
+__global__ void box_init_kernel(int* box);
 __global__ void svf_bush_flags_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
                                       const sw100_step* steps, uint32_t* flags);
 __global__ void sun_march_kernel(const float4* src4, SitePlanes site, int rows, int cols,
@@ -186,6 +192,77 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
   svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
                                            site->vmax, out_planes, out_bits);
   return check_launch("svf_sweep_kernel");
+}
+
+int sw100_svf_window_workspace_bytes(int rows, int cols, int64_t* bytes) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(bytes, "bytes"))) return rc;
+  *bytes = align_up((int64_t)rows * cols * 16);
+  return 0;
+}
+
+int sw100_svf_window(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                     const sw100_step* steps, int n_steps, const int32_t* corridor, const int32_t rect[4],
+                     const int32_t window[4], float* planes, uint32_t* bits, void* workspace,
+                     int64_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_march(site))) return rc;
+  if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(corridor, "corridor")) ||
+      (rc = check_ptr(rect, "rect")) || (rc = check_ptr(window, "window")) || (rc = check_ptr(planes, "planes")) ||
+      (rc = check_ptr(bits, "bits")))
+    return rc;
+  if (site->bush_any) return fail(SW100_E_ARG, "windowed recompute refuses rasters with bush");
+  if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
+  const int w0 = window[0], w1 = window[1], w2 = window[2], w3 = window[3];
+  if (w0 < 0 || w1 >= rows || w2 < 0 || w3 >= cols || w0 > w1 || w2 > w3)
+    return fail(SW100_E_ARG, "window {%d, %d, %d, %d} must be a non-empty box inside the %d x %d grid", w0, w1, w2,
+                w3, rows, cols);
+  if (rect[0] > rect[1] || rect[2] > rect[3]) return fail(SW100_E_ARG, "rect must be non-empty");
+  int64_t need = 0;
+  if ((rc = sw100_svf_window_workspace_bytes(rows, cols, &need))) return rc;
+  if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* src4 = static_cast<float4*>(workspace);
+  if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
+  dim3 block(32, 4);
+  dim3 grid((w3 - w2 + 1 + 31) / 32, (w1 - w0 + 1 + 3) / 4);
+  svf_window_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, corridor, site->vmax,
+                                            make_int4(rect[0], rect[1], rect[2], rect[3]),
+                                            make_int4(w0, w1, w2, w3), planes, bits);
+  return check_launch("svf_window_kernel");
+}
+
+int sw100_diff_bbox_workspace_bytes(int rows, int cols, int64_t* bytes) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(bytes, "bytes"))) return rc;
+  *bytes = 2 * align_up((int64_t)rows * cols * 16);
+  return 0;
+}
+
+int sw100_diff_bbox(const sw100_site_planes* before, const sw100_site_planes* after, int rows, int cols,
+                    int32_t* box, void* workspace, int64_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_march(before)) || (rc = validate_site_march(after))) return rc;
+  if ((rc = check_ptr(box, "box"))) return rc;
+  int64_t need = 0;
+  if ((rc = sw100_diff_bbox_workspace_bytes(rows, cols, &need))) return rc;
+  if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* a = static_cast<float4*>(workspace);
+  float4* b = reinterpret_cast<float4*>(static_cast<char*>(workspace) + align_up((int64_t)rows * cols * 16));
+  if ((rc = launch_pack(*before, rows, cols, a, st))) return rc;
+  if ((rc = launch_pack(*after, rows, cols, b, st))) return rc;
+  box_init_kernel<<<1, 32, 0, st>>>(box);
+  if ((rc = check_launch("box_init_kernel"))) return rc;
+  const size_t n = (size_t)rows * cols;
+  const int threads = 256;
+  const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 8);
+  diff_bbox_kernel<<<blocks, threads, 0, st>>>(a, b, rows, cols, box);
+  return check_launch("diff_bbox_kernel");
 }
 
 int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbshvegshmat, int rows, int cols,

@@ -13,6 +13,7 @@
 // (patch-major, annulus-minor), so the sums are bit-identical; the three
 // patch masks are packed into 5-word bit cubes per pixel (60 B/px instead of
 // the reference's 1836 B/px of float cubes).
+#include <climits>
 #include <cmath>
 
 #include "sw_common.cuh"
@@ -156,69 +157,50 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
   vb_out = 1.f - ((vb_any ? 1.f : 0.f) - vegf);
 }
 
-__global__ void __launch_bounds__(128) svf_sweep_kernel(
-    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
-    const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
-    float* __restrict__ out, uint32_t* __restrict__ bits) {
-  __shared__ sw100_svf_plan plan;
-  {
-    const int* s = reinterpret_cast<const int*>(plan_g);
-    int* d = reinterpret_cast<int*>(&plan);
-    const int nw = sizeof(sw100_svf_plan) / 4;
-    for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < nw; i += blockDim.x * blockDim.y) d[i] = s[i];
+// Adds patch q's (sh, vegsh, vbshvegsh) to the 15 SVF sums in the
+// reference's order: annulus by annulus, each direction sum after the
+// isotropic one (shadow.py:560-585).
+__device__ __forceinline__ void svf_add_patch(SvfAcc& A, const sw100_svf_plan& plan, int q, float sh, float veg,
+                                              float vb) {
+  const int ring = plan.ring[q];
+  const int fl = plan.dir_flags[q];
+  const int na = plan.ring_annuli[ring];
+  for (int k = 0; k < na; ++k) {
+    const float wi = plan.w_iso[ring][k];
+    const float wa = plan.w_aniso[ring][k];
+    A.svf = A.svf + wi * sh;
+    const float wsh_ = wa * sh;
+    if (fl & 1) A.svfE = A.svfE + wsh_;
+    if (fl & 2) A.svfS = A.svfS + wsh_;
+    if (fl & 4) A.svfW = A.svfW + wsh_;
+    if (fl & 8) A.svfN = A.svfN + wsh_;
+    A.veg = A.veg + wi * veg;
+    A.aveg = A.aveg + wi * vb;
+    const float wv = wa * veg, wb = wa * vb;
+    if (fl & 1) { A.vegE = A.vegE + wv; A.avegE = A.avegE + wb; }
+    if (fl & 2) { A.vegS = A.vegS + wv; A.avegS = A.avegS + wb; }
+    if (fl & 4) { A.vegW = A.vegW + wv; A.avegW = A.avegW + wb; }
+    if (fl & 8) { A.vegN = A.vegN + wv; A.avegN = A.avegN + wb; }
   }
-  __syncthreads();
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
-  if (r >= rows || c >= cols) return;
-  const size_t npix = (size_t)rows * cols;
-  const size_t p = (size_t)r * cols + c;
-  const float4 self = src4[p];
-  const float a = self.x, veg2_p = self.z, bush_p = self.w;
-  const bool bush_any = plan.bush_any != 0;
-  const bool fast = plan.all_finite != 0 && !(bush_any && bush_p > 1.f);
+}
 
-  SvfAcc A = {};
-  uint32_t wsh[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
-  uint32_t wveg[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
-  uint32_t wvb[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+// Patch bits of one march result.  Marches of at most one step leave
+// vbshvegsh in {1, 2}: their bit keeps "== 1"; every other patch keeps
+// "!= 0" (values {0, 1}).
+__device__ __forceinline__ void svf_set_bits(uint32_t* wsh, uint32_t* wveg, uint32_t* wvb, int q, int n, float sh,
+                                             float veg, float vb) {
+  const uint32_t bit = 1u << (q & 31);
+  if (sh != 0.f) wsh[q >> 5] |= bit;
+  if (veg != 0.f) wveg[q >> 5] |= bit;
+  if (n <= 1 ? (vb == 1.f) : (vb != 0.f)) wvb[q >> 5] |= bit;
+}
 
-  for (int q = 0; q < plan.n_patches; ++q) {
-    const int off = plan.step_offset[q];
-    float sh, veg, vb;
-    if (fast)
-      march_patch_fast(src4, rows, cols, r, c, a, veg2_p, steps + off, plan.step_count[q], vmax, sh, veg, vb);
-    else
-      march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, plan.step_count[q],
-                  bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);
-    const uint32_t bit = 1u << (q & 31);
-    if (sh != 0.f) wsh[q >> 5] |= bit;
-    if (veg != 0.f) wveg[q >> 5] |= bit;
-    // marches of at most one step leave vbshvegsh in {1, 2}: their bit keeps
-    // "== 1"; every other patch keeps "!= 0" (values {0, 1})
-    if (plan.step_count[q] <= 1 ? (vb == 1.f) : (vb != 0.f)) wvb[q >> 5] |= bit;
-    const int ring = plan.ring[q];
-    const int fl = plan.dir_flags[q];
-    const int na = plan.ring_annuli[ring];
-    for (int k = 0; k < na; ++k) {
-      const float wi = plan.w_iso[ring][k];
-      const float wa = plan.w_aniso[ring][k];
-      A.svf = A.svf + wi * sh;
-      const float wsh_ = wa * sh;
-      if (fl & 1) A.svfE = A.svfE + wsh_;
-      if (fl & 2) A.svfS = A.svfS + wsh_;
-      if (fl & 4) A.svfW = A.svfW + wsh_;
-      if (fl & 8) A.svfN = A.svfN + wsh_;
-      A.veg = A.veg + wi * veg;
-      A.aveg = A.aveg + wi * vb;
-      const float wv = wa * veg, wb = wa * vb;
-      if (fl & 1) { A.vegE = A.vegE + wv; A.avegE = A.avegE + wb; }
-      if (fl & 2) { A.vegS = A.vegS + wv; A.avegS = A.avegS + wb; }
-      if (fl & 4) { A.vegW = A.vegW + wv; A.avegW = A.avegW + wb; }
-      if (fl & 8) { A.vegN = A.vegN + wv; A.avegN = A.avegN + wb; }
-    }
-  }
-  // tails and clamps (shadow.py:587-613)
+// Tails, clamps (shadow.py:587-613), the 16 SVF planes, the three
+// time-loop statics and the bit cubes of pixel p.
+__device__ __forceinline__ void svf_finish(SvfAcc& A, const sw100_svf_plan& plan, float veg2_p, size_t p,
+                                           size_t npix, const uint32_t* wsh, const uint32_t* wveg,
+                                           const uint32_t* wvb, float* __restrict__ out,
+                                           uint32_t* __restrict__ bits) {
   const float tail = plan.tail;
   A.svfS = A.svfS + tail;
   A.svfW = A.svfW + tail;
@@ -233,8 +215,8 @@ __global__ void __launch_bounds__(128) svf_sweep_kernel(
   clamp1(A.aveg); clamp1(A.avegE); clamp1(A.avegS); clamp1(A.avegW); clamp1(A.avegN);
   const float total = A.svf - (1.f - A.veg) * (1.f - plan.trans);
   // reference tuple order (shadow.py:625) without the cubes, then SVFtotal
-  const float vals[SW100_SVF_PLANES] = {A.svf,  A.aveg,  A.svfE, A.avegE, A.vegE, A.svfN, A.avegN, A.vegN,
-                                        A.svfS, A.avegS, A.vegS, A.veg,   A.svfW, A.avegW, A.vegW, total};
+  const float vals[16] = {A.svf,  A.aveg,  A.svfE, A.avegE, A.vegE, A.svfN, A.avegN, A.vegN,
+                          A.svfS, A.avegS, A.vegS, A.veg,   A.svfW, A.avegW, A.vegW, total};
 #pragma unroll
   for (int k = 0; k < 16; ++k) out[k * npix + p] = vals[k];
   // time-loop statics (utci_process.py:864-897): every float32 operation of
@@ -254,6 +236,169 @@ __global__ void __launch_bounds__(128) svf_sweep_kernel(
     bits[(0 * SW100_CUBE_WORDS + w) * npix + p] = wsh[w];
     bits[(1 * SW100_CUBE_WORDS + w) * npix + p] = wveg[w];
     bits[(2 * SW100_CUBE_WORDS + w) * npix + p] = wvb[w];
+  }
+}
+
+__device__ __forceinline__ void load_plan(const sw100_svf_plan* __restrict__ plan_g, sw100_svf_plan& plan) {
+  const int* s = reinterpret_cast<const int*>(plan_g);
+  int* d = reinterpret_cast<int*>(&plan);
+  const int nw = sizeof(sw100_svf_plan) / 4;
+  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < nw; i += blockDim.x * blockDim.y) d[i] = s[i];
+}
+
+__global__ void __launch_bounds__(128) svf_sweep_kernel(
+    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
+    const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
+    float* __restrict__ out, uint32_t* __restrict__ bits) {
+  __shared__ sw100_svf_plan plan;
+  load_plan(plan_g, plan);
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  if (r >= rows || c >= cols) return;
+  const size_t npix = (size_t)rows * cols;
+  const size_t p = (size_t)r * cols + c;
+  const float4 self = src4[p];
+  const float a = self.x, veg2_p = self.z, bush_p = self.w;
+  const bool bush_any = plan.bush_any != 0;
+  const bool fast = plan.all_finite != 0 && !(bush_any && bush_p > 1.f);
+
+  SvfAcc A = {};
+  uint32_t wsh[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+  uint32_t wveg[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+  uint32_t wvb[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+
+  for (int q = 0; q < plan.n_patches; ++q) {
+    const int off = plan.step_offset[q];
+    const int n = plan.step_count[q];
+    float sh, veg, vb;
+    if (fast)
+      march_patch_fast(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb);
+    else
+      march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, n,
+                  bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);
+    svf_set_bits(wsh, wveg, wvb, q, n, sh, veg, vb);
+    svf_add_patch(A, plan, q, sh, veg, vb);
+  }
+  svf_finish(A, plan, veg2_p, p, npix, wsh, wveg, wvb, out, bits);
+}
+
+// Does the march of pixel (tr, tc) along this patch's steps read a cell of
+// the edited rectangle [r0, r1] x [c0, c1], or is the pixel inside it?
+// The patch's major shift is s * (k + 1) at step k along one axis and its
+// minor shift moves by at most one cell per step, monotonically (checked on
+// the host, which marks any other patch `SW100_CORRIDOR_ALWAYS`, and a
+// patch whose result does not depend on the heights it reads
+// `SW100_CORRIDOR_LOCAL`).  The steps
+// whose major shift lands in the rectangle's band form one interval
+// [ka, kb]; the minor shifts over it cover every integer between the
+// interval's end values, so the test needs two step reads.
+__device__ __forceinline__ bool svf_in_corridor(int tr, int tc, const sw100_step* __restrict__ st, int n,
+                                                int desc, int r0, int r1, int c0, int c1) {
+  if (tr >= r0 && tr <= r1 && tc >= c0 && tc <= c1) return true;
+  const int axis = desc & 3;
+  if (n <= 0 || axis == SW100_CORRIDOR_LOCAL) return false;
+  if (axis == SW100_CORRIDOR_ALWAYS) return true;
+  const bool neg = (desc & 4) != 0;
+  const int tM = axis == 0 ? tr : tc, lo = axis == 0 ? r0 : c0, hi = axis == 0 ? r1 : c1;
+  const int tm = axis == 0 ? tc : tr, mlo = axis == 0 ? c0 : r0, mhi = axis == 0 ? c1 : r1;
+  int ka = neg ? tM - hi : lo - tM;  // range of k + 1
+  int kb = neg ? tM - lo : hi - tM;
+  ka = max(ka, 1);
+  kb = min(kb, n);
+  if (ka > kb) return false;
+  const sw100_step sa = load_step(&st[ka - 1]), sb = load_step(&st[kb - 1]);
+  const int ma = axis == 0 ? sa.dy : sa.dx, mb = axis == 0 ? sb.dy : sb.dx;
+  return tm + max(ma, mb) >= mlo && tm + min(ma, mb) <= mhi;
+}
+
+// Windowed exact recompute after an edit of the march rasters inside the
+// rectangle `rect` = (r0, r1, c0, c1), inclusive.  Pixels of `win` re-march
+// only the patches whose march reads the rectangle (or that start in it),
+// keep the stored bits of every other patch, and re-accumulate all sums in
+// the sweep's order: the result equals a full sweep of the edited rasters
+// bit for bit.  Pixels outside `win` are not touched (no march of theirs
+// reaches the rectangle).  Bush rasters are excluded by the host (their
+// whole-grid step flags would change).
+__global__ void __launch_bounds__(128) svf_window_kernel(
+    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
+    const sw100_step* __restrict__ steps, const int32_t* __restrict__ corridor, float vmax, int4 rect, int4 win,
+    float* __restrict__ out, uint32_t* __restrict__ bits) {
+  __shared__ sw100_svf_plan plan;
+  load_plan(plan_g, plan);
+  __syncthreads();
+  const int c = win.z + blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = win.x + blockIdx.y * blockDim.y + threadIdx.y;
+  if (r > win.y || c > win.w) return;
+  const size_t npix = (size_t)rows * cols;
+  const size_t p = (size_t)r * cols + c;
+  const float4 self = src4[p];
+  const float a = self.x, veg2_p = self.z;
+  const bool fast = plan.all_finite != 0;
+
+  uint32_t osh[SW100_CUBE_WORDS], oveg[SW100_CUBE_WORDS], ovb[SW100_CUBE_WORDS];
+#pragma unroll
+  for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+    osh[w] = bits[(0 * SW100_CUBE_WORDS + w) * npix + p];
+    oveg[w] = bits[(1 * SW100_CUBE_WORDS + w) * npix + p];
+    ovb[w] = bits[(2 * SW100_CUBE_WORDS + w) * npix + p];
+  }
+  SvfAcc A = {};
+  uint32_t wsh[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+  uint32_t wveg[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+  uint32_t wvb[SW100_CUBE_WORDS] = {0, 0, 0, 0, 0};
+  for (int q = 0; q < plan.n_patches; ++q) {
+    const int off = plan.step_offset[q];
+    const int n = plan.step_count[q];
+    float sh, veg, vb;
+    if (svf_in_corridor(r, c, steps + off, n, corridor[q], rect.x, rect.y, rect.z, rect.w)) {
+      if (fast)
+        march_patch_fast(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb);
+      else
+        march_patch(src4, rows, cols, r, c, a, veg2_p, 0.f, steps + off, n, nullptr, false, vmax, sh, veg, vb);
+    } else {
+      const uint32_t bit = 1u << (q & 31);
+      const int w = q >> 5;
+      sh = (osh[w] & bit) ? 1.f : 0.f;
+      veg = (oveg[w] & bit) ? 1.f : 0.f;
+      vb = (ovb[w] & bit) ? 1.f : (n <= 1 ? 2.f : 0.f);
+    }
+    svf_set_bits(wsh, wveg, wvb, q, n, sh, veg, vb);
+    svf_add_patch(A, plan, q, sh, veg, vb);
+  }
+  svf_finish(A, plan, veg2_p, p, npix, wsh, wveg, wvb, out, bits);
+}
+
+__global__ void box_init_kernel(int* box) {
+  if (threadIdx.x == 0) {
+    box[0] = INT_MAX; box[1] = -1; box[2] = INT_MAX; box[3] = -1;
+  }
+}
+
+// Bounding box of the cells where two packed march sources differ (bit
+// comparison of all four channels); box = {rmin, rmax, cmin, cmax}, set to
+// {INT_MAX, -1, INT_MAX, -1} by the caller.
+__global__ void diff_bbox_kernel(const float4* __restrict__ a, const float4* __restrict__ b, int rows, int cols,
+                                 int* __restrict__ box) {
+  const size_t n = (size_t)rows * cols;
+  int rmin = INT_MAX, rmax = -1, cmin = INT_MAX, cmax = -1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int4 x = reinterpret_cast<const int4*>(a)[i];
+    const int4 y = reinterpret_cast<const int4*>(b)[i];
+    if (x.x != y.x || x.y != y.y || x.z != y.z || x.w != y.w) {
+      const int r = (int)(i / cols), c = (int)(i % cols);
+      rmin = min(rmin, r); rmax = max(rmax, r); cmin = min(cmin, c); cmax = max(cmax, c);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+    rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+    cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+    cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  }
+  if ((threadIdx.x & 31) == 0 && rmax >= 0) {
+    atomicMin(&box[0], rmin); atomicMax(&box[1], rmax);
+    atomicMin(&box[2], cmin); atomicMax(&box[3], cmax);
   }
 }
 

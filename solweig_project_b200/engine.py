@@ -130,10 +130,9 @@ class DeviceSite:
         if self.rows * self.cols >= 2 ** 31:
             raise ValueError("grid too large")
         vegdsm, vegdsm2, bush, amax, buildings = march_inputs(a, trees, dem)
+        self.amax_fixed = amaxvalue is not None
         self.amax = F32(amaxvalue) if amaxvalue is not None else amax
-        self.bush_any = bool(bush.max() > 0)
-        self.vmax = F32(max(a.max(), vegdsm.max(), vegdsm2.max()))
-        self.all_finite = bool(np.isfinite(a).all() and np.isfinite(vegdsm).all() and np.isfinite(vegdsm2).all())
+        self._set_march_stats(a, vegdsm, vegdsm2, bush)
         self.scale = float(scale)
         d = self.device
         self.t = {
@@ -166,9 +165,8 @@ class DeviceSite:
         vegdsm2 = np.asarray(vegdsm2, F32)
         bush = np.asarray(bush, F32)
         self.amax = F32(amaxvalue)
-        self.bush_any = bool(bush.max() > 0)
-        self.vmax = F32(max(a.max(), vegdsm.max(), vegdsm2.max()))
-        self.all_finite = bool(np.isfinite(a).all() and np.isfinite(vegdsm).all() and np.isfinite(vegdsm2).all())
+        self.amax_fixed = True
+        self._set_march_stats(a, vegdsm, vegdsm2, bush)
         self.scale = float(scale)
         d = self.device
         self.t = {"dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
@@ -179,6 +177,12 @@ class DeviceSite:
         self._keep = []
         self._cache = {}
         return self
+
+    def _set_march_stats(self, a, vegdsm, vegdsm2, bush):
+        self.bush_any = bool(bush.max() > 0)
+        self.vmax = F32(max(a.max(), vegdsm.max(), vegdsm2.max()))
+        self.all_finite = bool(np.isfinite(a).all() and np.isfinite(vegdsm).all() and np.isfinite(vegdsm2).all())
+        self.hmax = float(max(np.abs(a).max(), np.abs(vegdsm).max(), np.abs(vegdsm2).max()))
 
     # --------------------------------------------------------------- SVF
     def site_struct(self) -> N.SitePlanes:
@@ -208,7 +212,76 @@ class DeviceSite:
             ws_bytes = N.workspace_bytes("sw100_svf_workspace_bytes", self.rows, self.cols, len(steps))
             self._cache[key] = (_table(plan, d), _table(steps, d), len(steps), single,
                                 torch.empty(ws_bytes, dtype=torch.uint8, device=d))
+            self._cache[("svf_host", patch_option)] = (plan, steps)
         return self._cache[key]
+
+    def edit_svf(self, dsm, trees, dem, walls=None, aspect_deg=None, patch_option=2) -> dict:
+        """Exact SVF update after an edit of the rasters: the new march
+        rasters are diffed against the current ones on the device, and only
+        the pixels whose marches can read the changed box re-march, only the
+        patches that do (the corridor closure of the reference's incremental
+        exact march, solweig_core/sparse_work.py:633-781, spliced into the
+        stored result as incremental/solver.py:861-1135 does).  The planes
+        and bits equal a full sweep of the new rasters bit for bit.  A full
+        sweep runs instead when the step tables would change (a new
+        amaxvalue), when either scene has bush, or when a raster holds a
+        non-finite value.  Returns {"mode": "window" | "full" | "none",
+        "rect", "window", "pixels"}."""
+        if self.svf_result is None:
+            raise RuntimeError("run_svf() (or set_svf()) must come before edit_svf()")
+        a = np.asarray(dsm, F32)
+        if a.shape != (self.rows, self.cols):
+            raise ValueError(f"edited rasters must keep the grid shape {(self.rows, self.cols)}")
+        vegdsm, vegdsm2, bush, amax, buildings = march_inputs(a, trees, dem)
+        new_amax = self.amax if self.amax_fixed else amax
+        old = {k: self.t[k] for k in ("dsm", "vegdsm", "vegdsm2", "bush")}
+        old_site = self.site_struct()
+        old_bush, old_hmax = self.bush_any, self.hmax
+        d = self.device
+        self.t.update(dsm=_dev(a, d), vegdsm=_dev(vegdsm, d), vegdsm2=_dev(vegdsm2, d),
+                      bush=_dev(bush, d) if bush.max() > 0 else None, buildings=_dev(buildings, d))
+        if walls is not None:
+            self.t["walls"] = _dev(np.asarray(walls, F32), d)
+        if aspect_deg is not None:
+            self.t["aspect_rad"] = _dev((np.asarray(aspect_deg, F32) * F32(np.pi)) / F32(180.), d)
+        self._set_march_stats(a, vegdsm, vegdsm2, bush)
+        if old_bush or self.bush_any or new_amax != self.amax or not self.all_finite:
+            self.amax = new_amax
+            self._cache = {k: v for k, v in self._cache.items() if k[0] not in ("svf", "svf_host")}
+            self.run_svf(patch_option)
+            return {"mode": "full", "rect": None, "window": (0, self.rows - 1, 0, self.cols - 1),
+                    "pixels": self.rows * self.cols}
+        new_site = self.site_struct()
+        key = ("diff_ws",)
+        ws_bytes = N.workspace_bytes("sw100_diff_bbox_workspace_bytes", self.rows, self.cols)
+        if key not in self._cache:
+            self._cache[key] = (torch.empty(ws_bytes, dtype=torch.uint8, device=d),
+                                torch.empty(4, dtype=torch.int32, device=d))
+        ws, box = self._cache[key]
+        N.call("sw100_diff_bbox", C.byref(old_site), C.byref(new_site), self.rows, self.cols, _ptr(box), _ptr(ws),
+               ws.numel(), _stream())
+        rect = tuple(int(v) for v in box.cpu().tolist())
+        del old
+        if rect[1] < 0:
+            return {"mode": "none", "rect": None, "window": None, "pixels": 0}
+        plan_d, steps_d, n_steps, _, _ = self.svf_tables(patch_option)
+        plan, steps = self._cache[("svf_host", patch_option)]
+        desc = T.svf_corridor(plan, steps, max(old_hmax, self.hmax))
+        window = T.edit_window(rect, plan, steps, desc, self.rows, self.cols)
+        key = ("window_ws",)
+        if key not in self._cache:
+            self._cache[key] = torch.empty(N.workspace_bytes("sw100_svf_window_workspace_bytes", self.rows,
+                                                             self.cols), dtype=torch.uint8, device=d)
+        wws = self._cache[key]
+        desc_d = _upload(torch.from_numpy(desc), d)
+        r = self.svf_result
+        N.call("sw100_svf_window", C.byref(new_site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), n_steps,
+               _ptr(desc_d), (C.c_int32 * 4)(*rect), (C.c_int32 * 4)(*window), _ptr(r.planes), _ptr(r.bits),
+               _ptr(wws), wws.numel(), _stream())
+        self._keep = [desc_d]
+        self._prepare_loop_statics()
+        return {"mode": "window", "rect": rect, "window": window,
+                "pixels": (window[1] - window[0] + 1) * (window[3] - window[2] + 1)}
 
     def launch_svf(self, planes, bits, patch_option=2):
         """The sweep alone into caller buffers (no host work once the tables

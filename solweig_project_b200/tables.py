@@ -262,6 +262,86 @@ def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03, 
     return plan, steps, single
 
 
+# ------------------------------------------- windowed SVF recompute
+def svf_corridor(plan: np.ndarray, steps: np.ndarray, height_bound: float):
+    """Corridor descriptors of the windowed recompute, one int32 per patch.
+
+    A patch whose step k shifts by s * (k + 1) along one axis (its major
+    axis) and whose other shift changes by at most one cell per step, in one
+    direction, gets ``axis | (4 if s < 0)``.  A patch whose every step drops
+    the source by more than twice ``height_bound`` (the largest |height| of
+    the march rasters before and after the edit) gets ``CORRIDOR_LOCAL``:
+    every in-grid source then shades the pixel whatever its height (the
+    zenith patch, whose float32 tan(90 deg) is a large negative number), so
+    only pixels inside the edit re-march it.  Any other table gets
+    ``CORRIDOR_ALWAYS`` (re-marched by every window pixel).  The device test
+    (csrc/svf_sweep.cu svf_in_corridor) relies on exactly these properties."""
+    n_p = int(plan["n_patches"][0])
+    desc = np.full(n_p, N.CORRIDOR_ALWAYS, np.int32)
+    blind = -(2.0 * float(height_bound) + 16.0)
+    for q in range(n_p):
+        off, n = int(plan["step_offset"][0, q]), int(plan["step_count"][0, q])
+        dx = steps["dx"][off:off + n].astype(np.int64)
+        dy = steps["dy"][off:off + n].astype(np.int64)
+        dz = steps["dz"][off:off + n].astype(np.float64)
+        if n == 0 or np.all(dz < blind):
+            desc[q] = N.CORRIDOR_LOCAL
+            continue
+        k1 = np.arange(1, n + 1)
+        for axis, major, minor in ((0, dx, dy), (1, dy, dx)):
+            s = 1 if np.array_equal(major, k1) else (-1 if np.array_equal(major, -k1) else 0)
+            if s == 0:
+                continue
+            d = np.diff(minor)
+            if np.all(np.abs(d) <= 1) and (np.all(d >= 0) or np.all(d <= 0)):
+                desc[q] = axis | (4 if s < 0 else 0)
+                break
+    return desc
+
+
+def in_corridor(desc: int, dx: np.ndarray, dy: np.ndarray, t, rect) -> bool:
+    """Host restatement of the device corridor test (svf_in_corridor)."""
+    tr, tc = t
+    r0, r1, c0, c1 = rect
+    if r0 <= tr <= r1 and c0 <= tc <= c1:
+        return True
+    n = len(dx)
+    axis = desc & 3
+    if n == 0 or axis == N.CORRIDOR_LOCAL:
+        return False
+    if axis == N.CORRIDOR_ALWAYS:
+        return True
+    neg = bool(desc & 4)
+    tM, lo, hi = (tr, r0, r1) if axis == 0 else (tc, c0, c1)
+    tm, mlo, mhi = (tc, c0, c1) if axis == 0 else (tr, r0, r1)
+    ka = max(tM - hi if neg else lo - tM, 1)
+    kb = min(tM - lo if neg else hi - tM, n)
+    if ka > kb:
+        return False
+    minor = dy if axis == 0 else dx
+    ma, mb = int(minor[ka - 1]), int(minor[kb - 1])
+    return tm + max(ma, mb) >= mlo and tm + min(ma, mb) <= mhi
+
+
+def edit_window(rect, plan: np.ndarray, steps: np.ndarray, desc: np.ndarray, rows: int, cols: int):
+    """Pixels whose marches can read the edited rectangle: the rectangle
+    and, per patch that is not local, the rectangle shifted back by every
+    executed step (a box per patch), clipped to the grid; inclusive bounds."""
+    r0, r1, c0, c1 = rect
+    w = [r0, r1, c0, c1]
+    for q in range(len(desc)):
+        if (desc[q] & 3) == N.CORRIDOR_LOCAL:
+            continue
+        off, n = int(plan["step_offset"][0, q]), int(plan["step_count"][0, q])
+        dx = steps["dx"][off:off + n]
+        dy = steps["dy"][off:off + n]
+        w[0] = min(w[0], r0 - int(dx.max()))
+        w[1] = max(w[1], r1 - int(dx.min()))
+        w[2] = min(w[2], c0 - int(dy.max()))
+        w[3] = max(w[3], c1 - int(dy.min()))
+    return (max(0, w[0]), min(rows - 1, w[1]), max(0, w[2]), min(cols - 1, w[3]))
+
+
 # ----------------------------------------------------- predicate bounds
 def _f32_to_key(x):
     b = np.asarray(x, F32).view(np.int32).astype(np.int64)

@@ -133,6 +133,8 @@ class DeviceSite:
         self.amax_fixed = amaxvalue is not None
         self.amax = F32(amaxvalue) if amaxvalue is not None else amax
         self._set_march_stats(a, vegdsm, vegdsm2, bush)
+        # host copies of the edited inputs (block edits update them in place)
+        self.host = {"dsm": a.copy(), "trees": np.asarray(trees, F32).copy(), "dem": np.asarray(dem, F32).copy()}
         self.scale = float(scale)
         d = self.device
         self.t = {
@@ -167,6 +169,7 @@ class DeviceSite:
         self.amax = F32(amaxvalue)
         self.amax_fixed = True
         self._set_march_stats(a, vegdsm, vegdsm2, bush)
+        self.host = None
         self.scale = float(scale)
         d = self.device
         self.t = {"dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
@@ -245,6 +248,9 @@ class DeviceSite:
         if aspect_deg is not None:
             self.t["aspect_rad"] = _dev((np.asarray(aspect_deg, F32) * F32(np.pi)) / F32(180.), d)
         self._set_march_stats(a, vegdsm, vegdsm2, bush)
+        self.hmax = max(self.hmax, old_hmax)  # a bound over the rasters before and after the edit
+        if self.host is not None:
+            self.host = {"dsm": a.copy(), "trees": np.asarray(trees, F32).copy(), "dem": np.asarray(dem, F32).copy()}
         if old_bush or self.bush_any or new_amax != self.amax or not self.all_finite:
             self.amax = new_amax
             self._cache = {k: v for k, v in self._cache.items() if k[0] not in ("svf", "svf_host")}
@@ -264,24 +270,70 @@ class DeviceSite:
         del old
         if rect[1] < 0:
             return {"mode": "none", "rect": None, "window": None, "pixels": 0}
+        return self._window_update(rect, patch_option)
+
+    def _corridor(self, patch_option):
+        """Corridor descriptors and per-patch shift bounds, cached while the
+        height bound they were built for still holds."""
+        key = ("corridor", patch_option)
+        hit = self._cache.get(key)
+        if hit is None or hit[0] < self.hmax:
+            plan_d, steps_d, n_steps, _, _ = self.svf_tables(patch_option)
+            plan, steps = self._cache[("svf_host", patch_option)]
+            bound = max(64.0, 2.0 * self.hmax)
+            desc = T.svf_corridor(plan, steps, bound)
+            self._cache[key] = hit = (bound, desc, _upload(torch.from_numpy(desc), self.device),
+                                      T.patch_shift_bounds(plan, steps, desc))
+        return hit[1], hit[2], hit[3]
+
+    def _window_update(self, rect, patch_option=2) -> dict:
         plan_d, steps_d, n_steps, _, _ = self.svf_tables(patch_option)
-        plan, steps = self._cache[("svf_host", patch_option)]
-        desc = T.svf_corridor(plan, steps, max(old_hmax, self.hmax))
-        window = T.edit_window(rect, plan, steps, desc, self.rows, self.cols)
+        desc, desc_d, bounds = self._corridor(patch_option)
+        window = T.window_from_bounds(rect, bounds, self.rows, self.cols)
         key = ("window_ws",)
         if key not in self._cache:
             self._cache[key] = torch.empty(N.workspace_bytes("sw100_svf_window_workspace_bytes", self.rows,
-                                                             self.cols), dtype=torch.uint8, device=d)
+                                                             self.cols), dtype=torch.uint8, device=self.device)
         wws = self._cache[key]
-        desc_d = _upload(torch.from_numpy(desc), d)
         r = self.svf_result
-        N.call("sw100_svf_window", C.byref(new_site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), n_steps,
+        site = self.site_struct()
+        N.call("sw100_svf_window", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), n_steps,
                _ptr(desc_d), (C.c_int32 * 4)(*rect), (C.c_int32 * 4)(*window), _ptr(r.planes), _ptr(r.bits),
                _ptr(wws), wws.numel(), _stream())
-        self._keep = [desc_d]
         self._prepare_loop_statics()
-        return {"mode": "window", "rect": rect, "window": window,
+        return {"mode": "window", "rect": tuple(rect), "window": window,
                 "pixels": (window[1] - window[0] + 1) * (window[3] - window[2] + 1)}
+
+    def edit_svf_block(self, r0, c0, dsm=None, trees=None, dem=None, patch_option=2) -> dict:
+        """Exact SVF update after replacing the block of the rasters at
+        (r0, c0) with the given arrays (any of dsm / trees / dem, same block
+        shape): only the block travels to the device and the block is the
+        edit rectangle.  Same result and fallbacks as :meth:`edit_svf`."""
+        if self.svf_result is None or self.host is None:
+            raise RuntimeError("edit_svf_block needs a site built from rasters and a computed SVF")
+        blk = next(np.asarray(x, F32) for x in (dsm, trees, dem) if x is not None)
+        h, w = blk.shape
+        if r0 < 0 or c0 < 0 or r0 + h > self.rows or c0 + w > self.cols or h == 0 or w == 0:
+            raise ValueError(f"block {h} x {w} at ({r0}, {c0}) is outside the {self.rows} x {self.cols} grid")
+        sl = (slice(r0, r0 + h), slice(c0, c0 + w))
+        for name, v in (("dsm", dsm), ("trees", trees), ("dem", dem)):
+            if v is not None:
+                self.host[name][sl] = np.asarray(v, F32)
+        a, t1, t2 = self.host["dsm"], self.host["trees"], self.host["dem"]
+        vegdsm_b, vegdsm2_b, bush_b, _, bld_b = march_inputs(a[sl], t1[sl], t2[sl])
+        amax = self.amax if self.amax_fixed else \
+            F32(max(a.max(), float((np.maximum(t1, 0) + t2).max())))
+        hb = float(max(np.abs(a[sl]).max(), np.abs(vegdsm_b).max(), np.abs(vegdsm2_b).max()))
+        if self.bush_any or bush_b.max() > 0 or amax != self.amax or \
+                not (np.isfinite(a[sl]).all() and np.isfinite(vegdsm_b).all() and np.isfinite(vegdsm2_b).all()):
+            return self.edit_svf(a, t1, t2, patch_option=patch_option)
+        for name, v in (("dsm", a[sl]), ("vegdsm", vegdsm_b), ("vegdsm2", vegdsm2_b), ("buildings", bld_b)):
+            self.t[name].view(self.rows, self.cols)[sl].copy_(_upload(torch.from_numpy(np.ascontiguousarray(v)),
+                                                                      self.device))
+        # bounds only need to stay above the true maxima (early exit, height-blind patches)
+        self.vmax = F32(max(float(self.vmax), float(a[sl].max()), float(vegdsm_b.max()), float(vegdsm2_b.max())))
+        self.hmax = max(self.hmax, hb)
+        return self._window_update((r0, r0 + h - 1, c0, c0 + w - 1), patch_option)
 
     def launch_svf(self, planes, bits, patch_option=2):
         """The sweep alone into caller buffers (no host work once the tables

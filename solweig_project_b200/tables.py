@@ -342,6 +342,26 @@ def edit_window(rect, plan: np.ndarray, steps: np.ndarray, desc: np.ndarray, row
     return (max(0, w[0]), min(rows - 1, w[1]), max(0, w[2]), min(cols - 1, w[3]))
 
 
+def patch_shift_bounds(plan: np.ndarray, steps: np.ndarray, desc: np.ndarray) -> np.ndarray:
+    """(min dx, max dx, min dy, max dy) over the executed steps of every
+    patch that is not local (rows of zeros for the others)."""
+    out = np.zeros((len(desc), 4), np.int64)
+    for q in range(len(desc)):
+        if (desc[q] & 3) == N.CORRIDOR_LOCAL:
+            continue
+        off, n = int(plan["step_offset"][0, q]), int(plan["step_count"][0, q])
+        dx, dy = steps["dx"][off:off + n], steps["dy"][off:off + n]
+        out[q] = (dx.min(), dx.max(), dy.min(), dy.max())
+    return out
+
+
+def window_from_bounds(rect, bounds: np.ndarray, rows: int, cols: int):
+    """:func:`edit_window` from the per-patch shift bounds."""
+    r0, r1, c0, c1 = rect
+    return (max(0, r0 - int(bounds[:, 1].max(initial=0))), min(rows - 1, r1 - int(bounds[:, 0].min(initial=0))),
+            max(0, c0 - int(bounds[:, 3].max(initial=0))), min(cols - 1, c1 - int(bounds[:, 2].min(initial=0))))
+
+
 # ----------------------------------------------------- predicate bounds
 def _f32_to_key(x):
     b = np.asarray(x, F32).view(np.int32).astype(np.int64)

@@ -136,3 +136,26 @@ def test_windowed_recompute_falls_back_to_a_full_sweep(cuda):
     ref = DeviceSite(d, city.trees, city.dem, city.walls, city.aspect, city.scale)
     assert np.array_equal(site.svf_result.planes.cpu().numpy().view(np.uint32),
                           ref.run_svf().planes.cpu().numpy().view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_block_edits_equal_full_sweeps(cuda):
+    from solweig_project_b200.engine import DeviceSite
+    city = _scene(8, 120, 140)
+    site = DeviceSite(city.dsm, city.trees, city.dem, city.walls, city.aspect, city.scale)
+    site.run_svf()
+    rng = np.random.default_rng(3)
+    dsm, trees = city.dsm.copy(), city.trees.copy()
+    for k in range(4):
+        r0, c0 = int(rng.integers(0, 100)), int(rng.integers(0, 120))
+        h, w = int(rng.integers(3, 20)), int(rng.integers(3, 20))
+        blk = dsm[r0:r0 + h, c0:c0 + w].copy()
+        blk[:] = F32(rng.uniform(2, 30)) if k % 2 == 0 else city.dem[r0:r0 + h, c0:c0 + w]
+        dsm[r0:r0 + h, c0:c0 + w] = blk
+        info = site.edit_svf_block(r0, c0, dsm=blk)
+        assert info["mode"] in ("window", "full")
+        ref = DeviceSite(dsm, trees, city.dem, city.walls, city.aspect, city.scale, amaxvalue=float(site.amax))
+        full = ref.run_svf()
+        assert np.array_equal(site.svf_result.planes.cpu().numpy().view(np.uint32),
+                              full.planes.cpu().numpy().view(np.uint32)), k
+        assert np.array_equal(site.svf_result.bits.cpu().numpy(), full.bits.cpu().numpy()), k

@@ -58,6 +58,7 @@ def _paint_buildings(rng, rows, cols, dsm, n_buildings, side_lo, side_hi, h_lo, 
     """
     placed = 0
     attempts = 0
+    built = int(np.count_nonzero(dsm > 0))
     limit = n_buildings if density is None else max(1, n_buildings) * 50
     while attempts < limit:
         attempts += 1
@@ -67,10 +68,13 @@ def _paint_buildings(rng, rows, cols, dsm, n_buildings, side_lo, side_hi, h_lo, 
         c0 = int(rng.integers(0, cols))
         height = np.float32(rng.uniform(h_lo, h_hi))
         blk = dsm[r0:r0 + h, c0:c0 + w]
+        before = int(np.count_nonzero(blk > 0)) if density is not None else 0
         np.maximum(blk, height, out=blk)
         placed += 1
-        if density is not None and float((dsm > 0).mean()) >= density:
-            break
+        if density is not None:
+            built += int(np.count_nonzero(blk > 0)) - before   # running count of (dsm > 0)
+            if built / dsm.size >= density:
+                break
     return placed
 
 
@@ -79,6 +83,7 @@ def _paint_trees(rng, rows, cols, canopy, n_trees, r_lo, r_hi, p_lo, p_hi, cover
     yy = np.arange(rows, dtype=np.float64)[:, None]
     xx = np.arange(cols, dtype=np.float64)[None, :]
     attempts = 0
+    covered = int(np.count_nonzero(canopy > 0))
     limit = n_trees if cover is None else max(1, n_trees) * 50
     while attempts < limit:
         attempts += 1
@@ -95,9 +100,12 @@ def _paint_trees(rng, rows, cols, canopy, n_trees, r_lo, r_hi, p_lo, p_hi, cover
         h = peak * np.exp(-d2 / (2.0 * sigma * sigma))
         h[d2 > rad * rad] = 0.0
         blk = canopy[r0:r1, c0:c1]
+        before = int(np.count_nonzero(blk > 0)) if cover is not None else 0
         np.maximum(blk, h.astype(np.float32), out=blk)
-        if cover is not None and float((canopy > 0).mean()) >= cover:
-            break
+        if cover is not None:
+            covered += int(np.count_nonzero(blk > 0)) - before   # running count of (canopy > 0)
+            if covered / canopy.size >= cover:
+                break
 
 
 def make_city(rows: int, cols: int | None = None, seed: int = 1234, *,

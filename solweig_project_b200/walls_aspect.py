@@ -46,17 +46,6 @@ def get_ders(dsm: np.ndarray, scale: float):
     return grad, asp
 
 
-def _window_sum(plane: np.ndarray, offsets, rows_rng, cols_rng, dtype):
-    """Sequential sum over ``offsets`` (row-major order) of shifted planes,
-    evaluated on the pixel block ``rows_rng`` x ``cols_rng``."""
-    r0, r1 = rows_rng
-    c0, c1 = cols_rng
-    acc = np.zeros((r1 - r0, c1 - c0), dtype)
-    for di, dj in offsets:
-        acc = acc + plane[r0 + di:r1 + di, c0 + dj:c1 + dj].astype(dtype, copy=False)
-    return acc
-
-
 def filter1Goodwin_as_aspect_v3(walls: np.ndarray, scale: float, a: np.ndarray) -> np.ndarray:
     """Wall aspect in degrees by a rotating line filter
     (walls_aspect.py:99-161): for each of 180 orientations the number of wall
@@ -79,7 +68,6 @@ def filter1Goodwin_as_aspect_v3(walls: np.ndarray, scale: float, a: np.ndarray) 
     buildfilt[hc - 1, hc:] = 2
 
     y = np.zeros((rows, cols))
-    z = np.zeros((rows, cols))
     x = np.zeros((rows, cols))
     wall_u8 = (walls > 0).astype(np.uint8)
     a32 = np.asarray(a, np.float32)
@@ -88,7 +76,11 @@ def filter1Goodwin_as_aspect_v3(walls: np.ndarray, scale: float, a: np.ndarray) 
     i0, i1 = hc - 1, rows - hc - 1
     j0, j1 = hc - 1, cols - hc - 1
     if i1 > i0 and j1 > j0:
-        block_walls = wall_u8[i0:i1, j0:j1] == 1
+        # only wall pixels of the block are ever updated: evaluate the
+        # filters there (same per-pixel sums, in the same order)
+        wr, wc = np.nonzero(wall_u8[i0:i1, j0:j1] == 1)
+        wr, wc = wr + i0, wc + j0
+        zw = np.zeros(wr.size, np.float64)
         for h in range(0, 180):
             filt1 = np.round(rotate(filtmatrix, h, order=1, reshape=False, mode='nearest'))
             filtb = np.round(rotate(buildfilt, h, order=0, reshape=False, mode='nearest'))
@@ -103,22 +95,26 @@ def filter1Goodwin_as_aspect_v3(walls: np.ndarray, scale: float, a: np.ndarray) 
             offs = [(di - hf, dj - hf) for di in range(filtersize) for dj in range(filtersize)
                     if filt1[di, dj] != 0]
             weights = [filt1[di + hf, dj + hf] for di, dj in offs]
-            cnt = np.zeros((i1 - i0, j1 - j0), np.float64)
+            cnt = np.zeros(wr.size, np.float64)
             for (di, dj), w in zip(offs, weights):
-                cnt = cnt + wall_u8[i0 + di:i1 + di, j0 + dj:j1 + dj] * w
-            zb = z[i0:i1, j0:j1]
-            upd = block_walls & (zb < cnt)
+                cnt = cnt + wall_u8[wr + di, wc + dj] * w
+            upd = zw < cnt
             if not upd.any():
                 continue
             o1 = [(di - hf, dj - hf) for di in range(filtersize) for dj in range(filtersize)
                   if filtb[di, dj] == 1]
             o2 = [(di - hf, dj - hf) for di in range(filtersize) for dj in range(filtersize)
                   if filtb[di, dj] == 2]
-            s1 = _window_sum(a32, o1, (i0, i1), (j0, j1), np.float32)
-            s2 = _window_sum(a32, o2, (i0, i1), (j0, j1), np.float32)
-            zb[upd] = cnt[upd]
-            x[i0:i1, j0:j1][upd] = np.where(s1[upd] > s2[upd], 1, 2)
-            y[i0:i1, j0:j1][upd] = index
+            ur, uc = wr[upd], wc[upd]
+            s1 = np.zeros(ur.size, np.float32)
+            for di, dj in o1:
+                s1 = s1 + a32[ur + di, uc + dj]
+            s2 = np.zeros(ur.size, np.float32)
+            for di, dj in o2:
+                s2 = s2 + a32[ur + di, uc + dj]
+            zw[upd] = cnt[upd]
+            x[ur, uc] = np.where(s1 > s2, 1, 2)
+            y[ur, uc] = index
 
     y[x == 1] -= 180
     y[y < 0] += 360

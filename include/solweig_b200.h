@@ -328,6 +328,60 @@ typedef struct {
 #define SW100_OUT_LDOWN  (1 << 5)
 #define SW100_OUT_SHADOW (1 << 6)
 
+/* ------------------------------------------------------------ batches -- */
+/* One site of a batched launch.  A device array of these, and device tile
+ * lists, drive the sw100_batch_* entry points: every stage of every site of
+ * the batch runs in one launch per stage (the reference runs one site at a
+ * time, utci_process.py:1472-1651 run_utci_tiles / solweig_gpu.py:387-497).
+ * All pointers are device memory.  `site.bits`, `site.svfbuveg`,
+ * `site.hsvf` and `site.tan_alfa` point into `svf_bits` / `svf_planes`
+ * (planes 16, 17, 18), `site.single_step` holds the SVF plan's one-step
+ * patches, so the time loop reads what the sweep of the same batch wrote. */
+typedef struct {
+  sw100_site_planes site;
+  int32_t rows, cols;
+  const sw100_svf_plan* plan;   /* SVF tables of the site (sw100_svf_sweep) */
+  const sw100_step* steps;
+  sw100_series series;          /* time-series tables of the site (sw100_time_loop) */
+  float* svf_planes;            /* SW100_SVF_PLANES * npix, written by the sweep */
+  uint32_t* svf_bits;           /* 3 * SW100_CUBE_WORDS * npix, written by the sweep */
+  float* src4;                  /* 4 * npix, packed march source */
+  uint32_t* bflags;             /* one word per SVF table step, zeroed by the caller (bush sites) */
+  float* gsrc;                  /* 4 * n_day * npix, sun-march records */
+  float* state;                 /* 6 * npix thermal state, carried across calls */
+  float* outputs;               /* popcount(out_mask) * n_t * npix */
+  uint32_t out_mask;
+  int32_t pad;
+} sw100_batch_site;
+
+/* Tile list entry {site index, tile column, tile row, daytime row}: the
+ * tile covers pixels [tile column * block_x, +block_x) x [tile row *
+ * block_y, +block_y) of its site; the daytime row is used by the sun march
+ * only.  Lists are ordered by the caller (heaviest sites first). */
+typedef struct {
+  int32_t site, tx, ty, day;
+} sw100_tile;
+
+/* Checks a host copy of the batch descriptors (sizes, pointers, patch
+ * counts) before the caller uploads it. */
+int sw100_batch_validate(const sw100_batch_site* host_sites, int n_sites);
+/* Each launch runs `grid` blocks of block_x * block_y == 128 threads over
+ * the tile list (grid < n_tiles: blocks stride over the list, a persistent
+ * launch; grid == n_tiles: one tile per block).  Stages: pack the march
+ * sources; the bush step flags of bush sites (tiles of those sites only);
+ * the SVF sweep; the sun march (tiles carry the daytime row); the flux
+ * loop. */
+int sw100_batch_pack(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                     int block_y, int grid, void* stream);
+int sw100_batch_bush_flags(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                           int block_y, int grid, void* stream);
+int sw100_batch_svf(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x, int block_y,
+                    int grid, void* stream);
+int sw100_batch_sun_march(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                          int block_y, int grid, void* stream);
+int sw100_batch_flux_loop(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                          int block_y, int grid, void* stream);
+
 /* Sun march for every daytime row of the series in one launch.  Writes the
  * per-row ground-view-factor source records (4 floats per pixel:
  * shadow, Lup, albedo, flag bits) to gsrc (n_day * npix * 4 floats) and,

@@ -34,7 +34,9 @@ OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDO
 SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noalloc", "sw100_pack_cubes", "sw100_sun_march_workspace_bytes",
            "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop", "sw100_flux_loop", "sw100_utci",
            "sw100_abi_version", "sw100_last_error", "sw100_launch_count", "sw100_svf_window_workspace_bytes",
-           "sw100_svf_window", "sw100_diff_bbox_workspace_bytes", "sw100_diff_bbox")
+           "sw100_svf_window", "sw100_diff_bbox_workspace_bytes", "sw100_diff_bbox", "sw100_batch_validate",
+           "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
+           "sw100_batch_flux_loop")
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
 
@@ -160,6 +162,10 @@ def load(path: str = LIB_PATH):
         "sw100_svf_window": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp,
                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32), vp, vp, vp, C.c_int64, vp]),
         "sw100_diff_bbox_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
+        "sw100_batch_validate": (C.c_int, [vp, C.c_int]),
+        **{name: (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]) for name in (
+            "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
+            "sw100_batch_flux_loop")},
         "sw100_diff_bbox": (C.c_int, [C.POINTER(SitePlanes), C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp,
                                       C.c_int64, vp]),
     }

@@ -26,6 +26,11 @@ __global__ void svf_window_kernel(const float4* src4, int rows, int cols, const 
                                   float* out, uint32_t* bits);
 __global__ void diff_bbox_kernel(const float4* a, const float4* b, int rows, int cols, int* box);
 __global__ void box_init_kernel(int* box);
+__global__ void pack_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
+__global__ void svf_bush_flags_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
+__global__ void svf_sweep_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
+__global__ void sun_march_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
+__global__ void time_loop_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void svf_bush_flags_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
                                       const sw100_step* steps, uint32_t* flags);
 __global__ void sun_march_kernel(const float4* src4, SitePlanes site, int rows, int cols,
@@ -263,6 +268,87 @@ int sw100_diff_bbox(const sw100_site_planes* before, const sw100_site_planes* af
   const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, 148 * 8);
   diff_bbox_kernel<<<blocks, threads, 0, st>>>(a, b, rows, cols, box);
   return check_launch("diff_bbox_kernel");
+}
+
+int sw100_batch_validate(const sw100_batch_site* host_sites, int n_sites) {
+  int rc;
+  if (n_sites < 0) return fail(SW100_E_ARG, "n_sites must be >= 0");
+  if (n_sites > 0 && (rc = check_ptr(host_sites, "host_sites"))) return rc;
+  for (int i = 0; i < n_sites; ++i) {
+    const sw100_batch_site& b = host_sites[i];
+    if ((rc = check_grid(b.rows, b.cols))) return fail(rc, "site %d: %s", i, g_last_error.c_str());
+    if ((rc = validate_site_march(&b.site))) return fail(rc, "site %d: %s", i, g_last_error.c_str());
+    const void* ptrs[] = {b.plan, b.steps, b.svf_planes, b.svf_bits, b.src4, b.state};
+    const char* names[] = {"plan", "steps", "svf_planes", "svf_bits", "src4", "state"};
+    for (int k = 0; k < 6; ++k)
+      if (!ptrs[k]) return fail(SW100_E_ARG, "site %d: %s must not be NULL", i, names[k]);
+    if (b.site.bush_any && !b.bflags) return fail(SW100_E_ARG, "site %d: bflags must not be NULL with bush", i);
+    if ((rc = validate_series(&b.series))) return fail(rc, "site %d: %s", i, g_last_error.c_str());
+    if (b.series.n_day > 0 && !b.gsrc) return fail(SW100_E_ARG, "site %d: gsrc must not be NULL", i);
+    if (b.out_mask & ~0x7Fu) return fail(SW100_E_ARG, "site %d: unknown output bits 0x%x", i, b.out_mask);
+    if (b.out_mask && !b.outputs) return fail(SW100_E_ARG, "site %d: outputs must not be NULL", i);
+    if (b.site.bits != b.svf_bits || b.site.svfbuveg != b.svf_planes + (size_t)16 * b.rows * b.cols ||
+        b.site.hsvf != b.svf_planes + (size_t)17 * b.rows * b.cols ||
+        b.site.tan_alfa != b.svf_planes + (size_t)18 * b.rows * b.cols)
+      return fail(SW100_E_ARG, "site %d: site statics must point into svf_planes / svf_bits", i);
+    const void* loop[] = {b.site.buildings, b.site.walls, b.site.aspect_rad, b.site.tgk, b.site.tstart,
+                          b.site.alb, b.site.emis, b.site.class_idx, b.site.windcoeff};
+    for (int k = 0; k < 9; ++k)
+      if (!loop[k]) return fail(SW100_E_ARG, "site %d: a time-loop plane is NULL", i);
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class Kernel>
+int launch_batch(Kernel kernel, const char* name, const sw100_batch_site* sites, const sw100_tile* tiles,
+                 int n_tiles, int block_x, int block_y, int grid, void* stream) {
+  int rc;
+  if (n_tiles < 0) return fail(SW100_E_ARG, "n_tiles must be >= 0");
+  if (n_tiles == 0) return 0;
+  if ((rc = check_ptr(sites, "sites")) || (rc = check_ptr(tiles, "tiles"))) return rc;
+  if (block_x <= 0 || block_y <= 0 || block_x * block_y != 128)
+    return fail(SW100_E_ARG, "block %d x %d: batch kernels run 128 threads per block", block_x, block_y);
+  if (grid <= 0) return fail(SW100_E_ARG, "grid must be positive");
+  grid = std::min(grid, n_tiles);
+  kernel<<<grid, dim3(block_x, block_y), 0, static_cast<cudaStream_t>(stream)>>>(sites, tiles, n_tiles);
+  return check_launch(name);
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw100_batch_pack(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                     int block_y, int grid, void* stream) {
+  return launch_batch(pack_batch_kernel, "pack_batch_kernel", sites, tiles, n_tiles, block_x, block_y, grid, stream);
+}
+
+int sw100_batch_bush_flags(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                           int block_y, int grid, void* stream) {
+  return launch_batch(svf_bush_flags_batch_kernel, "svf_bush_flags_batch_kernel", sites, tiles, n_tiles, block_x,
+                      block_y, grid, stream);
+}
+
+int sw100_batch_svf(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x, int block_y,
+                    int grid, void* stream) {
+  return launch_batch(svf_sweep_batch_kernel, "svf_sweep_batch_kernel", sites, tiles, n_tiles, block_x, block_y,
+                      grid, stream);
+}
+
+int sw100_batch_sun_march(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                          int block_y, int grid, void* stream) {
+  return launch_batch(sun_march_batch_kernel, "sun_march_batch_kernel", sites, tiles, n_tiles, block_x, block_y,
+                      grid, stream);
+}
+
+int sw100_batch_flux_loop(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                          int block_y, int grid, void* stream) {
+  return launch_batch(time_loop_batch_kernel, "time_loop_batch_kernel", sites, tiles, n_tiles, block_x, block_y,
+                      grid, stream);
 }
 
 int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbshvegshmat, int rows, int cols,

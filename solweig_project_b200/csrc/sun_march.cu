@@ -91,15 +91,15 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
   return o;
 }
 
-__global__ void __launch_bounds__(256) sun_march_kernel(const float4* __restrict__ src4, SitePlanes site, int rows,
-                                                         int cols, const sw100_sun_step* __restrict__ sun_steps,
-                                                         const sw100_time_step* __restrict__ tsteps,
-                                                         const sw100_step* __restrict__ table, float vmax,
-                                                         float4* __restrict__ gsrc, float* __restrict__ debug8) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
-  const int d = blockIdx.z;  // daytime step row
-  if (r >= rows || c >= cols) return;
+// Daytime row d of pixel (r, c): march, wall tail and the ground-view-factor
+// source record.  `Site` is SitePlanes or sw100_site_planes.
+template <class Site>
+__device__ __forceinline__ void sun_march_pixel(const float4* __restrict__ src4, const Site& site, int rows, int cols,
+                                                const sw100_sun_step* __restrict__ sun_steps,
+                                                const sw100_time_step* __restrict__ tsteps,
+                                                const sw100_step* __restrict__ table, float vmax,
+                                                float4* __restrict__ gsrc, float* __restrict__ debug8, int r, int c,
+                                                int d) {
   const size_t npix = (size_t)rows * cols;
   const size_t p = (size_t)r * cols + c;
   const sw100_sun_step S = sun_steps[d];
@@ -121,6 +121,32 @@ __global__ void __launch_bounds__(256) sun_march_kernel(const float4* __restrict
     float* o8 = debug8 + (size_t)d * 8 * npix + p;
     o8[0 * npix] = o.vegsh; o8[1 * npix] = o.sh; o8[2 * npix] = o.vbsh; o8[3 * npix] = o.wallsh;
     o8[4 * npix] = o.wallsun; o8[5 * npix] = o.wallshve; o8[6 * npix] = o.facesh; o8[7 * npix] = o.facesun;
+  }
+}
+
+__global__ void __launch_bounds__(256) sun_march_kernel(const float4* __restrict__ src4, SitePlanes site, int rows,
+                                                         int cols, const sw100_sun_step* __restrict__ sun_steps,
+                                                         const sw100_time_step* __restrict__ tsteps,
+                                                         const sw100_step* __restrict__ table, float vmax,
+                                                         float4* __restrict__ gsrc, float* __restrict__ debug8) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  if (r >= rows || c >= cols) return;
+  sun_march_pixel(src4, site, rows, cols, sun_steps, tsteps, table, vmax, gsrc, debug8, r, c, blockIdx.z);
+}
+
+// Sun march of every daytime row of every site of a batch: each tile
+// carries its daytime row.
+__global__ void __launch_bounds__(128) sun_march_batch_kernel(const sw100_batch_site* __restrict__ sites,
+                                                              const sw100_tile* __restrict__ tiles, int n_tiles) {
+  for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {
+    const sw100_tile T = tiles[i];
+    const sw100_batch_site& S = sites[T.site];
+    const int c = T.tx * blockDim.x + threadIdx.x;
+    const int r = T.ty * blockDim.y + threadIdx.y;
+    if (r >= S.rows || c >= S.cols || T.day >= S.series.n_day) continue;
+    sun_march_pixel(reinterpret_cast<const float4*>(S.src4), S.site, S.rows, S.cols, S.series.sun, S.series.steps,
+                    S.series.sun_table, S.site.vmax, reinterpret_cast<float4*>(S.gsrc), nullptr, r, c, T.day);
   }
 }
 

@@ -246,16 +246,11 @@ __device__ __forceinline__ void load_plan(const sw100_svf_plan* __restrict__ pla
   for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < nw; i += blockDim.x * blockDim.y) d[i] = s[i];
 }
 
-__global__ void __launch_bounds__(128) svf_sweep_kernel(
-    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
-    const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
-    float* __restrict__ out, uint32_t* __restrict__ bits) {
-  __shared__ sw100_svf_plan plan;
-  load_plan(plan_g, plan);
-  __syncthreads();
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
-  if (r >= rows || c >= cols) return;
+// The 153 patch marches, the sums and the outputs of pixel (r, c).
+__device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4, int rows, int cols,
+                                                const sw100_svf_plan& plan, const sw100_step* __restrict__ steps,
+                                                const uint32_t* __restrict__ bflags, float vmax,
+                                                float* __restrict__ out, uint32_t* __restrict__ bits, int r, int c) {
   const size_t npix = (size_t)rows * cols;
   const size_t p = (size_t)r * cols + c;
   const float4 self = src4[p];
@@ -281,6 +276,85 @@ __global__ void __launch_bounds__(128) svf_sweep_kernel(
     svf_add_patch(A, plan, q, sh, veg, vb);
   }
   svf_finish(A, plan, veg2_p, p, npix, wsh, wveg, wvb, out, bits);
+}
+
+__global__ void __launch_bounds__(128) svf_sweep_kernel(
+    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
+    const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
+    float* __restrict__ out, uint32_t* __restrict__ bits) {
+  __shared__ sw100_svf_plan plan;
+  load_plan(plan_g, plan);
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  if (r >= rows || c >= cols) return;
+  svf_sweep_pixel(src4, rows, cols, plan, steps, bflags, vmax, out, bits, r, c);
+}
+
+// ------------------------------------------------------------- batches
+// Tile t of a batch: pixel (r, c) of this thread, and whether it exists.
+__device__ __forceinline__ bool batch_pixel(const sw100_batch_site& S, const sw100_tile& T, int& r, int& c) {
+  c = T.tx * blockDim.x + threadIdx.x;
+  r = T.ty * blockDim.y + threadIdx.y;
+  return r < S.rows && c < S.cols;
+}
+
+// SVF sweep of every site of a batch, tiles taken in list order.
+__global__ void __launch_bounds__(128) svf_sweep_batch_kernel(const sw100_batch_site* __restrict__ sites,
+                                                              const sw100_tile* __restrict__ tiles, int n_tiles) {
+  __shared__ sw100_svf_plan plan;
+  for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {
+    const sw100_tile T = tiles[i];
+    const sw100_batch_site& S = sites[T.site];
+    __syncthreads();  // the previous tile is done with the shared plan
+    load_plan(S.plan, plan);
+    __syncthreads();
+    int r, c;
+    if (batch_pixel(S, T, r, c))
+      svf_sweep_pixel(reinterpret_cast<const float4*>(S.src4), S.rows, S.cols, plan, S.steps,
+                      S.site.bush_any ? S.bflags : nullptr, S.site.vmax, S.svf_planes, S.svf_bits, r, c);
+  }
+}
+
+// Packs {dsm, vegdsm, vegdsm2, bush} of every site of a batch.
+__global__ void __launch_bounds__(128) pack_batch_kernel(const sw100_batch_site* __restrict__ sites,
+                                                         const sw100_tile* __restrict__ tiles, int n_tiles) {
+  for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {
+    const sw100_tile T = tiles[i];
+    const sw100_batch_site& S = sites[T.site];
+    int r, c;
+    if (!batch_pixel(S, T, r, c)) continue;
+    const size_t p = (size_t)r * S.cols + c;
+    reinterpret_cast<float4*>(S.src4)[p] =
+        make_float4(S.site.dsm[p], S.site.vegdsm[p], S.site.vegdsm2[p], S.site.bush_any ? S.site.bush[p] : 0.f);
+  }
+}
+
+// The whole-grid bush step flags of the sites of a batch that have bush
+// (the tile list holds tiles of those sites only).
+__global__ void __launch_bounds__(128) svf_bush_flags_batch_kernel(const sw100_batch_site* __restrict__ sites,
+                                                                   const sw100_tile* __restrict__ tiles, int n_tiles) {
+  for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {
+    const sw100_tile T = tiles[i];
+    const sw100_batch_site& S = sites[T.site];
+    int r, c;
+    if (!batch_pixel(S, T, r, c)) continue;
+    const float4* src4 = reinterpret_cast<const float4*>(S.src4);
+    const float4 self = src4[(size_t)r * S.cols + c];
+    if (!(self.w > 0.f)) continue;
+    const sw100_svf_plan* plan = S.plan;
+    const int np = plan->n_patches;
+    for (int q = 0; q < np; ++q) {
+      const int off = plan->step_offset[q], n = plan->step_count[q];
+      for (int k = 0; k < n; ++k) {
+        const sw100_step st = S.steps[off + k];
+        const int sr = r + st.dx, sc = c + st.dy;
+        float tv = 0.f;
+        if (in_grid(sr, sc, S.rows, S.cols)) tv = __fsub_rn(src4[(size_t)sr * S.cols + sc].y, st.dz);
+        if (tv > self.x && S.bflags[off + k] == 0u) atomicExch(&S.bflags[off + k], 1u);
+      }
+    }
+  }
 }
 
 // Does the march of pixel (tr, tc) along this patch's steps read a cell of

@@ -35,7 +35,9 @@ __host__ inline SitePlanes make_site(const sw100_site_planes& s) {
 // Ground temperature of the daytime parameterisation (solweig.py:2102-2122):
 // Tg = (TgK * altmax + Tstart) * sin-wave factor of the pixel's TmaxLST class,
 // times CI_TgG, floored at 0 when land cover is used.
-__device__ __forceinline__ float ground_temperature(const SitePlanes& site, const sw100_time_step& P, size_t p) {
+// (`Site` is SitePlanes or sw100_site_planes: the same member names.)
+template <class Site>
+__device__ __forceinline__ float ground_temperature(const Site& site, const sw100_time_step& P, size_t p) {
   const float tgamp = site.tgk[p] * P.altmax32 + site.tstart[p];
   float tg = tgamp * P.tg_factor[site.class_idx[p]];
   tg = tg * P.cig;

@@ -189,11 +189,16 @@ struct GvfSums {
   float LupE, albE, albnoshE, LupS, albS, albnoshS, LupW, albW, albnoshW, LupN, albN, albnoshN;
 };
 
-__global__ void __launch_bounds__(128, 5) time_loop_kernel(
-    SitePlanes site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
+// All steps of the pixels of tile (bx, by); every thread of the block calls
+// it (the step tables are staged in shared memory).  `Site` is SitePlanes
+// (a kernel parameter) or sw100_site_planes (a batch descriptor in global
+// memory): the same member names.
+template <class Site>
+__device__ __forceinline__ void time_loop_tile(
+    const Site& site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, float* __restrict__ state,
-    uint32_t out_mask, float* __restrict__ outputs) {
+    uint32_t out_mask, float* __restrict__ outputs, int bx, int by) {
   // PP is filled with 16-byte vector stores: the array must be 16-byte
   // aligned (the struct itself only requires 8)
   __shared__ __align__(16) sw100_time_step P;
@@ -216,8 +221,8 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
     AZ[tid].facesh_hi = gvf_az[tid].facesh_hi;
     AZ[tid].dir_flags = gvf_az[tid].dir_flags;
   }
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  const int c = bx * blockDim.x + threadIdx.x;
+  const int r = by * blockDim.y + threadIdx.y;
   const bool live = (r < rows) && (c < cols);
   const size_t npix = (size_t)rows * cols;
   const size_t p = live ? (size_t)r * cols + c : 0;
@@ -502,6 +507,28 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
   if (live) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) state[k * npix + p] = st[k];
+  }
+}
+
+__global__ void __launch_bounds__(128, 5) time_loop_kernel(
+    SitePlanes site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
+    const sw100_patch_step* __restrict__ patch_steps, int n_patches,
+    const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, float* __restrict__ state,
+    uint32_t out_mask, float* __restrict__ outputs) {
+  time_loop_tile(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, state, out_mask, outputs,
+                 blockIdx.x, blockIdx.y);
+}
+
+// The time loop of every site of a batch, tiles taken in list order.
+__global__ void __launch_bounds__(128, 5) time_loop_batch_kernel(const sw100_batch_site* __restrict__ sites,
+                                                                 const sw100_tile* __restrict__ tiles, int n_tiles) {
+  for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {
+    const sw100_tile T = tiles[i];
+    const sw100_batch_site& S = sites[T.site];
+    __syncthreads();  // the previous tile is done with the shared tables
+    time_loop_tile(S.site, S.rows, S.cols, S.series.steps, S.series.n_t, S.series.patch, S.series.n_patches,
+                   S.series.gvf, reinterpret_cast<const float4*>(S.gsrc), S.state, S.out_mask, S.outputs, T.tx,
+                   T.ty);
   }
 }
 

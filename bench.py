@@ -43,6 +43,9 @@ WORKLOADS = {
     # name: (side, h_max, description)
     "exact500": (500, 40.0, "500x500 px @1 m, 24 hourly steps, SVF sweep + shadows + fluxes + Tmrt + UTCI"),
     "tile4096": (4096, 120.0, "4096x4096 px @1 m, buildings up to 120 m, 24 hourly steps, full exact chain"),
+    "batched64": (None, 40.0, "64 seeded sites, sides log-uniform 128-1024 px, density 10-45 %, canopy 0-30 %, "
+                              "latitudes 0-60 N, 24 hourly steps each; one launch per stage for all sites, "
+                              "replayed as a CUDA graph, autotuned launch shapes"),
 }
 FLUX_BYTES_PER_PX_STEP = 190      # compulsory HBM bytes per pixel and step of the flux stage
 SVF_GATHER_BYTES_PER_STEP = 12    # 3 float32 gathers per march step
@@ -72,6 +75,12 @@ def parse():
 
 def make_workload(name, rank, side=None):
     from solweig_project_b200 import synthetic
+    if name == "batched64":   # the first site of the batch (reference arm sample)
+        sp = synthetic.multi_site_specs()[0]
+        city = synthetic.make_city(side or sp["side"], side or sp["side"], seed=sp["seed"], density=sp["density"],
+                                   canopy_cover=sp["canopy"])
+        return city, synthetic.make_met(sp["seed"]), synthetic.load_sun_geometry("multi0"), \
+            synthetic.default_lc_class()
     side0, hmax, _ = WORKLOADS[name]
     side = side or side0
     city = synthetic.make_city(side, side, seed=1234 + rank, h_max=hmax)
@@ -172,7 +181,7 @@ def run_reference(args):
             times.append(time.perf_counter() - t0)
     t = sum(times) / len(times)
     value = crop * crop * N_STEPS_DAY / t
-    side = WORKLOADS[args.workload][0]
+    side = city.shape[0]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
@@ -184,6 +193,147 @@ def run_reference(args):
                                    f"CPU oracle with {cores} torch threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def run_batched(args, world, rank, local):
+    """The batched workload: this rank's share of the 64 sites (LPT split by
+    pixels, strong scaling) in one graph-replayed launch per stage."""
+    import torch
+    import torch.distributed as dist
+    from solweig_project_b200 import _native as N
+    from solweig_project_b200 import batch as B
+    from solweig_project_b200 import build, synthetic
+    from solweig_project_b200.engine import DeviceSite
+    build.build()
+    specs = synthetic.multi_site_specs()
+    mine = B.partition_sites([s["side"] ** 2 for s in specs], world)[rank]
+    lc_class = synthetic.default_lc_class()
+    sites, series, cities, mets, geos, locs = [], [], [], [], [], []
+    for i in mine:
+        sp = specs[i]
+        c = synthetic.make_city(sp["side"], sp["side"], seed=sp["seed"], density=sp["density"],
+                                canopy_cover=sp["canopy"])
+        met = synthetic.make_met(sp["seed"])
+        geo = synthetic.load_sun_geometry(f"multi{i}")
+        loc = {"latitude": sp["latitude"], "longitude": sp["longitude"], "altitude": 3.0}
+        s = DeviceSite(c.dsm, c.trees, c.dem, c.walls, c.aspect, c.scale, landcover=c.landcover, lc_class=lc_class)
+        series.append(s.build_series(met, geo["altitude"], geo["azimuth"], geo["zen"], geo["jday"], geo["dectime"],
+                                     geo["altmax"], loc))
+        sites.append(s)
+        cities.append(c)
+    dev = sites[0].device
+    tuner = B.Autotuner()
+    batch = B.SiteBatch(sites, series, requested=("utci", "tmrt"), tuner=tuner)
+    tuned = tuner.tune(batch)
+    batch.capture()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        batch.replay()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    launches0 = N.launch_count()
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            events[k][0].record(stream)
+            batch.replay()
+            events[k][1].record(stream)
+        torch.cuda.synchronize()
+    direct_launches = N.launch_count() - launches0   # launches outside the graph (none expected)
+    step_ms = sum(e[0].elapsed_time(e[1]) for e in events) / args.steps
+    t_max = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    step_ms = float(t_max.item())
+    total_px = sum(s["side"] ** 2 for s in specs)
+    value = total_px * N_STEPS_DAY / (step_ms / 1e3)
+    # stage breakdown (one launch per stage, outside the graph)
+    stage_ms = {}
+    for st in B.STAGES:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.launch(st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        stage_ms[st] = e0.elapsed_time(e1)
+    # e2e: rasters from pinned host memory into the resident batch, the graph,
+    # UTCI / Tmrt back to pinned host memory
+    # the site's march rasters and wall planes, as the sweep / time loop read them
+    pinned_in = []
+    for m in batch.members:
+        for k in ("dsm", "vegdsm", "vegdsm2", "walls", "aspect_rad"):
+            pinned_in.append((m.site.t[k], m.site.t[k].detach().cpu().pin_memory()))
+    pinned_out = [torch.empty(tuple(batch.members[i].outputs.shape), dtype=torch.float32).pin_memory()
+                  for i in range(len(sites))]
+    e2e_times = []
+    for it in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for d_t, h in pinned_in:
+            d_t.copy_(h, non_blocking=True)
+        batch.replay()
+        for m, h in zip(batch.members, pinned_out):
+            h.copy_(m.outputs, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it >= 1:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = torch.tensor([sum(e2e_times) / len(e2e_times)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    h2d = sum(h.numel() * 4 for _, h in pinned_in)
+    d2h = sum(h.numel() * 4 for h in pinned_out)
+    # the graph replays the non-empty stage launches of the batch once per step
+    per_replay = sum(1 for st in B.STAGES if batch.tiles(st, batch.shapes[st][0])[1] > 0)
+    launches = args.steps * per_replay + direct_launches
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        npix_rank = batch.pixels
+        svf_steps = sum(m.n_steps * m.site.rows * m.site.cols for m in batch.members)
+        dom = max(("svf", "flux"), key=lambda k: stage_ms[k])
+        if dom == "svf":
+            achieved = SVF_GATHER_BYTES_PER_STEP * svf_steps / (stage_ms["svf"] * 1e6)
+            note = "march gather bytes (12 B x executed steps per pixel) / launch time"
+        else:
+            achieved = FLUX_BYTES_PER_PX_STEP * npix_rank * N_STEPS_DAY / (stage_ms["flux"] * 1e6)
+            note = "compulsory 190 B per pixel-step / launch time"
+        clk = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (64 seeded cities + 24 h forcing each)",
+            "config": {"workload": "batched64", "description": WORKLOADS["batched64"][2], "sites": len(specs),
+                       "pixels": total_px, "timesteps": N_STEPS_DAY,
+                       "launch_shapes": {k: [list(v[0]), v[1]] for k, v in batch.shapes.items()},
+                       "l2": "flushed (256 MiB write) before every timed step; inputs far above L2",
+                       "parallelism": f"sites LPT-split over {world} rank(s)"},
+            "roofline": {"bound": "hbm", "kernel": dom + "_batch", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback",
+                         "definition": note},
+            "stages_ms": stage_ms,
+            "autotune_ms": {k: v[2] for k, v in tuned.items()},
+            "gpu_launches": int(launches),
+            "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "e2e": {"value": total_px * N_STEPS_DAY / (float(e2e_ms.item()) / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": float(e2e_ms.item())},
+        }
+        print(json.dumps(line), flush=True)
+    batch.graph = None
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():
@@ -200,6 +350,9 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    if args.workload == "batched64":
+        run_batched(args, world, rank, local)
+        return
 
     from solweig_project_b200 import _native as N
     from solweig_project_b200 import api, build

@@ -71,6 +71,23 @@ def build_tiles(dims, shape, order) -> np.ndarray:
     return np.concatenate(parts) if parts else np.zeros(0, TILE_DTYPE)
 
 
+def partition_sites(costs, n_ranks: int):
+    """Longest-processing-time split of sites over ranks: sites in
+    decreasing cost, each to the rank with the least work so far (ties to
+    the lower rank).  Returns one list of site indices per rank, each in
+    increasing index order.  Sites are independent, so no data crosses
+    ranks."""
+    if n_ranks <= 0:
+        raise ValueError("n_ranks must be positive")
+    load = [0.0] * n_ranks
+    parts = [[] for _ in range(n_ranks)]
+    for i in sorted(range(len(costs)), key=lambda k: (-float(costs[k]), k)):
+        r = min(range(n_ranks), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(p) for p in parts]
+
+
 def size_bucket(sides) -> str:
     """Grid-size bucket of a batch: its pixel-weighted median side."""
     sides = np.sort(np.asarray(sides, np.int64))

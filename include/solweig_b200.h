@@ -411,6 +411,17 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
                     const float* gsrc, float* state, uint32_t out_mask, float* outputs, void* stream);
 
 /* ---------------------------------------------------------------- UTCI -- */
+/* UTCI-only recompute of whole steps: the met fast path of
+ * utci_process.py:1093-1196 (recompute_utci_steps), for wind speed / urban
+ * heat island edits that leave Tmrt unchanged.  steps: n_steps records whose
+ * ta_mat, rh32, ws32, utci_pa and utci_k are set (the other fields are not
+ * read); tmrt: n_steps * npix stored Tmrt planes; buildings: 1 where UTCI
+ * is defined (NaN elsewhere); windcoeff: npix or NULL (1).  out: n_steps *
+ * npix.  The arithmetic is the time loop's UTCI tail, so the result equals
+ * the UTCI a full run would give for the same forcing and Tmrt. */
+int sw100_utci_steps(const sw100_time_step* steps, int n_steps, const float* tmrt, const float* buildings,
+                     const float* windcoeff, int64_t npix, float* out, void* stream);
+
 /* utci_calculator over n float32 elements: saturation vapour pressure from
  * Ta, then the 210-term regression in float64; -999 where any input is
  * <= -999 (calculate_utci.py:259-330). */

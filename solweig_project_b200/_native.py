@@ -36,7 +36,7 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noal
            "sw100_abi_version", "sw100_last_error", "sw100_launch_count", "sw100_svf_window_workspace_bytes",
            "sw100_svf_window", "sw100_diff_bbox_workspace_bytes", "sw100_diff_bbox", "sw100_batch_validate",
            "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
-           "sw100_batch_flux_loop")
+           "sw100_batch_flux_loop", "sw100_utci_steps")
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
 
@@ -163,6 +163,7 @@ def load(path: str = LIB_PATH):
                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32), vp, vp, vp, C.c_int64, vp]),
         "sw100_diff_bbox_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
         "sw100_batch_validate": (C.c_int, [vp, C.c_int]),
+        "sw100_utci_steps": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_int64, vp, vp]),
         **{name: (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]) for name in (
             "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
             "sw100_batch_flux_loop")},

@@ -3,6 +3,7 @@
 * :func:`svf_calculator`   <- ``solweig_gpu/shadow.py:409-625``
 * :func:`run_utci_window`  <- ``solweig_gpu/utci_process.py:477-1090``
 * :func:`utci_calculator`  <- ``solweig_gpu/calculate_utci.py:259-330``
+* :func:`recompute_utci_steps` <- ``solweig_gpu/utci_process.py:1093-1196``
 * :func:`run_exact_chain`  -- the whole chain for one site from host rasters
   (what ``compute_utci`` does between its raster I/O, utci_process.py:1376-1470)
 
@@ -231,6 +232,44 @@ def utci_calculator(Ta, RH, Tmrt, va10m):
     flat = [torch.as_tensor(np.asarray(x, F32) if not isinstance(x, torch.Tensor) else x,
                             dtype=torch.float32).reshape(-1) for x in (Ta, RH, Tmrt, va10m)]
     return E.utci(*flat).reshape(shape)
+
+
+def recompute_utci_steps(met_file, time_indices, tmrt_planes, buildings_dsm, dem):
+    """UTCI-only recompute of the steps ``time_indices`` from stored Tmrt
+    planes (utci_process.py:1093-1196, the met fast path for wind speed /
+    urban-heat-island edits): same arguments, errors and result
+    ((len(time_indices), rows, cols) float32, NaN outside buildings == 1) as
+    the reference, computed by the library's UTCI tail on the GPU."""
+    a = _np32(buildings_dsm)
+    rows, cols = a.shape
+    d = _np32(dem)
+    if d.shape != a.shape:
+        raise ValueError(f"dem shape {d.shape} != buildings_dsm shape {a.shape}")
+    indices = tuple(int(i) for i in time_indices)
+    if not indices:
+        raise ValueError("time_indices must be non-empty")
+    met_file = np.asarray(met_file)
+    for i in indices:
+        if not 0 <= i < met_file.shape[0]:
+            raise ValueError(f"time index {i} outside the met table ({met_file.shape[0]} steps)")
+        plane = tmrt_planes.get(i)
+        if plane is None:
+            raise ValueError(f"no published tmrt plane for timestep {i}")
+        if tuple(plane.shape) != (rows, cols):
+            raise ValueError(f"tmrt plane t={i} shape {tuple(plane.shape)} != tile {(rows, cols)}")
+    E.require_cuda()
+    dev = torch.device("cuda")
+    buildings = a - d
+    buildings[buildings < 2.] = 1.
+    buildings[buildings >= 2.] = 0.
+    rec = TS.utci_step_records(met_file, indices)
+    steps_d = E._table(rec, dev)
+    tmrt = torch.stack([torch.as_tensor(_np32(tmrt_planes[i])) for i in indices]).pin_memory().to(dev)
+    bld = E._dev(buildings, dev)
+    out = torch.empty((len(indices), rows, cols), dtype=torch.float32, device=dev)
+    N.call("sw100_utci_steps", E._ptr(steps_d), len(indices), E._ptr(tmrt), E._ptr(bld), None, rows * cols,
+           E._ptr(out), E._stream())
+    return E.to_host(out)
 
 
 def run_exact_chain(*, dsm, trees, dem, walls, aspect, scale, met_file, altitude, azimuth, zen, jday, dectime,

@@ -42,6 +42,8 @@ __global__ void time_loop_kernel(SitePlanes site, int rows, int cols, const sw10
                                  uint32_t out_mask, float* outputs);
 __global__ void pack_cubes_kernel(const float* sh, const float* veg, const float* vb, size_t npix, int n_patches,
                                   Single5 single, uint32_t* bits);
+__global__ void utci_steps_kernel(const sw100_time_step* steps, int n_steps, const float* tmrt,
+                                  const float* buildings, const float* windcoeff, int64_t npix, float* out);
 __global__ void utci_kernel(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n,
                             float* out);
 }  // namespace sw100
@@ -526,4 +528,21 @@ extern "C" int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, 
   svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
                                            site->vmax, out_planes, out_bits);
   return check_launch("svf_sweep_kernel");
+}
+
+extern "C" int sw100_utci_steps(const sw100_time_step* steps, int n_steps, const float* tmrt,
+                                const float* buildings, const float* windcoeff, int64_t npix, float* out,
+                                void* stream) {
+  int rc;
+  if (n_steps < 0 || npix < 0) return fail(SW100_E_ARG, "n_steps and npix must be >= 0");
+  if (n_steps == 0 || npix == 0) return 0;
+  if ((rc = check_ptr(steps, "steps")) || (rc = check_ptr(tmrt, "tmrt")) || (rc = check_ptr(buildings, "buildings")) ||
+      (rc = check_ptr(out, "out")))
+    return rc;
+  const int threads = 256;
+  const int bx = (int)std::min<int64_t>((npix + threads - 1) / threads, 148 * 4);
+  const dim3 grid(bx, std::min(n_steps, 65535));
+  utci_steps_kernel<<<grid, threads, 0, static_cast<cudaStream_t>(stream)>>>(steps, n_steps, tmrt, buildings,
+                                                                             windcoeff, npix, out);
+  return check_launch("utci_steps_kernel");
 }

@@ -300,6 +300,23 @@ def _utci_table(ta_mat: np.float32, rh32: np.float32):
     return pa_pows, k
 
 
+def utci_step_records(met_file, indices) -> np.ndarray:
+    """Time-step records carrying only what the UTCI tail reads (ta_mat,
+    rh32, ws32 and the UTCI table) for the forcing rows ``indices``, with
+    the reference's met reads and float32 roundings
+    (utci_process.py:1158-1191)."""
+    met_file = np.asarray(met_file)
+    uhii = met_file[:, 24] if met_file.shape[1] > 24 else np.zeros(met_file.shape[0])
+    rec = np.zeros(len(indices), N.TIME_STEP_DTYPE)
+    for k, i in enumerate(indices):
+        S = rec[k]
+        S["rh32"] = F32(met_file[i, 10])
+        S["ws32"] = F32(met_file[i, 9])
+        S["ta_mat"] = (F32(0) + F32(met_file[i, 11])) + F32(uhii[i])
+        S["utci_pa"], S["utci_k"] = _utci_table(S["ta_mat"], S["rh32"])
+    return rec
+
+
 # -------------------------------------------------------------- the series
 @dataclass
 class LandCoverProps:

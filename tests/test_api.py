@@ -183,3 +183,44 @@ def test_utci_calculator_against_oracle(cuda):
     # calm, mild conditions (the chain's usual range) stay within 1e-3 C
     calm = (va[5:] <= 4) & (ta[5:] <= 35)
     assert diff[calm].max() <= 1e-3
+
+
+def test_recompute_utci_steps_validates_like_the_reference():
+    d = load_golden("city36")
+    planes = {0: np.zeros((36, 36), np.float32)}
+    with pytest.raises(ValueError, match="non-empty"):
+        api.recompute_utci_steps(d["met"], [], planes, d["dsm"], d["dem"])
+    with pytest.raises(ValueError, match="outside the met table"):
+        api.recompute_utci_steps(d["met"], [99], planes, d["dsm"], d["dem"])
+    with pytest.raises(ValueError, match="no published tmrt plane"):
+        api.recompute_utci_steps(d["met"], [0, 1], planes, d["dsm"], d["dem"])
+    with pytest.raises(ValueError, match="shape"):
+        api.recompute_utci_steps(d["met"], [0], {0: np.zeros((5, 5), np.float32)}, d["dsm"], d["dem"])
+    with pytest.raises(ValueError, match="dem shape"):
+        api.recompute_utci_steps(d["met"], [0], planes, d["dsm"], d["dem"][:5])
+
+
+@pytest.mark.gpu
+def test_recompute_utci_steps_equals_a_full_run(cuda):
+    """Wind speed and urban heat island enter only the UTCI tail: the
+    fast path from the first run's Tmrt equals a full run with the edited
+    forcing, bit for bit."""
+    from oracle.svf import scene_from_rasters
+    d = load_golden("city36")
+    vegdsm, vegdsm2, bush, amax = scene_from_rasters(d["dsm"], d["trees"], d["dem"])
+    packed = api.svf_calculator(2, amax, d["dsm"], vegdsm, vegdsm2, bush, 1.0, packed=True)
+    kw = dict(a=d["dsm"], temp2=d["dem"], walls=d["walls_ref"], dirwalls=d["aspect_ref"], svf_bundle=packed,
+              altitude=d["altitude"], azimuth=d["azimuth"], zen=d["zen"], jday=d["jday"], dectime=d["dectime"],
+              altmax=d["altmax"], location=golden_location(d), scale=1.0, amaxvalue=d["amaxvalue"],
+              landcover_grid=d["landcover"], lc_class=d["lc_class"], requested_variables=("utci", "tmrt"))
+    base = api.run_utci_window(temp1=d["trees"].copy(), met_file=d["met"], **kw)
+    met2 = np.array(d["met"], copy=True)
+    if met2.shape[1] <= 24:
+        met2 = np.concatenate([met2, np.zeros((met2.shape[0], 25 - met2.shape[1]))], axis=1)
+    met2[:, 9] = met2[:, 9] * 1.7 + 0.3          # wind speed
+    met2[:, 24] = 1.25                            # urban heat island
+    edited = api.run_utci_window(temp1=d["trees"].copy(), met_file=met2, **kw)
+    assert_bits_equal(edited["tmrt"], base["tmrt"], "tmrt unchanged by wind / uhii")
+    idx = [3, 11, 12, 20]
+    fast = api.recompute_utci_steps(met2, idx, {i: base["tmrt"][i] for i in idx}, d["dsm"], d["dem"])
+    assert_bits_equal(fast, edited["utci"][idx], "utci fast path")

@@ -45,39 +45,62 @@ def _geotransform_tags(gt):
             (34735, 3, 4, struct.pack("<4H", 1, 1, 0, 0))]
 
 
-def tiff_bytes(data: np.ndarray, geotransform=None) -> bytes:
-    """Baseline float32 TIFF (one strip), with GeoTIFF geotransform tags
-    when ``geotransform`` (GDAL order: x0, dx, 0, y0, 0, dy) is given."""
-    a = np.ascontiguousarray(np.asarray(data, F32))
-    rows, cols = a.shape
+def tiff_bytes(data: np.ndarray, geotransform=None, band_metadata=None) -> bytes:
+    """Baseline float32 TIFF, one strip per band (bands stored as separate
+    planes), with GeoTIFF geotransform tags when ``geotransform`` (GDAL
+    order: x0, dx, 0, y0, 0, dy) is given and per-band metadata
+    (``band_metadata[b] = {"Time": ...}``, written as GDAL's metadata tag)."""
+    a = np.asarray(data, F32)
+    if a.ndim == 2:
+        a = a[None]
+    bands, rows, cols = a.shape
+    a = np.ascontiguousarray(a)
+    band_bytes = rows * cols * 4
     pixels = a.astype("<f4").tobytes()
     entries = [(256, 4, 1, struct.pack("<I", cols)), (257, 4, 1, struct.pack("<I", rows)),
-               (258, 3, 1, struct.pack("<H", 32)), (259, 3, 1, struct.pack("<H", 1)),
-               (262, 3, 1, struct.pack("<H", 1)), (273, 4, 1, None), (277, 3, 1, struct.pack("<H", 1)),
-               (278, 4, 1, struct.pack("<I", rows)), (279, 4, 1, struct.pack("<I", len(pixels))),
-               (284, 3, 1, struct.pack("<H", 1)), (339, 3, 1, struct.pack("<H", 3))]
+               (258, 3, bands, struct.pack(f"<{bands}H", *([32] * bands))), (259, 3, 1, struct.pack("<H", 1)),
+               (262, 3, 1, struct.pack("<H", 1)), (273, 4, bands, None),
+               (277, 3, 1, struct.pack("<H", bands)), (278, 4, 1, struct.pack("<I", rows)),
+               (279, 4, bands, struct.pack(f"<{bands}I", *([band_bytes] * bands))),
+               (284, 3, 1, struct.pack("<H", 2 if bands > 1 else 1)),
+               (339, 3, bands, struct.pack(f"<{bands}H", *([3] * bands)))]
+    if bands > 1:
+        entries.append((338, 3, bands - 1, struct.pack(f"<{bands - 1}H", *([0] * (bands - 1)))))
     if geotransform is not None:
         entries += _geotransform_tags(geotransform)
+    if band_metadata:
+        items = "".join(f'<Item name="{k}" sample="{b}">{v}</Item>' for b, md in enumerate(band_metadata)
+                        for k, v in (md or {}).items())
+        xml = f"<GDALMetadata>{items}</GDALMetadata>".encode() + b"\0"
+        entries.append((42112, 2, len(xml), xml))
     entries.sort(key=lambda e: e[0])
     ifd_off = 8
     ifd_len = 2 + 12 * len(entries) + 4
     extra = bytearray()
     extra_off = ifd_off + ifd_len
-    fixed = []
+    placed = []
+    strip_slot = None
     for tag, typ, count, payload in entries:
-        if payload is not None and len(payload) > 4:
-            fixed.append((tag, typ, count, struct.pack("<I", extra_off + len(extra))))
+        if payload is None:                                  # StripOffsets: filled below
+            payload = bytes(4 * count)
+            if len(payload) > 4:
+                strip_slot = extra_off + len(extra)
+        if len(payload) > 4:
+            placed.append((tag, typ, count, struct.pack("<I", extra_off + len(extra))))
             extra += payload
             if len(extra) % 2:
                 extra += b"\0"
         else:
-            fixed.append((tag, typ, count, payload))
+            placed.append((tag, typ, count, payload))
     data_off = extra_off + len(extra)
+    offsets = struct.pack(f"<{bands}I", *[data_off + b * band_bytes for b in range(bands)])
+    if strip_slot is not None:
+        extra[strip_slot - extra_off:strip_slot - extra_off + len(offsets)] = offsets
     out = bytearray(b"II*\0" + struct.pack("<I", ifd_off))
-    out += struct.pack("<H", len(fixed))
-    for tag, typ, count, payload in fixed:
-        if payload is None:                     # StripOffsets
-            payload = struct.pack("<I", data_off)
+    out += struct.pack("<H", len(placed))
+    for tag, typ, count, payload in placed:
+        if tag == 273 and strip_slot is None:
+            payload = offsets
         out += struct.pack("<HHI", tag, typ, count) + payload.ljust(4, b"\0")
     out += struct.pack("<I", 0)
     out += extra
@@ -85,8 +108,11 @@ def tiff_bytes(data: np.ndarray, geotransform=None) -> bytes:
     return bytes(out)
 
 
-def read_tiff(buf: bytes):
-    """(array, geotransform or None) of a TIFF written by :func:`tiff_bytes`."""
+def read_tiff(buf: bytes, with_metadata: bool = False):
+    """(array, geotransform or None[, band metadata]) of a TIFF written by
+    :func:`tiff_bytes`; the array is (rows, cols) for one band, else
+    (bands, rows, cols)."""
+    import re
     if buf[:4] != b"II*\0":
         raise ValueError("not a little-endian TIFF")
     (ifd,) = struct.unpack_from("<I", buf, 4)
@@ -94,23 +120,37 @@ def read_tiff(buf: bytes):
     tags = {}
     for k in range(n):
         tag, typ, count, val = struct.unpack_from("<HHI4s", buf, ifd + 2 + 12 * k)
-        size = {3: 2, 4: 4, 12: 8}[typ] * count
-        raw = val[:size] if size <= 4 else buf[struct.unpack("<I", val)[0]:struct.unpack("<I", val)[0] + size]
-        fmt = {3: "H", 4: "I", 12: "d"}[typ]
-        tags[tag] = struct.unpack(f"<{count}{fmt}", raw)
+        size = {2: 1, 3: 2, 4: 4, 12: 8}[typ] * count
+        if size <= 4:
+            raw = val[:size]
+        else:
+            (off,) = struct.unpack("<I", val)
+            raw = buf[off:off + size]
+        tags[tag] = raw if typ == 2 else struct.unpack(f"<{count}{ {3: 'H', 4: 'I', 12: 'd'}[typ] }", raw)
     cols, rows = tags[256][0], tags[257][0]
-    if tags[258][0] != 32 or tags[339][0] != 3 or tags[259][0] != 1:
+    bands = tags.get(277, (1,))[0]
+    if any(b != 32 for b in tags[258]) or any(f != 3 for f in tags[339]) or tags[259][0] != 1:
         raise ValueError("only uncompressed float32 images are read")
-    off, nbytes = tags[273][0], tags[279][0]
-    if nbytes != rows * cols * 4 or off + nbytes > len(buf):
-        raise ValueError("truncated image data")
-    a = np.frombuffer(buf, "<f4", rows * cols, off).reshape(rows, cols).astype(F32)
+    planes = []
+    for b in range(bands):
+        off, nbytes = tags[273][b], tags[279][b]
+        if nbytes != rows * cols * 4 or off + nbytes > len(buf):
+            raise ValueError("truncated image data")
+        planes.append(np.frombuffer(buf, "<f4", rows * cols, off).reshape(rows, cols).astype(F32))
+    a = planes[0] if bands == 1 else np.stack(planes)
     gt = None
     if 33550 in tags and 33922 in tags:
         sx, sy, _ = tags[33550]
         x0, y0 = tags[33922][3], tags[33922][4]
         gt = (x0, sx, 0.0, y0, 0.0, -sy)
-    return a, gt
+    if not with_metadata:
+        return a, gt
+    md = [dict() for _ in range(bands)]
+    if 42112 in tags:
+        xml = tags[42112].rstrip(b"\0").decode()
+        for name, sample, value in re.findall(r'<Item name="([^"]+)" sample="(\d+)">([^<]*)</Item>', xml):
+            md[int(sample)][name] = value
+    return a, gt, md
 
 
 # ------------------------------------------------------------ packed bits

@@ -411,6 +411,57 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
                     const float* gsrc, float* state, uint32_t out_mask, float* outputs, void* stream);
 
 /* ---------------------------------------------------------------- UTCI -- */
+/* ---------------------------------------------------- learned preview -- */
+/* Kernels of the learned SVF preview (a small U-Net, BF16 on the tensor
+ * cores with FP32 accumulation).  No counterpart in the reference: the
+ * reference recomputes SVF exactly for every edit (shadow.py:409-625 /
+ * solweig_core/sparse_work.py); the preview is a fast approximate edit path
+ * whose error is judged, and replaced when too large, by the exact windowed
+ * recompute (sw100_svf_window).
+ *
+ * Activations are NHWC bf16; a layer reads / writes channels [coff, coff +
+ * C) of a buffer of `stride` channels (C, coff, stride multiples of 16).
+ * 3 x 3 convolutions use same padding and tap t = 3 (dy + 1) + (dx + 1);
+ * weights: forward layout [t][cout][cin] bf16, data-gradient layout
+ * [8 - t][cin][cout] bf16 (a data gradient is a forward convolution of the
+ * output gradient with it), float32 master weights / gradients in the
+ * forward layout. */
+int sw100_nn_conv3x3(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* wt,
+                     const float* bias, int cout, void* y, int ystride, int ycoff, int relu, int out_f32,
+                     void* stream);
+/* dw (float32, forward layout) and dbias (may be NULL) += the gradients of
+ * a 3 x 3 convolution given its input x and output gradient dy. */
+int sw100_nn_conv3x3_wgrad(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* dy,
+                           int cout, int dstride, int dcoff, float* dw, float* dbias, void* stream);
+/* float32 master weights -> bf16 forward layout wf and data-gradient layout wd (may be NULL). */
+int sw100_nn_weights(const float* master, int cin, int cout, void* wf, void* wd, void* stream);
+/* dy *= (y > 0) (ReLU backward on the layer's output y). */
+int sw100_nn_relu_bwd(void* dy, const void* y, int64_t npix, int c, int dstride, int dcoff, int ystride, int ycoff,
+                      void* stream);
+/* 2 x 2 average pooling (h, w: input size) and its backward (x = dY of
+ * size h/2 x w/2, y = dX, accumulate: add into dX). */
+int sw100_nn_pool2(const void* x, int n, int h, int w, int c, int xstride, int xcoff, void* y, int ystride, int ycoff,
+                   int backward, int accumulate, void* stream);
+/* nearest 2x upsampling (h, w: input size) and its backward (x = dY of
+ * size 2h x 2w, y = dX). */
+int sw100_nn_up2(const void* x, int n, int h, int w, int c, int xstride, int xcoff, void* y, int ystride, int ycoff,
+                 int backward, void* stream);
+/* mean squared error over the central box (margin cells cut on each side)
+ * and the first nc of c channels of float32 NHWC pred / target; loss
+ * (float32, may be NULL) += the mean, dpred (bf16, may be NULL) = its
+ * gradient. */
+int sw100_nn_mse(const float* pred, const float* target, int n, int h, int w, int c, int nc, int margin, void* dpred,
+                 float* loss, void* stream);
+/* One bias-corrected Adam step (Kingma & Ba 2015) on float32 parameters. */
+int sw100_nn_adam(float* param, const float* grad, float* m, float* v, int64_t n, float lr, float b1, float b2,
+                  float eps, int step, void* stream);
+/* Network input of n square windows of `size` cells at device origins
+ * {r0, c0} (int32 pairs) of a site: heights above ground of the building
+ * DSM, canopy top and trunk zone, / 40 m, bf16 NHWC with 16 channels (3
+ * used); cells outside the grid read 0.  dem may be NULL (flat 0). */
+int sw100_nn_input(const float* dsm, const float* vegdsm, const float* vegdsm2, const float* dem, int rows, int cols,
+                   const int32_t* origins, int n, int size, void* x, void* stream);
+
 /* UTCI-only recompute of whole steps: the met fast path of
  * utci_process.py:1093-1196 (recompute_utci_steps), for wind speed / urban
  * heat island edits that leave Tmrt unchanged.  steps: n_steps records whose

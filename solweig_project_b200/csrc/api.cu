@@ -13,6 +13,8 @@
 #include <mutex>
 #include <string>
 
+#include <cuda_bf16.h>
+
 #include "sw_common.cuh"
 #include "sw_internal.cuh"
 
@@ -46,6 +48,29 @@ __global__ void utci_steps_kernel(const sw100_time_step* steps, int n_steps, con
                                   const float* buildings, const float* windcoeff, int64_t npix, float* out);
 __global__ void utci_kernel(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n,
                             float* out);
+__global__ void nn_conv3x3_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
+                                  const __nv_bfloat16* Wt, const float* bias, int Cout, void* Yv, int ystride,
+                                  int ycoff, int relu, int out_f32);
+__global__ void nn_wgrad_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
+                                const __nv_bfloat16* dY, int Cout, int dstride, int dcoff, float* dW, float* dbias,
+                                int rows_per_block);
+__global__ void nn_weights_kernel(const float* Wm, int Cin, int Cout, __nv_bfloat16* Wf, __nv_bfloat16* Wd);
+__global__ void nn_relu_bwd_kernel(__nv_bfloat16* dY, const __nv_bfloat16* Y, int64_t npix, int C, int dstride,
+                                   int dcoff, int ystride, int ycoff);
+__global__ void nn_pool2_kernel(const __nv_bfloat16* X, int N, int H, int W, int C, int xstride, int xcoff,
+                                __nv_bfloat16* Y, int ystride, int ycoff);
+__global__ void nn_pool2_bwd_kernel(const __nv_bfloat16* dY, int N, int H, int W, int C, int dstride, int dcoff,
+                                    __nv_bfloat16* dX, int xstride, int xcoff, int accumulate);
+__global__ void nn_up2_kernel(const __nv_bfloat16* X, int N, int H, int W, int C, int xstride, int xcoff,
+                              __nv_bfloat16* Y, int ystride, int ycoff);
+__global__ void nn_up2_bwd_kernel(const __nv_bfloat16* dY, int N, int H, int W, int C, int dstride, int dcoff,
+                                  __nv_bfloat16* dX, int xstride, int xcoff);
+__global__ void nn_mse_kernel(const float* pred, const float* target, int N, int H, int W, int C, int nc, int m,
+                              float inv_count, __nv_bfloat16* dpred, float* loss);
+__global__ void nn_adam_kernel(float* p, const float* grad, float* m, float* v, int64_t n, float lr, float b1,
+                               float b2, float eps, float c1, float c2);
+__global__ void nn_input_kernel(const float* dsm, const float* vegdsm, const float* vegdsm2, const float* dem,
+                                int rows, int cols, const int2* origins, int n, int S, __nv_bfloat16* X);
 }  // namespace sw100
 
 using namespace sw100;
@@ -546,3 +571,157 @@ extern "C" int sw100_utci_steps(const sw100_time_step* steps, int n_steps, const
                                                                              windcoeff, npix, out);
   return check_launch("utci_steps_kernel");
 }
+
+// ------------------------------------------------------------ learned preview
+namespace {
+
+int check_act(int N, int H, int W, int C, int stride, int coff, const char* what) {
+  if (N <= 0 || H <= 0 || W <= 0 || C <= 0) return fail(SW100_E_SIZE, "%s: empty tensor", what);
+  if (C % 16 || stride % 16 || coff % 16 || coff + C > stride)
+    return fail(SW100_E_ARG, "%s: channels %d at offset %d of %d must be multiples of 16 inside the stride", what, C,
+                coff, stride);
+  if ((int64_t)N * H * W * stride >= (int64_t)1 << 31) return fail(SW100_E_SIZE, "%s: tensor too large", what);
+  return 0;
+}
+
+int grid1(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
+
+}  // namespace
+
+extern "C" {
+
+int sw100_nn_conv3x3(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* wt,
+                     const float* bias, int cout, void* y, int ystride, int ycoff, int relu, int out_f32,
+                     void* stream) {
+  int rc;
+  if ((rc = check_ptr(x, "x")) || (rc = check_ptr(wt, "wt")) || (rc = check_ptr(y, "y"))) return rc;
+  if ((rc = check_act(n, h, w, cin, xstride, xcoff, "x")) || (rc = check_act(n, h, w, cout, ystride, ycoff, "y")))
+    return rc;
+  const int co_tiles = (cout + 63) / 64;
+  if ((int64_t)n * co_tiles > 65535 || h > 65535) return fail(SW100_E_SIZE, "conv grid too large");
+  dim3 grid((w + 63) / 64, h, n * co_tiles);
+  nn_conv3x3_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const __nv_bfloat16*>(x), n, h, w, cin, xstride, xcoff, static_cast<const __nv_bfloat16*>(wt), bias,
+      cout, y, ystride, ycoff, relu, out_f32);
+  return check_launch("nn_conv3x3_kernel");
+}
+
+int sw100_nn_conv3x3_wgrad(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* dy,
+                           int cout, int dstride, int dcoff, float* dw, float* dbias, void* stream) {
+  int rc;
+  if ((rc = check_ptr(x, "x")) || (rc = check_ptr(dy, "dy")) || (rc = check_ptr(dw, "dw"))) return rc;
+  if ((rc = check_act(n, h, w, cin, xstride, xcoff, "x")) || (rc = check_act(n, h, w, cout, dstride, dcoff, "dy")))
+    return rc;
+  const int rows = n * h;
+  const int rows_per_block = std::max(1, rows / 148);
+  dim3 grid((rows + rows_per_block - 1) / rows_per_block, 9, ((cout + 63) / 64) * ((cin + 63) / 64));
+  nn_wgrad_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const __nv_bfloat16*>(x), n, h, w, cin, xstride, xcoff, static_cast<const __nv_bfloat16*>(dy), cout,
+      dstride, dcoff, dw, dbias, rows_per_block);
+  return check_launch("nn_wgrad_kernel");
+}
+
+int sw100_nn_weights(const float* master, int cin, int cout, void* wf, void* wd, void* stream) {
+  int rc;
+  if ((rc = check_ptr(master, "master")) || (rc = check_ptr(wf, "wf"))) return rc;
+  if (cin <= 0 || cout <= 0 || cin % 16 || cout % 16) return fail(SW100_E_ARG, "channels must be multiples of 16");
+  nn_weights_kernel<<<grid1(9 * cin * cout), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      master, cin, cout, static_cast<__nv_bfloat16*>(wf), static_cast<__nv_bfloat16*>(wd));
+  return check_launch("nn_weights_kernel");
+}
+
+int sw100_nn_relu_bwd(void* dy, const void* y, int64_t npix, int c, int dstride, int dcoff, int ystride, int ycoff,
+                      void* stream) {
+  int rc;
+  if ((rc = check_ptr(dy, "dy")) || (rc = check_ptr(y, "y"))) return rc;
+  if (npix <= 0 || c <= 0 || dcoff + c > dstride || ycoff + c > ystride) return fail(SW100_E_ARG, "bad relu extents");
+  nn_relu_bwd_kernel<<<grid1(npix * c), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<__nv_bfloat16*>(dy), static_cast<const __nv_bfloat16*>(y), npix, c, dstride, dcoff, ystride, ycoff);
+  return check_launch("nn_relu_bwd_kernel");
+}
+
+int sw100_nn_pool2(const void* x, int n, int h, int w, int c, int xstride, int xcoff, void* y, int ystride, int ycoff,
+                   int backward, int accumulate, void* stream) {
+  int rc;
+  if ((rc = check_ptr(x, "x")) || (rc = check_ptr(y, "y"))) return rc;
+  if (h % 2 || w % 2) return fail(SW100_E_ARG, "pooling needs even sizes");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!backward) {
+    if ((rc = check_act(n, h, w, c, xstride, xcoff, "x")) || (rc = check_act(n, h / 2, w / 2, c, ystride, ycoff, "y")))
+      return rc;
+    nn_pool2_kernel<<<grid1((int64_t)n * h * w * c / 4), 256, 0, st>>>(static_cast<const __nv_bfloat16*>(x), n, h, w, c,
+                                                                        xstride, xcoff, static_cast<__nv_bfloat16*>(y),
+                                                                        ystride, ycoff);
+    return check_launch("nn_pool2_kernel");
+  }
+  // backward: x = dY (h/2 x w/2), y = dX (h x w)
+  if ((rc = check_act(n, h / 2, w / 2, c, xstride, xcoff, "dy")) || (rc = check_act(n, h, w, c, ystride, ycoff, "dx")))
+    return rc;
+  nn_pool2_bwd_kernel<<<grid1((int64_t)n * h * w * c), 256, 0, st>>>(static_cast<const __nv_bfloat16*>(x), n, h, w, c,
+                                                                      xstride, xcoff, static_cast<__nv_bfloat16*>(y),
+                                                                      ystride, ycoff, accumulate);
+  return check_launch("nn_pool2_bwd_kernel");
+}
+
+int sw100_nn_up2(const void* x, int n, int h, int w, int c, int xstride, int xcoff, void* y, int ystride, int ycoff,
+                 int backward, void* stream) {
+  int rc;
+  if ((rc = check_ptr(x, "x")) || (rc = check_ptr(y, "y"))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!backward) {
+    if ((rc = check_act(n, h, w, c, xstride, xcoff, "x")) || (rc = check_act(n, 2 * h, 2 * w, c, ystride, ycoff, "y")))
+      return rc;
+    nn_up2_kernel<<<grid1((int64_t)n * 4 * h * w * c), 256, 0, st>>>(static_cast<const __nv_bfloat16*>(x), n, h, w, c,
+                                                                      xstride, xcoff, static_cast<__nv_bfloat16*>(y),
+                                                                      ystride, ycoff);
+    return check_launch("nn_up2_kernel");
+  }
+  // backward: x = dY (2h x 2w), y = dX (h x w)
+  if ((rc = check_act(n, 2 * h, 2 * w, c, xstride, xcoff, "dy")) || (rc = check_act(n, h, w, c, ystride, ycoff, "dx")))
+    return rc;
+  nn_up2_bwd_kernel<<<grid1((int64_t)n * h * w * c), 256, 0, st>>>(static_cast<const __nv_bfloat16*>(x), n, h, w, c,
+                                                                    xstride, xcoff, static_cast<__nv_bfloat16*>(y),
+                                                                    ystride, ycoff);
+  return check_launch("nn_up2_bwd_kernel");
+}
+
+int sw100_nn_mse(const float* pred, const float* target, int n, int h, int w, int c, int nc, int margin, void* dpred,
+                 float* loss, void* stream) {
+  int rc;
+  if ((rc = check_ptr(pred, "pred")) || (rc = check_ptr(target, "target"))) return rc;
+  if (n <= 0 || h <= 2 * margin || w <= 2 * margin || nc <= 0 || nc > c || margin < 0)
+    return fail(SW100_E_ARG, "bad loss extents");
+  const float inv = 1.f / ((float)n * (h - 2 * margin) * (w - 2 * margin) * nc);
+  nn_mse_kernel<<<grid1((int64_t)n * h * w * c), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      pred, target, n, h, w, c, nc, margin, inv, static_cast<__nv_bfloat16*>(dpred), loss);
+  return check_launch("nn_mse_kernel");
+}
+
+int sw100_nn_adam(float* param, const float* grad, float* m, float* v, int64_t n, float lr, float b1, float b2,
+                  float eps, int step, void* stream) {
+  int rc;
+  if ((rc = check_ptr(param, "param")) || (rc = check_ptr(grad, "grad")) || (rc = check_ptr(m, "m")) ||
+      (rc = check_ptr(v, "v")))
+    return rc;
+  if (n <= 0 || step <= 0) return fail(SW100_E_ARG, "n and step must be positive");
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  nn_adam_kernel<<<grid1(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(param, grad, m, v, n, lr, b1, b2, eps, c1, c2);
+  return check_launch("nn_adam_kernel");
+}
+
+int sw100_nn_input(const float* dsm, const float* vegdsm, const float* vegdsm2, const float* dem, int rows, int cols,
+                   const int32_t* origins, int n, int size, void* x, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(dsm, "dsm")) || (rc = check_ptr(vegdsm, "vegdsm")) || (rc = check_ptr(vegdsm2, "vegdsm2")) ||
+      (rc = check_ptr(origins, "origins")) || (rc = check_ptr(x, "x")))
+    return rc;
+  if (n <= 0 || size <= 0) return fail(SW100_E_ARG, "n and size must be positive");
+  nn_input_kernel<<<grid1((int64_t)n * size * size), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      dsm, vegdsm, vegdsm2, dem, rows, cols, reinterpret_cast<const int2*>(origins), n, size,
+      static_cast<__nv_bfloat16*>(x));
+  return check_launch("nn_input_kernel");
+}
+
+}  // extern "C"
+

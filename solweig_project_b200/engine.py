@@ -140,6 +140,7 @@ class DeviceSite:
         self.t = {
             "dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
             "bush": _dev(bush, d) if self.bush_any else None, "buildings": _dev(buildings, d),
+            "dem": _dev(np.asarray(dem, F32), d),
             "walls": _dev(np.asarray(walls, F32), d),
             "aspect_rad": _dev((np.asarray(aspect_deg, F32) * F32(np.pi)) / F32(180.), d),
             "windcoeff": _dev(np.ones((self.rows, self.cols), F32) if windcoeff is None else
@@ -242,7 +243,8 @@ class DeviceSite:
         old_bush, old_hmax = self.bush_any, self.hmax
         d = self.device
         self.t.update(dsm=_dev(a, d), vegdsm=_dev(vegdsm, d), vegdsm2=_dev(vegdsm2, d),
-                      bush=_dev(bush, d) if bush.max() > 0 else None, buildings=_dev(buildings, d))
+                      bush=_dev(bush, d) if bush.max() > 0 else None, buildings=_dev(buildings, d),
+                      dem=_dev(np.asarray(dem, F32), d))
         if walls is not None:
             self.t["walls"] = _dev(np.asarray(walls, F32), d)
         if aspect_deg is not None:
@@ -309,8 +311,16 @@ class DeviceSite:
         (r0, c0) with the given arrays (any of dsm / trees / dem, same block
         shape): only the block travels to the device and the block is the
         edit rectangle.  Same result and fallbacks as :meth:`edit_svf`."""
+        blk = next(np.asarray(x, F32) for x in (dsm, trees, dem) if x is not None)
+        self.update_rasters_block(r0, c0, dsm=dsm, trees=trees, dem=dem)
+        return self.refresh_svf_after_block(r0, c0, blk.shape[0], blk.shape[1], patch_option)
+
+    def update_rasters_block(self, r0, c0, dsm=None, trees=None, dem=None):
+        """Replace the block at (r0, c0) of the edited inputs (host copies
+        and device march rasters); the SVF result is left as it was (see
+        :meth:`refresh_svf_after_block`)."""
         if self.svf_result is None or self.host is None:
-            raise RuntimeError("edit_svf_block needs a site built from rasters and a computed SVF")
+            raise RuntimeError("block edits need a site built from rasters and a computed SVF")
         blk = next(np.asarray(x, F32) for x in (dsm, trees, dem) if x is not None)
         h, w = blk.shape
         if r0 < 0 or c0 < 0 or r0 + h > self.rows or c0 + w > self.cols or h == 0 or w == 0:
@@ -321,18 +331,37 @@ class DeviceSite:
                 self.host[name][sl] = np.asarray(v, F32)
         a, t1, t2 = self.host["dsm"], self.host["trees"], self.host["dem"]
         vegdsm_b, vegdsm2_b, bush_b, _, bld_b = march_inputs(a[sl], t1[sl], t2[sl])
-        amax = self.amax if self.amax_fixed else \
-            F32(max(a.max(), float((np.maximum(t1, 0) + t2).max())))
-        hb = float(max(np.abs(a[sl]).max(), np.abs(vegdsm_b).max(), np.abs(vegdsm2_b).max()))
-        if self.bush_any or bush_b.max() > 0 or amax != self.amax or \
-                not (np.isfinite(a[sl]).all() and np.isfinite(vegdsm_b).all() and np.isfinite(vegdsm2_b).all()):
-            return self.edit_svf(a, t1, t2, patch_option=patch_option)
-        for name, v in (("dsm", a[sl]), ("vegdsm", vegdsm_b), ("vegdsm2", vegdsm2_b), ("buildings", bld_b)):
+        self._pending_full = bool(self.bush_any or bush_b.max() > 0 or not (
+            np.isfinite(a[sl]).all() and np.isfinite(vegdsm_b).all() and np.isfinite(vegdsm2_b).all()))
+        if not self.amax_fixed:
+            amax = F32(max(a.max(), float((np.maximum(t1, 0) + t2).max())))
+            self._pending_full = self._pending_full or amax != self.amax
+        for name, v in (("dsm", a[sl]), ("vegdsm", vegdsm_b), ("vegdsm2", vegdsm2_b), ("buildings", bld_b),
+                        ("dem", t2[sl])):
             self.t[name].view(self.rows, self.cols)[sl].copy_(_upload(torch.from_numpy(np.ascontiguousarray(v)),
                                                                       self.device))
         # bounds only need to stay above the true maxima (early exit, height-blind patches)
+        hb = float(max(np.abs(a[sl]).max(), np.abs(vegdsm_b).max(), np.abs(vegdsm2_b).max()))
         self.vmax = F32(max(float(self.vmax), float(a[sl].max()), float(vegdsm_b.max()), float(vegdsm2_b.max())))
         self.hmax = max(self.hmax, hb)
+
+    def refresh_svf_after_block(self, r0, c0, h, w, patch_option=2) -> dict:
+        """Exact SVF update for rasters changed inside the block (r0, c0, h,
+        w) by :meth:`update_rasters_block`: the windowed recompute, or a full
+        sweep when the edit changed the step tables or brought bush."""
+        if getattr(self, "_pending_full", False):
+            a, t1, t2 = self.host["dsm"], self.host["trees"], self.host["dem"]
+            vegdsm, vegdsm2, bush, amax, _ = march_inputs(a, t1, t2)
+            self._set_march_stats(a, vegdsm, vegdsm2, bush)
+            if bush.max() > 0:
+                self.t["bush"] = _dev(bush, self.device)
+            if not self.amax_fixed:
+                self.amax = amax
+            self._cache = {k: v for k, v in self._cache.items() if k[0] not in ("svf", "svf_host", "corridor")}
+            self._pending_full = False
+            self.run_svf(patch_option)
+            return {"mode": "full", "rect": None, "window": (0, self.rows - 1, 0, self.cols - 1),
+                    "pixels": self.rows * self.cols}
         return self._window_update((r0, r0 + h - 1, c0, c0 + w - 1), patch_option)
 
     def launch_svf(self, planes, bits, patch_option=2):

@@ -173,6 +173,18 @@ int sw100_svf_window(const sw100_site_planes* site, int rows, int cols, const sw
                      const int32_t window[4], float* planes, uint32_t* bits, void* workspace,
                      int64_t workspace_bytes, void* stream);
 
+/* Exact SVF planes and bits of the pixels of a box after an edit inside it,
+ * one thread per (pixel, patch) march (low latency for small boxes), then
+ * the planes re-accumulated from the bits in the sweep's order.  Pixels
+ * outside the box are untouched (their marches may read the box: use
+ * sw100_svf_window for an exact update of the whole affected area).  Same
+ * tables, corridor descriptors, workspace and refusals as
+ * sw100_svf_window.  No counterpart in the reference: it serves the
+ * learned preview, which takes the box's own pixels from the exact march. */
+int sw100_svf_box(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                  const sw100_step* steps, const int32_t* corridor, const int32_t box[4], float* planes,
+                  uint32_t* bits, void* workspace, int64_t workspace_bytes, void* stream);
+
 /* Bounding box of the cells whose march rasters (dsm, vegdsm, vegdsm2,
  * bush) differ between two sites of the same grid, bit for bit (the
  * composed-source diff C of solweig_core/sparse_work.py:199-251).  Writes

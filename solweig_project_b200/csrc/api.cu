@@ -26,6 +26,8 @@ __global__ void svf_sweep_kernel(const float4* src4, int rows, int cols, const s
 __global__ void svf_window_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                   const sw100_step* steps, const int32_t* corridor, float vmax, int4 rect, int4 win,
                                   float* out, uint32_t* bits);
+__global__ void svf_box_pairs_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
+                                     const sw100_step* steps, float vmax, int4 box, uint32_t* bits);
 __global__ void diff_bbox_kernel(const float4* a, const float4* b, int rows, int cols, int* box);
 __global__ void box_init_kernel(int* box);
 __global__ void pack_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
@@ -263,6 +265,37 @@ int sw100_svf_window(const sw100_site_planes* site, int rows, int cols, const sw
   svf_window_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, corridor, site->vmax,
                                             make_int4(rect[0], rect[1], rect[2], rect[3]),
                                             make_int4(w0, w1, w2, w3), planes, bits);
+  return check_launch("svf_window_kernel");
+}
+
+int sw100_svf_box(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                  const sw100_step* steps, const int32_t* corridor, const int32_t box[4], float* planes,
+                  uint32_t* bits, void* workspace, int64_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_march(site))) return rc;
+  if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(corridor, "corridor")) ||
+      (rc = check_ptr(box, "box")) || (rc = check_ptr(planes, "planes")) || (rc = check_ptr(bits, "bits")))
+    return rc;
+  if (site->bush_any) return fail(SW100_E_ARG, "box recompute refuses rasters with bush");
+  if (box[0] < 0 || box[1] >= rows || box[2] < 0 || box[3] >= cols || box[0] > box[1] || box[2] > box[3])
+    return fail(SW100_E_ARG, "box must be a non-empty box inside the grid");
+  int64_t need = 0;
+  if ((rc = sw100_svf_window_workspace_bytes(rows, cols, &need))) return rc;
+  if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  float4* src4 = static_cast<float4*>(workspace);
+  if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
+  const int4 b4 = make_int4(box[0], box[1], box[2], box[3]);
+  const int64_t pairs = (int64_t)(box[1] - box[0] + 1) * (box[3] - box[2] + 1) * SW100_MAX_PATCHES;
+  const int blocks = (int)std::min<int64_t>((pairs + 127) / 128, 148 * 32);
+  svf_box_pairs_kernel<<<blocks, 128, 0, st>>>(src4, rows, cols, plan, steps, site->vmax, b4, bits);
+  if ((rc = check_launch("svf_box_pairs_kernel"))) return rc;
+  // re-accumulate from the new bits: a rectangle outside the grid, read by no march
+  dim3 block(32, 4);
+  dim3 grid((box[3] - box[2] + 1 + 31) / 32, (box[1] - box[0] + 1 + 3) / 4);
+  svf_window_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, corridor, site->vmax,
+                                            make_int4(-4, -4, -4, -4), b4, planes, bits);
   return check_launch("svf_window_kernel");
 }
 

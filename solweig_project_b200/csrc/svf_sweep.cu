@@ -449,6 +449,42 @@ __global__ void box_init_kernel(int* box) {
   }
 }
 
+// The patch marches of every (pixel, patch) pair of a box, one thread per
+// pair, writing the pixels' patch bits (atomic bit updates: each thread
+// owns its bit).  Followed by svf_window_kernel over the box with a
+// rectangle that no march reads, which re-accumulates the planes from the
+// new bits in the sweep's order.  Rasters without bush only.
+__global__ void __launch_bounds__(128) svf_box_pairs_kernel(
+    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan,
+    const sw100_step* __restrict__ steps, float vmax, int4 box, uint32_t* __restrict__ bits) {
+  const int bw = box.w - box.z + 1, bh = box.y - box.x + 1;
+  const int np = plan->n_patches;
+  const int64_t total = (int64_t)bw * bh * np;
+  const size_t npix = (size_t)rows * cols;
+  const bool finite = plan->all_finite != 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(i % np);
+    const int64_t px = i / np;
+    const int r = box.x + (int)(px / bw), c = box.z + (int)(px % bw);
+    const size_t p = (size_t)r * cols + c;
+    const float4 self = src4[p];
+    const int off = plan->step_offset[q], n = plan->step_count[q];
+    float sh, veg, vb;
+    if (finite)
+      march_patch_fast(src4, rows, cols, r, c, self.x, self.z, steps + off, n, vmax, sh, veg, vb);
+    else
+      march_patch(src4, rows, cols, r, c, self.x, self.z, 0.f, steps + off, n, nullptr, false, vmax, sh, veg, vb);
+    const uint32_t bit = 1u << (q & 31);
+    const int w = q >> 5;
+    uint32_t* wsh = &bits[(0 * SW100_CUBE_WORDS + w) * npix + p];
+    uint32_t* wveg = &bits[(1 * SW100_CUBE_WORDS + w) * npix + p];
+    uint32_t* wvb = &bits[(2 * SW100_CUBE_WORDS + w) * npix + p];
+    if (sh != 0.f) atomicOr(wsh, bit); else atomicAnd(wsh, ~bit);
+    if (veg != 0.f) atomicOr(wveg, bit); else atomicAnd(wveg, ~bit);
+    if (n <= 1 ? (vb == 1.f) : (vb != 0.f)) atomicOr(wvb, bit); else atomicAnd(wvb, ~bit);
+  }
+}
+
 // Bounding box of the cells where two packed march sources differ (bit
 // comparison of all four channels); box = {rmin, rmax, cmin, cmax}, set to
 // {INT_MAX, -1, INT_MAX, -1} by the caller.

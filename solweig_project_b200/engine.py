@@ -288,6 +288,24 @@ class DeviceSite:
                                       T.patch_shift_bounds(plan, steps, desc))
         return hit[1], hit[2], hit[3]
 
+    def exact_svf_box(self, r0, c0, h, w, patch_option=2):
+        """Exact SVF planes and bits of the box's own pixels after an edit
+        of the rasters inside it, one thread per (pixel, patch) march
+        (sw100_svf_box); pixels outside keep what they hold."""
+        plan_d, steps_d, _, _, _ = self.svf_tables(patch_option)
+        _, desc_d, _ = self._corridor(patch_option)
+        key = ("window_ws",)
+        if key not in self._cache:
+            self._cache[key] = torch.empty(N.workspace_bytes("sw100_svf_window_workspace_bytes", self.rows,
+                                                             self.cols), dtype=torch.uint8, device=self.device)
+        wws = self._cache[key]
+        r = self.svf_result
+        site = self.site_struct()
+        box = (r0, r0 + h - 1, c0, c0 + w - 1)
+        N.call("sw100_svf_box", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), _ptr(desc_d),
+               (C.c_int32 * 4)(*box), _ptr(r.planes), _ptr(r.bits), _ptr(wws), wws.numel(), _stream())
+        return {"mode": "box", "rect": box, "window": box, "pixels": h * w}
+
     def _window_update(self, rect, patch_option=2) -> dict:
         plan_d, steps_d, n_steps, _, _ = self.svf_tables(patch_option)
         desc, desc_d, bounds = self._corridor(patch_option)
@@ -336,10 +354,12 @@ class DeviceSite:
         if not self.amax_fixed:
             amax = F32(max(a.max(), float((np.maximum(t1, 0) + t2).max())))
             self._pending_full = self._pending_full or amax != self.amax
-        for name, v in (("dsm", a[sl]), ("vegdsm", vegdsm_b), ("vegdsm2", vegdsm2_b), ("buildings", bld_b),
-                        ("dem", t2[sl])):
-            self.t[name].view(self.rows, self.cols)[sl].copy_(_upload(torch.from_numpy(np.ascontiguousarray(v)),
-                                                                      self.device))
+        names = ("dsm", "vegdsm", "vegdsm2", "buildings", "dem")
+        stack = np.stack([a[sl], vegdsm_b, vegdsm2_b, bld_b, t2[sl]]).astype(F32)
+        TRANSFER["h2d"] += stack.nbytes
+        dev = torch.from_numpy(stack).to(self.device)      # one small copy for the five planes
+        for k, name in enumerate(names):
+            self.t[name].view(self.rows, self.cols)[sl].copy_(dev[k])
         # bounds only need to stay above the true maxima (early exit, height-blind patches)
         hb = float(max(np.abs(a[sl]).max(), np.abs(vegdsm_b).max(), np.abs(vegdsm2_b).max()))
         self.vmax = F32(max(float(self.vmax), float(a[sl].max()), float(vegdsm_b.max()), float(vegdsm2_b.max())))

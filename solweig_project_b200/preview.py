@@ -329,13 +329,22 @@ def train(net: UNet, sites, planes, *, steps=600, batch=8, size=256, margin=64, 
 
 
 class SvfPreview:
-    """Edit preview on a site whose exact SVF is known: predicted change of
-    the 15 SVF planes over the central block of a window, spliced into the
-    site's planes; exact fallback when the net's error on the known pre-edit
-    window exceeds ``threshold`` (mean absolute SVF error)."""
+    """Edit preview on a site whose exact SVF is known.
 
-    def __init__(self, net: UNet, size=256, margin=64, threshold=0.02):
+    For an edited box: the net's change of the 15 SVF planes over the
+    central block of a window around the box (net(after) - net(before),
+    added to the exact planes before the edit), then the exact windowed
+    recompute restricted to the box's own pixels (their planes and patch
+    bits exact: the edited cells change most).  Cells of the block outside
+    the box keep their patch bits from before the edit.  When the net's
+    mean absolute error on the window before the edit -- where the exact
+    answer is known -- exceeds ``threshold``, the exact windowed recompute
+    runs instead.  The net's forward pass is replayed from a CUDA graph."""
+
+    def __init__(self, net: UNet, size=256, margin=64, threshold=0.02, graph=True):
         self.net, self.size, self.margin, self.threshold = net, size, margin, threshold
+        self.use_graph = graph
+        self._graph = None
 
     def window_origin(self, site, r0, c0, h, w):
         """Window whose central block covers the edited box (clipped so the
@@ -349,29 +358,200 @@ class SvfPreview:
         cc = min(max(cc, 0), max(0, site.cols - self.size))
         return rr, cc
 
+    def _forward(self, b):
+        if not self.use_graph:
+            return self.net.forward(b)
+        if self._graph is None:
+            self.net.forward(b)                       # warm-up outside the capture
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.net.forward(b)
+            self._graph = g
+        self._graph.replay()
+        return b["out"]
+
     def edit(self, site: E.DeviceSite, r0, c0, dsm=None, trees=None, dem=None):
         """Apply a block edit with the preview; returns a record with the
-        mode ("preview" or "exact"), the window and the net's pre-edit error."""
+        mode ("preview" or "exact"), the window and the net's error before
+        the edit."""
         blk = next(np.asarray(x, np.float32) for x in (dsm, trees, dem) if x is not None)
         h, w = blk.shape
         orr, occ = self.window_origin(site, r0, c0, h, w)
         S, m = self.size, self.margin
         b = self.net.buffers(2, S)
         planes = site.svf_result.planes
-        # net on the window before the edit (row 0) ...
-        window_inputs(site, [(orr, occ)], S, b["x"][0:1])
-        # ... apply the edit to the rasters (SVF untouched), net after it (row 1)
+        window_inputs(site, [(orr, occ)], S, b["x"][0:1])          # before the edit
         site.update_rasters_block(r0, c0, dsm=dsm, trees=trees, dem=dem)
-        window_inputs(site, [(orr, occ)], S, b["x"][1:2])
-        out = self.net.forward(b)
+        if getattr(site, "_pending_full", False):                 # new step tables / bush: exact only
+            return {"mode": "exact", "window": (orr, occ), "pre_error": None,
+                    "exact": site.refresh_svf_after_block(r0, c0, h, w)}
+        window_inputs(site, [(orr, occ)], S, b["x"][1:2])          # after it
+        out = self._forward(b)
         ra, ca = orr + m, occ + m
         cs = S - 2 * m
         exact_pre = planes[:N_OUT, ra:ra + cs, ca:ca + cs].permute(1, 2, 0)
         pre = out[0, m:S - m, m:S - m, :N_OUT]
-        err = (pre - exact_pre).abs().mean()
-        if float(err.item()) > self.threshold:
-            info = site.refresh_svf_after_block(r0, c0, h, w)
-            return {"mode": "exact", "window": (orr, occ), "pre_error": float(err.item()), **info}
+        err = float((pre - exact_pre).abs().mean().item())
+        if err > self.threshold:
+            return {"mode": "exact", "window": (orr, occ), "pre_error": err,
+                    "exact": site.refresh_svf_after_block(r0, c0, h, w)}
         new = (exact_pre + (out[1, m:S - m, m:S - m, :N_OUT] - pre)).clamp_(0.0, 1.0)
         planes[:N_OUT, ra:ra + cs, ca:ca + cs] = new.permute(2, 0, 1)
-        return {"mode": "preview", "window": (orr, occ), "pre_error": float(err.item())}
+        refresh_statics(planes, ra, ca, cs, cs, site.params.transVeg)
+        site.exact_svf_box(r0, c0, h, w)
+        return {"mode": "preview", "window": (orr, occ), "pre_error": err}
+
+
+# ------------------------------------------------------------ statics
+def refresh_statics(planes: torch.Tensor, r0, c0, h, w, trans_veg=0.03):
+    """Time-loop statics (planes 16-18) of a block from its SVF planes
+    (utci_process.py:864-897): svfbuveg, tan(acos(sqrt(svf))) and
+    tan(asin(exp(log(1 - max(svf + svfveg - 1, 0)) / 2)))."""
+    sl = (slice(r0, r0 + h), slice(c0, c0 + w))
+    svf, svfveg = planes[0][sl], planes[11][sl]
+    planes[16][sl] = svf - (1.0 - svfveg) * (1.0 - trans_veg)
+    planes[17][sl] = torch.tan(torch.acos(torch.sqrt(svf)))
+    tmp = (svf + svfveg - 1.0).clamp(min=0.0)
+    planes[18][sl] = torch.tan(torch.asin(torch.exp(torch.log(1.0 - tmp) / 2.0)))
+
+
+# --------------------------------------------------------- training data
+def training_sites(n_sites=8, side=512, seed=77):
+    """Seeded synthetic cities with their exact SVF (the sweep is the
+    teacher): [(DeviceSite, planes)]."""
+    from . import synthetic
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_sites):
+        c = synthetic.make_city(side, side, seed=int(seed * 100 + k), density=float(rng.uniform(0.10, 0.45)),
+                                canopy_cover=float(rng.uniform(0.0, 0.30)))
+        s = E.DeviceSite(c.dsm, c.trees, c.dem, c.walls, c.aspect, c.scale, amaxvalue=48.0)
+        res = s.run_svf()
+        out.append((s, res.planes))
+    return out
+
+
+def random_edit(site: E.DeviceSite, rng, block=128):
+    """A seeded building edit inside a block: add a building, remove the
+    built cells of a box, or raise / lower the built cells of a box by
+    5-30 m.  Returns (kind, r0, c0, new_dsm_block)."""
+    h = int(rng.integers(10, 41))
+    w = int(rng.integers(10, 41))
+    r0 = int(rng.integers(block, site.rows - block - h))
+    c0 = int(rng.integers(block, site.cols - block - w))
+    sl = (slice(r0, r0 + h), slice(c0, c0 + w))
+    dsm, dem = site.host["dsm"][sl].copy(), site.host["dem"][sl]
+    kind = ("add", "remove", "height")[int(rng.integers(3))]
+    built = dsm - dem >= 2.0
+    if kind == "add" or not built.any():
+        kind = "add"
+        dsm = np.maximum(dsm, dem + np.float32(rng.uniform(5, 30)))
+    elif kind == "remove":
+        dsm = np.where(built, dem, dsm).astype(np.float32)
+    else:
+        dz = np.float32(rng.uniform(5, 30) * (1 if rng.random() < 0.5 else -1))
+        dsm = np.where(built, np.maximum(dem + 2.5, dsm + dz), dsm).astype(np.float32)
+    return kind, r0, c0, dsm.astype(np.float32)
+
+
+def evaluate_edits(net: UNet, site: E.DeviceSite, series, n_edits=50, seed=5, threshold=1.0):
+    """Seeded edits on a site with exact SVF: per edit, the exact windowed
+    recompute, the preview and the stale (unchanged) SVF, with device times
+    and, over the edit window's central block, the SVF mean absolute error
+    and the Tmrt RMSE of the whole 24-step chain against the exact chain.
+    Shadows are recomputed exactly in every variant (the sun march reads the
+    edited rasters); the patch cubes stay those before the edit for the
+    preview and stale variants."""
+    rng = np.random.default_rng(seed)
+    prev = SvfPreview(net, threshold=threshold)
+    r = site.svf_result
+    base_planes, base_bits = r.planes.clone(), r.bits.clone()
+    s_struct, s_dev = site.upload_series(series)
+    rows = []
+    S, m = prev.size, prev.margin
+    cs = S - 2 * m
+
+    def tmrt():
+        site.state.zero_()
+        return site.run_time_loop(series, requested=("tmrt",), series_dev=(s_struct, s_dev))["tmrt"]
+
+    for k in range(n_edits):
+        kind, r0, c0, new = random_edit(site, rng)
+        h, w = new.shape
+        old = site.host["dsm"][r0:r0 + h, c0:c0 + w].copy()
+        orr, occ = prev.window_origin(site, r0, c0, h, w)
+        win = (slice(orr + m, orr + m + cs), slice(occ + m, occ + m + cs))
+        # exact
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        site.edit_svf_block(r0, c0, dsm=new)
+        e1.record()
+        torch.cuda.synchronize()
+        t_exact = e0.elapsed_time(e1)
+        exact_planes = r.planes[:N_OUT][(slice(None),) + win].clone()
+        t_ex = tmrt()[(slice(None),) + win].clone()
+        # stale SVF, edited rasters
+        r.planes.copy_(base_planes)
+        r.bits.copy_(base_bits)
+        t_st = tmrt()[(slice(None),) + win].clone()
+        stale_planes = r.planes[:N_OUT][(slice(None),) + win].clone()
+        # preview from the state before the edit
+        site.update_rasters_block(r0, c0, dsm=old)
+        e0.record()
+        info = prev.edit(site, r0, c0, dsm=new)
+        e1.record()
+        torch.cuda.synchronize()
+        t_prev = e0.elapsed_time(e1)
+        prev_planes = r.planes[:N_OUT][(slice(None),) + win].clone()
+        t_pv = tmrt()[(slice(None),) + win].clone()
+        # back to the base state for the next edit
+        site.update_rasters_block(r0, c0, dsm=old)
+        r.planes.copy_(base_planes)
+        r.bits.copy_(base_bits)
+        valid = torch.isfinite(t_ex) & torch.isfinite(t_pv) & torch.isfinite(t_st)
+        rmse = lambda a: float(torch.sqrt(((a - t_ex)[valid] ** 2).mean()).item())  # noqa: E731
+        rows.append({"kind": kind, "mode": info["mode"], "ms_exact": t_exact, "ms_preview": t_prev,
+                     "svf_mae_preview": float((prev_planes - exact_planes).abs().mean().item()),
+                     "svf_mae_stale": float((stale_planes - exact_planes).abs().mean().item()),
+                     "tmrt_rmse_preview": rmse(t_pv), "tmrt_rmse_stale": rmse(t_st)})
+    return rows
+
+
+WEIGHTS = __import__("os").path.join(__import__("os").path.dirname(__file__), "data", "preview_weights.npz")
+
+
+def load_pretrained(path: str = WEIGHTS, seed: int = 0) -> UNet:
+    """The network with the weights trained by :func:`main` (the file
+    shipped with the package: 3000 steps of 8 windows of 256 x 256 cells
+    from 12 seeded 512 x 512 cities)."""
+    net = UNet(seed=seed)
+    with np.load(path) as z:
+        net.load_state_dict({"master": z["master"], "step": int(z["step"])})
+    return net
+
+
+def main(argv=None):
+    """Train the preview on seeded cities and save its weights:
+    python -m solweig_project_b200.preview --out weights.npz [--steps N]"""
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--sites", type=int, default=12)
+    ap.add_argument("--side", type=int, default=512)
+    args = ap.parse_args(argv)
+    from . import build
+    build.build()
+    data = training_sites(args.sites, args.side)
+    net = UNet(seed=0)
+    rep = train(net, [s for s, _ in data], [p for _, p in data], steps=args.steps, log_every=100)
+    st = net.state_dict()
+    np.savez_compressed(args.out, master=st["master"], step=st["step"], loss_first=rep.loss_first,
+                        loss_last=rep.loss_last, seconds=rep.seconds, windows=rep.windows)
+    print(f"trained {rep.steps} steps ({rep.windows} windows) in {rep.seconds:.1f} s: "
+          f"loss {rep.loss_first:.4g} -> {rep.loss_last:.4g}; saved {args.out}")
+
+
+if __name__ == "__main__":
+    main()

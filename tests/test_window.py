@@ -159,3 +159,26 @@ def test_block_edits_equal_full_sweeps(cuda):
         assert np.array_equal(site.svf_result.planes.cpu().numpy().view(np.uint32),
                               full.planes.cpu().numpy().view(np.uint32)), k
         assert np.array_equal(site.svf_result.bits.cpu().numpy(), full.bits.cpu().numpy()), k
+
+
+@pytest.mark.gpu
+def test_box_recompute_is_exact_inside_the_box(cuda):
+    from solweig_project_b200.engine import DeviceSite
+    city = _scene(12, 100, 110)
+    site = DeviceSite(city.dsm, city.trees, city.dem, city.walls, city.aspect, city.scale, amaxvalue=45.0)
+    before = site.run_svf()
+    planes0, bits0 = before.planes.clone(), before.bits.clone()
+    dsm = city.dsm.copy()
+    blk = np.full((14, 9), F32(22.0))
+    dsm[40:54, 50:59] = blk
+    site.update_rasters_block(40, 50, dsm=blk)
+    site.exact_svf_box(40, 50, 14, 9)
+    ref = DeviceSite(dsm, city.trees, city.dem, city.walls, city.aspect, city.scale, amaxvalue=45.0).run_svf()
+    box = (slice(None), slice(40, 54), slice(50, 59))
+    got_p, got_b = site.svf_result.planes.cpu().numpy(), site.svf_result.bits.cpu().numpy()
+    assert np.array_equal(got_p[box].view(np.uint32), ref.planes.cpu().numpy()[box].view(np.uint32))
+    assert np.array_equal(got_b[(slice(None),) + box], ref.bits.cpu().numpy()[(slice(None),) + box])
+    # pixels outside the box keep what they held
+    mask = np.ones((100, 110), bool)
+    mask[40:54, 50:59] = False
+    assert np.array_equal(got_p[:, mask].view(np.uint32), planes0.cpu().numpy()[:, mask].view(np.uint32))

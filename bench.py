@@ -43,6 +43,9 @@ WORKLOADS = {
     # name: (side, h_max, description)
     "exact500": (500, 40.0, "500x500 px @1 m, 24 hourly steps, SVF sweep + shadows + fluxes + Tmrt + UTCI"),
     "tile4096": (4096, 120.0, "4096x4096 px @1 m, buildings up to 120 m, 24 hourly steps, full exact chain"),
+    "preview1024": (1024, 40.0, "learned SVF preview of seeded building edits (add / remove / height change, "
+                                "10-40 px boxes) on a held-out 1024x1024 city vs the exact windowed recompute and "
+                                "the full sweep; Tmrt of the 24-step chain over the edit window"),
     "batched64": (None, 40.0, "64 seeded sites, sides log-uniform 128-1024 px, density 10-45 %, canopy 0-30 %, "
                               "latitudes 0-60 N, 24 hourly steps each; one launch per stage for all sites, "
                               "replayed as a CUDA graph, autotuned launch shapes"),
@@ -336,6 +339,62 @@ def run_batched(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_preview(args, world, rank, local):
+    """The learned-preview workload: per seeded edit, the preview's device
+    latency against the exact windowed recompute, and SVF / Tmrt errors
+    against the exact chain (with the stale SVF as the method without it)."""
+    import torch
+    from solweig_project_b200 import build, synthetic
+    from solweig_project_b200 import preview as PV
+    from solweig_project_b200.engine import DeviceSite
+    build.build()
+    if rank != 0:
+        return
+    net = PV.load_pretrained()
+    c = synthetic.make_city(1024, 1024, seed=4242, density=0.3, canopy_cover=0.15)
+    site = DeviceSite(c.dsm, c.trees, c.dem, c.walls, c.aspect, c.scale, landcover=c.landcover,
+                      lc_class=synthetic.default_lc_class(), amaxvalue=48.0)
+    site.run_svf()
+    met = synthetic.make_met(1234)
+    geo = synthetic.load_sun_geometry("single")
+    ser = site.build_series(met, geo["altitude"], geo["azimuth"], geo["zen"], geo["jday"], geo["dectime"],
+                            geo["altmax"], dict(synthetic.DEFAULT_LOCATION))
+    PV.evaluate_edits(net, site, ser, n_edits=max(1, args.warmup), seed=99)      # warm-up (graph capture etc.)
+    n_edits = max(20, 20 * args.steps)
+    with ClockSampler(local) as clocks:
+        rows = PV.evaluate_edits(net, site, ser, n_edits=n_edits, seed=5)
+    full = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        site.launch_svf(site.svf_result.planes, site.svf_result.bits)
+        e1.record()
+        torch.cuda.synchronize()
+        full.append(e0.elapsed_time(e1))
+    mean = lambda k: float(np.mean([r[k] for r in rows]))  # noqa: E731
+    med = lambda k: float(np.median([r[k] for r in rows]))  # noqa: E731
+    full_ms = float(np.median(full))
+    clk = clocks.summary()
+    print(json.dumps({
+        "metric": "SVF edit latency, learned preview (device ms per edit)", "value": med("ms_preview"), "unit": "ms",
+        "n_gpus": 1, "steps": n_edits, "warmup": args.warmup, "ms_per_step": med("ms_preview"),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+        "data": "synthetic (held-out seeded 1024x1024 city, seeded edits)",
+        "config": {"workload": "preview1024", "description": WORKLOADS["preview1024"][2], "edits": n_edits,
+                   "net_params": net.n_params, "window": "256x256 (128x128 block + 64 px context)"},
+        "exact_window_ms": med("ms_exact"), "full_sweep_ms": full_ms,
+        "speedup_vs_exact_window": med("ms_exact") / med("ms_preview"),
+        "speedup_vs_full_sweep": full_ms / med("ms_preview"),
+        "svf_mae": {"preview": mean("svf_mae_preview"), "stale": mean("svf_mae_stale")},
+        "tmrt_rmse_K": {"preview": mean("tmrt_rmse_preview"), "stale": mean("tmrt_rmse_stale")},
+        "modes": {m: sum(r["mode"] == m for r in rows) for m in ("preview", "exact")},
+        "gpu_launches": None,
+        "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "e2e": {"value": med("ms_preview"), "unit": "ms", "h2d_bytes_per_step": 5 * 4 * 40 * 40,
+                "d2h_bytes_per_step": 4},
+    }), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -352,6 +411,12 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     if args.workload == "batched64":
         run_batched(args, world, rank, local)
+        return
+    if args.workload == "preview1024":
+        run_preview(args, world, rank, local)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
         return
 
     from solweig_project_b200 import _native as N

@@ -9,7 +9,7 @@ if REPO not in sys.path:
     sys.path.insert(0, REPO)
 
 GOLDEN = os.path.join(REPO, "tests", "golden")
-FULL_CASES = ("city36", "city24x40_s05", "dem_bush")
+FULL_CASES = ("city36", "city24x40_s05", "dem_bush", "bush24")
 SVF_CASES = FULL_CASES + ("strip1x16", "lowveg16")
 
 

@@ -68,6 +68,11 @@ CASES = {
                  {"n_buildings": 4, "n_trees": 4, "side_range": (3, 8)}),
     "strip1x16": (1, 16, 14, 1.0, 0.0, False,
                   {"n_buildings": 2, "n_trees": 3, "side_range": (1, 3)}),
+    # bush: ground lowered to -0.25 x canopy under the trees of the left half,
+    # so that vegdem2 == 0 != vegdem there and the reference's bush raster
+    # (utci_process.py:669-672) is non-zero
+    "bush24": (24, 28, 16, 1.0, 0.0, True,
+               {"n_buildings": 3, "n_trees": 7, "side_range": (3, 8), "bush_left_half": True}),
     # low vegetation only: patches of the 78 degree ring stop after one step,
     # which is where vbshvegsh can take the value 2
     "lowveg16": (16, 16, 15, 1.0, 0.0, False,
@@ -102,8 +107,14 @@ def run_case(name, spec, ref):
     import solweig_gpu.walls_aspect as rwa
 
     rows, cols, seed, scale, dem_level, full, kw = spec
+    kw = dict(kw)
+    bush_left_half = kw.pop("bush_left_half", False)
     city = synthetic.make_city(rows, cols, seed, scale=scale, dem_level=dem_level,
                                with_walls=False, **kw)
+    if bush_left_half:
+        sel = (city.trees > 0) & (np.arange(cols)[None, :] < cols // 2)
+        city.dem[sel] = np.float32(-0.25) * city.trees[sel]
+        city.dsm = np.maximum(city.dsm, city.dem).astype(np.float32)
     out = {"rows": rows, "cols": cols, "seed": seed, "scale": scale, "dem_level": dem_level,
            "dsm": city.dsm, "trees": city.trees, "dem": city.dem, "landcover": city.landcover}
     t0 = time.time()

@@ -435,12 +435,18 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
  * C) of a buffer of `stride` channels (C, coff, stride multiples of 16).
  * 3 x 3 convolutions use same padding and tap t = 3 (dy + 1) + (dx + 1);
  * weights: forward layout [t][cout][cin] bf16, data-gradient layout
- * [8 - t][cin][cout] bf16 (a data gradient is a forward convolution of the
- * output gradient with it), float32 master weights / gradients in the
+ * [8 - t][cin][cout] bf16, float32 master weights / gradients in the
  * forward layout. */
-int sw100_nn_conv3x3(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* wt,
-                     const float* bias, int cout, void* y, int ystride, int ycoff, int relu, int out_f32,
-                     void* stream);
+/* y[., ycoff + co] = act(bias[co] + sum_{t, ci} x[shifted, xcoff + ci] *
+ * wt[t][co][ci]) on the 5th-generation tensor cores (tcgen05.mma with the
+ * accumulator in tensor memory; cout <= 128); relu: max(0, .), out_f32:
+ * float32 output instead of bf16, bias may be NULL.  A data gradient is
+ * this call on the output gradient with the data-gradient weight layout.
+ * err (device int32, may be NULL) is set to 1 when a bounded wait of the
+ * kernel expired. */
+int sw100_nn_conv3x3_tc(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* wt,
+                        const float* bias, int cout, void* y, int ystride, int ycoff, int relu, int out_f32,
+                        int32_t* err, void* stream);
 /* dw (float32, forward layout) and dbias (may be NULL) += the gradients of
  * a 3 x 3 convolution given its input x and output gradient dy. */
 int sw100_nn_conv3x3_wgrad(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* dy,

@@ -36,9 +36,9 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noal
            "sw100_abi_version", "sw100_last_error", "sw100_launch_count", "sw100_svf_window_workspace_bytes",
            "sw100_svf_window", "sw100_diff_bbox_workspace_bytes", "sw100_diff_bbox", "sw100_batch_validate",
            "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
-           "sw100_batch_flux_loop", "sw100_utci_steps", "sw100_nn_conv3x3", "sw100_nn_conv3x3_wgrad",
+           "sw100_batch_flux_loop", "sw100_utci_steps", "sw100_nn_conv3x3_wgrad",
            "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2", "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam",
-           "sw100_nn_input", "sw100_svf_box")
+           "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc")
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
 
@@ -168,7 +168,7 @@ def load(path: str = LIB_PATH):
                                     vp, C.c_int64, vp]),
         "sw100_batch_validate": (C.c_int, [vp, C.c_int]),
         "sw100_utci_steps": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_int64, vp, vp]),
-        "sw100_nn_conv3x3": (C.c_int, [vp] + [C.c_int] * 6 + [vp, vp, C.c_int, vp] + [C.c_int] * 4 + [vp]),
+        "sw100_nn_conv3x3_tc": (C.c_int, [vp] + [C.c_int] * 6 + [vp, vp, C.c_int, vp] + [C.c_int] * 4 + [vp, vp]),
         "sw100_nn_conv3x3_wgrad": (C.c_int, [vp] + [C.c_int] * 6 + [vp] + [C.c_int] * 3 + [vp, vp, vp]),
         "sw100_nn_weights": (C.c_int, [vp, C.c_int, C.c_int, vp, vp, vp]),
         "sw100_nn_relu_bwd": (C.c_int, [vp, vp, C.c_int64] + [C.c_int] * 5 + [vp]),

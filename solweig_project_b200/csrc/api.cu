@@ -50,9 +50,9 @@ __global__ void utci_steps_kernel(const sw100_time_step* steps, int n_steps, con
                                   const float* buildings, const float* windcoeff, int64_t npix, float* out);
 __global__ void utci_kernel(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n,
                             float* out);
-__global__ void nn_conv3x3_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
-                                  const __nv_bfloat16* Wt, const float* bias, int Cout, void* Yv, int ystride,
-                                  int ycoff, int relu, int out_f32);
+__global__ void nn_conv3x3_tc_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
+                                     const __nv_bfloat16* Wt, const float* bias, int Cout, void* Yv, int ystride,
+                                     int ycoff, int relu, int out_f32, int* err);
 __global__ void nn_wgrad_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
                                 const __nv_bfloat16* dY, int Cout, int dstride, int dcoff, float* dW, float* dbias,
                                 int rows_per_block);
@@ -623,20 +623,27 @@ int grid1(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
 
 extern "C" {
 
-int sw100_nn_conv3x3(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* wt,
-                     const float* bias, int cout, void* y, int ystride, int ycoff, int relu, int out_f32,
-                     void* stream) {
+int sw100_nn_conv3x3_tc(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* wt,
+                        const float* bias, int cout, void* y, int ystride, int ycoff, int relu, int out_f32,
+                        int32_t* err, void* stream) {
   int rc;
   if ((rc = check_ptr(x, "x")) || (rc = check_ptr(wt, "wt")) || (rc = check_ptr(y, "y"))) return rc;
   if ((rc = check_act(n, h, w, cin, xstride, xcoff, "x")) || (rc = check_act(n, h, w, cout, ystride, ycoff, "y")))
     return rc;
-  const int co_tiles = (cout + 63) / 64;
-  if ((int64_t)n * co_tiles > 65535 || h > 65535) return fail(SW100_E_SIZE, "conv grid too large");
-  dim3 grid((w + 63) / 64, h, n * co_tiles);
-  nn_conv3x3_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+  if (cout > 128) return fail(SW100_E_ARG, "the tensor-core convolution takes at most 128 output channels");
+  const int64_t total = (int64_t)n * h * w;
+  const int64_t blocks = (total + 127) / 128;
+  const int smem = 3 * 2 * 4 * 4096;   // three stages of A and B tiles (4 K steps of 4 KB each)
+  static bool attr_set = false;    // the attribute is per function and process: set it once
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(nn_conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return fail((int)e, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    attr_set = true;
+  }
+  nn_conv3x3_tc_kernel<<<(unsigned)blocks, 128, smem, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const __nv_bfloat16*>(x), n, h, w, cin, xstride, xcoff, static_cast<const __nv_bfloat16*>(wt), bias,
-      cout, y, ystride, ycoff, relu, out_f32);
-  return check_launch("nn_conv3x3_kernel");
+      cout, y, ystride, ycoff, relu, out_f32, err);
+  return check_launch("nn_conv3x3_tc_kernel");
 }
 
 int sw100_nn_conv3x3_wgrad(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* dy,

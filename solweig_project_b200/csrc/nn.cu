@@ -1,6 +1,7 @@
 // Kernels of the learned SVF preview: a small U-Net in BF16 with FP32
-// accumulation on the tensor cores (mma.sync m16n8k16), trained on the GPU
-// by these forward and backward kernels.
+// accumulation on the tensor cores (tcgen05.mma for the convolutions'
+// forward and data-gradient passes, mma.sync m16n8k16 for the weight
+// gradients), trained on the GPU by these forward and backward kernels.
 //
 // Layout: activations NHWC bf16 with a channel stride (a buffer may hold a
 // concatenation: a layer reads / writes channels [coff, coff + C) of a
@@ -12,12 +13,11 @@
 //                    channel roles swapped, so dgrad is a forward conv)
 //   master / grads  float32 in the forward layout, bias float32[co].
 //
-// Convolution as an implicit GEMM: a block owns 64 consecutive pixels of
-// one image row (M) and 64 output channels (N); K runs over (tap, 16
-// input channels).  The A tile (64 px x 16 ch) and the B tile (64 co x 16
-// ch) are staged in shared memory (rows padded to 48 bytes: conflict-free
-// fragment loads), each of the 4 warps issues 8 mma per K step for its 16
-// pixels.
+// Convolutions are implicit GEMMs.  Forward and data gradient: tcgen05.mma
+// (below).  Weight gradient: a block reduces 64 output channels (M) x 64
+// input channels (N) over a run of pixels (K) with mma.sync; its tiles are
+// staged in shared memory with rows padded to 48 bytes (conflict-free
+// fragment loads).
 #include <cstdint>
 #include <cuda_bf16.h>
 
@@ -25,9 +25,7 @@
 
 namespace sw100 {
 
-constexpr int kNnPix = 64;   // pixels per block
-constexpr int kNnCo = 64;    // output channels per block
-constexpr int kPad = 24;     // bf16 per staged row (16 used)
+constexpr int kPad = 24;     // bf16 per staged row of the weight-gradient tiles (16 used)
 
 __device__ __forceinline__ uint32_t ld_smem_u32(const __nv_bfloat16* p) {
   return *reinterpret_cast<const uint32_t*>(p);
@@ -41,84 +39,225 @@ __device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, const uint
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// Y[n, h, w, ycoff + co] = act(bias[co] + sum_{t, ci} X[n, h + dy, w + dx, xcoff + ci] * Wt[t][co][ci])
-// grid: (ceil(W / 64), H, N * ceil(Cout / 64)); block 128.
-// out_f32: write float32 instead of bf16.  relu: max(0, .).
-__global__ void __launch_bounds__(128) nn_conv3x3_kernel(const __nv_bfloat16* __restrict__ X, int N, int H, int W,
-                                                         int Cin, int xstride, int xcoff,
-                                                         const __nv_bfloat16* __restrict__ Wt,
-                                                         const float* __restrict__ bias, int Cout, void* Yv,
-                                                         int ystride, int ycoff, int relu, int out_f32) {
-  __shared__ __align__(16) __nv_bfloat16 As[kNnPix][kPad];
-  __shared__ __align__(16) __nv_bfloat16 Bs[kNnCo][kPad];
-  const int n_co_tiles = (Cout + kNnCo - 1) / kNnCo;
-  const int n = blockIdx.z / n_co_tiles;
-  const int co0 = (blockIdx.z % n_co_tiles) * kNnCo;
-  const int h = blockIdx.y;
-  const int w0 = blockIdx.x * kNnPix;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int g = lane >> 2, tq = lane & 3;
-  float acc[8][4];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+// ------------------------------------------------- tcgen05 convolution
+// The same 3 x 3 convolution on the 5th-generation tensor cores: one CTA
+// (4 warps) owns 128 consecutive pixels of the flattened (n, h, w) index
+// (M = 128) and every output channel (N = Cout, 16..128); K runs over
+// (tap, 16 input channels).  A pipeline stage holds 4 K steps: per step the
+// 128 x 16 A tile and the Cout x 16 B tile in the no-swizzle K-major
+// core-matrix layout (8 rows x 16 bytes per core matrix; the two 8-element
+// halves of K 128 bytes apart, row groups 256 bytes apart), filled by
+// cp.async straight from global memory.  Three stages rotate: the copies of
+// stage g + 2 run while the MMAs of stage g do; one thread issues
+// the stage's tcgen05.mma (kind::f16, BF16 x BF16 -> FP32) into a TMEM
+// accumulator and tcgen05.commit arrives on the stage's mbarrier when they
+// have read it.  The epilogue reads the accumulator
+// with tcgen05.ld (warp w owns TMEM lanes 32 w .. 32 w + 31 = its pixels).
+// Every wait is bounded: on expiry the CTA records an error, stops issuing
+// and still frees its TMEM.
+namespace tc {
 
-  for (int t = 0; t < 9; ++t) {
-    const int dy = t / 3 - 1, dx = t % 3 - 1;
-    const int hs = h + dy;
-    for (int ci0 = 0; ci0 < Cin; ci0 += 16) {
-      // stage A: pixel p = tid / 2, channels ci0 + 8 * (tid & 1) .. +8
-      {
-        const int p = tid >> 1, half = tid & 1;
-        const int ws = w0 + p + dx;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (hs >= 0 && hs < H && ws >= 0 && ws < W)
-          v = *reinterpret_cast<const uint4*>(X + (((size_t)n * H + hs) * W + ws) * xstride + xcoff + ci0 + 8 * half);
-        *reinterpret_cast<uint4*>(&As[p][8 * half]) = v;
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; false when it gave up
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); ++i)
+    if (mbar_try_wait(addr, parity)) return true;
+  return false;
+}
+
+// 64-bit shared-memory matrix descriptor: no swizzle, K-major, LBO / SBO in bytes
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+  return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, M x N
+__device__ __forceinline__ uint32_t instr_desc(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+// core-matrix offset (bytes) of row r, K half h in a 16-wide K-major tile
+__device__ __forceinline__ int core_off(int r, int h) { return (r >> 3) * 256 + h * 128 + (r & 7) * 16; }
+
+}  // namespace tc
+
+// K steps of 16 per pipeline stage, the shared-memory bytes of a stage's A
+// (and B) tiles, and the stages in flight
+constexpr int kTcStepsPerStage = 4;
+constexpr int kTcStageBytes = kTcStepsPerStage * 4096;
+constexpr int kTcStages = 3;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+__global__ void __launch_bounds__(128) nn_conv3x3_tc_kernel(const __nv_bfloat16* __restrict__ X, int N, int H, int W,
+                                                            int Cin, int xstride, int xcoff,
+                                                            const __nv_bfloat16* __restrict__ Wt,
+                                                            const float* __restrict__ bias, int Cout, void* Yv,
+                                                            int ystride, int ycoff, int relu, int out_f32,
+                                                            int* __restrict__ err) {
+  // dynamic shared memory: kTcStages A stage buffers, then kTcStages B
+  // stage buffers, 1024-byte aligned; 96 KB per CTA also caps the CTAs per
+  // SM at 2, so TMEM (<= 128 columns each) is never oversubscribed
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  __shared__ __align__(8) uint64_t mbar[kTcStages];
+  __shared__ uint32_t tmem_base;
+  const uint32_t a_base = tc::smem_u32(tc_smem);
+  const uint32_t b_base = a_base + kTcStages * kTcStageBytes;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t total = (int64_t)N * H * W;
+  const int64_t p0 = (int64_t)blockIdx.x * 128;
+  const int ncols = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : 128);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_base)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int k = 0; k < kTcStages; ++k) tc::mbar_init(tc::smem_u32(&mbar[k]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+
+  // this thread's pixel (A row) and output channel (B row)
+  const int64_t pix = p0 + tid;
+  int n = 0, h = 0, w = 0;
+  const bool live = pix < total;
+  if (live) {
+    w = (int)(pix % W);
+    h = (int)((pix / W) % H);
+    n = (int)(pix / ((int64_t)W * H));
+  }
+  const uint32_t idesc = tc::instr_desc(128, Cout);
+  const int kchunks = Cin / 16;
+  const int nsteps = 9 * kchunks;
+  const int nstages = (nsteps + kTcStepsPerStage - 1) / kTcStepsPerStage;
+
+  // asynchronous copies of stage g into its buffer (zero fill outside the image)
+  auto load_stage = [&](int g) {
+    const int buf = g % kTcStages;
+    const int s0 = g * kTcStepsPerStage;
+    const int ns = min(kTcStepsPerStage, nsteps - s0);
+    for (int j = 0; j < ns; ++j) {
+      const int s = s0 + j;
+      const int t = s / kchunks, ci0 = (s % kchunks) * 16;
+      const int hs = h + t / 3 - 1, ws = w + t % 3 - 1;
+      const bool in = live && hs >= 0 && hs < H && ws >= 0 && ws < W;
+      const __nv_bfloat16* src = in ? X + (((size_t)n * H + hs) * W + ws) * xstride + xcoff + ci0 : X;
+      const uint32_t a = a_base + buf * kTcStageBytes + j * 4096;
+      cp_async16(a + tc::core_off(tid, 0), src, in ? 16 : 0);
+      cp_async16(a + tc::core_off(tid, 1), src + 8, in ? 16 : 0);
+      if (tid < Cout) {
+        const __nv_bfloat16* wsrc = Wt + ((size_t)t * Cout + tid) * Cin + ci0;
+        const uint32_t b = b_base + buf * kTcStageBytes + j * 4096;
+        cp_async16(b + tc::core_off(tid, 0), wsrc, 16);
+        cp_async16(b + tc::core_off(tid, 1), wsrc + 8, 16);
       }
-      // stage B: output channel co0 + tid / 2, the same 8 input channels
-      {
-        const int j = tid >> 1, half = tid & 1;
-        const int co = co0 + j;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (co < Cout) v = *reinterpret_cast<const uint4*>(Wt + ((size_t)t * Cout + co) * Cin + ci0 + 8 * half);
-        *reinterpret_cast<uint4*>(&Bs[j][8 * half]) = v;
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  bool ok = true;
+  load_stage(0);
+  if (nstages > 1) load_stage(1);
+  for (int g = 0; g < nstages; ++g) {
+    const int buf = g % kTcStages;
+    // this stage's copies are done (the next stage's may still be in flight)
+    if (g + 1 < nstages) asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0 && ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int s0 = g * kTcStepsPerStage;
+      const int ns = min(kTcStepsPerStage, nsteps - s0);
+      for (int j = 0; j < ns; ++j) {
+        const uint64_t ad = tc::smem_desc(a_base + buf * kTcStageBytes + j * 4096, 128, 256);
+        const uint64_t bd = tc::smem_desc(b_base + buf * kTcStageBytes + j * 4096, 128, 256);
+        tc::mma_f16(tmem, ad, bd, idesc, (s0 + j) > 0 ? 1u : 0u);
       }
-      __syncthreads();
-      uint32_t a[4];
-      const int r0 = warp * 16 + g;
-      a[0] = ld_smem_u32(&As[r0][2 * tq]);
-      a[1] = ld_smem_u32(&As[r0 + 8][2 * tq]);
-      a[2] = ld_smem_u32(&As[r0][2 * tq + 8]);
-      a[3] = ld_smem_u32(&As[r0 + 8][2 * tq + 8]);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        uint32_t b[2];
-        b[0] = ld_smem_u32(&Bs[j * 8 + g][2 * tq]);
-        b[1] = ld_smem_u32(&Bs[j * 8 + g][2 * tq + 8]);
-        mma_bf16(acc[j], a, b);
-      }
-      __syncthreads();
+      tc::commit(tc::smem_u32(&mbar[buf]));
+    }
+    // stage g + 2 reuses the buffer of stage g - 1: wait for its MMAs first
+    if (g + 2 < nstages) {
+      if (g >= 1 && ok) ok = tc::mbar_wait(tc::smem_u32(&mbar[(g - 1) % kTcStages]), ((g - 1) / kTcStages) & 1);
+      load_stage(g + 2);
     }
   }
-  // epilogue: rows (pixels) warp * 16 + g (+ 8), columns (channels) j * 8 + 2 * tq (+ 1)
+  // the last stage's MMAs (its commit covers every earlier one)
+  if (ok && nstages > 0)
+    ok = tc::mbar_wait(tc::smem_u32(&mbar[(nstages - 1) % kTcStages]), ((nstages - 1) / kTcStages) & 1);
+  if (!ok && err) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // epilogue: 16 columns at a time from this warp's 32 TMEM lanes
+  if (ok) {
+    for (int c0 = 0; c0 < Cout; c0 += 16) {
+      uint32_t v[16];
+      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (live) {
+        const size_t o = (size_t)pix * ystride + ycoff + c0;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int w = w0 + warp * 16 + g + 8 * half;
-      if (w >= W) continue;
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int co = co0 + j * 8 + 2 * tq + e;
-        if (co >= Cout) continue;
-        float v = acc[j][2 * half + e] + (bias ? bias[co] : 0.f);
-        if (relu) v = fmaxf(v, 0.f);
-        const size_t o = (((size_t)n * H + h) * W + w) * ystride + ycoff + co;
-        if (out_f32) reinterpret_cast<float*>(Yv)[o] = v;
-        else reinterpret_cast<__nv_bfloat16*>(Yv)[o] = __float2bfloat16_rn(v);
+        for (int e = 0; e < 16; ++e) {
+          float x = __uint_as_float(v[e]) + (bias ? bias[c0 + e] : 0.f);
+          if (relu) x = fmaxf(x, 0.f);
+          if (out_f32) reinterpret_cast<float*>(Yv)[o + e] = x;
+          else reinterpret_cast<__nv_bfloat16*>(Yv)[o + e] = __float2bfloat16_rn(x);
+        }
       }
     }
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
 // dW[t][co][ci] += sum_px dY[px, co] * X[px + (dy, dx), ci] over a chunk of

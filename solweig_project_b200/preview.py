@@ -1,7 +1,9 @@
 """Learned SVF preview for edits.
 
 A small U-Net (5 levels, ~340k parameters, BF16 weights and activations,
-FP32 accumulation on the tensor cores) maps a window of the march rasters
+FP32 accumulation on the 5th-generation tensor cores: tcgen05.mma with
+TMEM accumulators for the convolutions' forward and data-gradient passes)
+maps a window of the march rasters
 (building DSM, canopy top, trunk zone as heights above ground) to the 15
 SVF components.  It runs entirely on the library's own kernels
 (``sw100_nn_*``: implicit-GEMM 3 x 3 convolutions forward / data-gradient /
@@ -88,6 +90,7 @@ class UNet:
         self.m = torch.zeros_like(self.master)
         self.v = torch.zeros_like(self.master)
         self.step = 0
+        self.err = torch.zeros(1, dtype=torch.int32, device=d)   # set by a tensor-core kernel whose wait expired
         self.wf = {n: torch.empty(9 * co * ci, dtype=BF16, device=d) for n, ci, co, _ in UNET}
         self.wd = {n: torch.empty(9 * co * ci, dtype=BF16, device=d) for n, ci, co, _ in UNET}
         self._bufs = {}
@@ -144,15 +147,15 @@ class UNet:
         n = x.buf.shape[0]
         h, w = x.hw
         _, b = self._slices(self.master, name)
-        N.call("sw100_nn_conv3x3", _p(x.buf), n, h, w, cin, x.stride, x.coff, _p(self.wf[name]), _p(b), cout,
-               _p(y.buf), y.stride, y.coff, int(relu), int(out_f32), E._stream())
+        N.call("sw100_nn_conv3x3_tc", _p(x.buf), n, h, w, cin, x.stride, x.coff, _p(self.wf[name]), _p(b), cout,
+               _p(y.buf), y.stride, y.coff, int(relu), int(out_f32), _p(self.err), E._stream())
 
     def _dgrad(self, name, dy: Act, dx: Act):
         cin, cout, _ = self.layers[name]
         n = dy.buf.shape[0]
         h, w = dy.hw
-        N.call("sw100_nn_conv3x3", _p(dy.buf), n, h, w, cout, dy.stride, dy.coff, _p(self.wd[name]), None, cin,
-               _p(dx.buf), dx.stride, dx.coff, 0, 0, E._stream())
+        N.call("sw100_nn_conv3x3_tc", _p(dy.buf), n, h, w, cout, dy.stride, dy.coff, _p(self.wd[name]), None, cin,
+               _p(dx.buf), dx.stride, dx.coff, 0, 0, _p(self.err), E._stream())
 
     def _wgrad(self, name, x: Act, dy: Act):
         cin, cout, _ = self.layers[name]

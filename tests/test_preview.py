@@ -69,19 +69,11 @@ def test_conv_kernels_match_the_checker(cuda):
     p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)  # noqa: E731
     N.call("sw100_nn_weights", p(wm), cin, cout, p(wf), p(wd), E._stream())
     wq = _np(wf).reshape(9, cout, cin)                       # the bf16 weights the kernel uses
-    y = torch.zeros((n, h, w, cout), dtype=torch.float32, device="cuda")
-    N.call("sw100_nn_conv3x3", p(x), n, h, w, cin, cin, 0, p(wf), p(bias), cout, p(y), cout, 0, 0, 1, E._stream())
-    want = onn.conv3x3(_np(x), wq, _np(bias))
-    assert _rel(_np(y), want) < 1e-5
-    # relu + bf16 output into a channel slice of a wider buffer
-    yb = torch.zeros((n, h, w, cout + 16), dtype=torch.bfloat16, device="cuda")
-    N.call("sw100_nn_conv3x3", p(x), n, h, w, cin, cin, 0, p(wf), p(bias), cout, p(yb), cout + 16, 16, 1, 0,
-           E._stream())
-    assert _rel(_np(yb)[..., 16:], np.maximum(want, 0)) < 1e-2 and not _np(yb)[..., :16].any()
     # data gradient: a forward conv with the flipped layout
     dy = _bf(rng.standard_normal((n, h, w, cout))).cuda()
     dx = torch.zeros((n, h, w, cin), dtype=torch.bfloat16, device="cuda")
-    N.call("sw100_nn_conv3x3", p(dy), n, h, w, cout, cout, 0, p(wd), None, cin, p(dx), cin, 0, 0, 0, E._stream())
+    N.call("sw100_nn_conv3x3_tc", p(dy), n, h, w, cout, cout, 0, p(wd), None, cin, p(dx), cin, 0, 0, 0, None,
+           E._stream())
     assert _rel(_np(dx), onn.conv3x3_dgrad(_np(dy), wq)) < 1e-2
     # weight and bias gradients
     dw = torch.zeros(9 * cout * cin, dtype=torch.float32, device="cuda")
@@ -152,3 +144,33 @@ def test_network_gradients_match_the_checker(cuda):
         e = _rel(dw.cpu().numpy().astype(np.float64).reshape(9, cout, cin), grads[name][0])
         assert e < 0.08, (name, e)
         assert _rel(db.cpu().numpy().astype(np.float64), grads[name][1]) < 0.08, name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cin,cout,n,h,w", [(16, 16, 2, 20, 71), (32, 48, 1, 17, 33), (128, 64, 2, 8, 8),
+                                            (48, 128, 1, 40, 40)])
+def test_tensor_core_conv_matches_the_checker(cuda, cin, cout, n, h, w):
+    import torch
+    from solweig_project_b200 import _native as N
+    from solweig_project_b200 import engine as E
+    p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)  # noqa: E731
+    rng = np.random.default_rng(cin * 7 + cout)
+    x = _bf(rng.standard_normal((n, h, w, cin))).cuda()
+    wm = torch.tensor(rng.standard_normal((9, cout, cin)).astype(np.float32) * 0.2, device="cuda")
+    bias = torch.tensor(rng.standard_normal(cout).astype(np.float32), device="cuda")
+    wf = torch.empty(9 * cout * cin, dtype=torch.bfloat16, device="cuda")
+    N.call("sw100_nn_weights", p(wm), cin, cout, p(wf), None, E._stream())
+    wq = _np(wf).reshape(9, cout, cin)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    y = torch.zeros((n, h, w, cout), dtype=torch.float32, device="cuda")
+    N.call("sw100_nn_conv3x3_tc", p(x), n, h, w, cin, cin, 0, p(wf), p(bias), cout, p(y), cout, 0, 0, 1, p(err),
+           E._stream())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert _rel(_np(y), onn.conv3x3(_np(x), wq, _np(bias))) < 1e-5
+    # relu + bf16 into a channel slice, as the network writes concatenations
+    yb = torch.zeros((n, h, w, cout + 16), dtype=torch.bfloat16, device="cuda")
+    N.call("sw100_nn_conv3x3_tc", p(x), n, h, w, cin, cin, 0, p(wf), p(bias), cout, p(yb), cout + 16, 16, 1, 0,
+           p(err), E._stream())
+    want = np.maximum(onn.conv3x3(_np(x), wq, _np(bias)), 0)
+    assert _rel(_np(yb)[..., 16:], want) < 1e-2 and not _np(yb)[..., :16].any()

@@ -182,7 +182,7 @@ int sw100_svf_window(const sw100_site_planes* site, int rows, int cols, const sw
  * sw100_svf_window.  No counterpart in the reference: it serves the
  * learned preview, which takes the box's own pixels from the exact march. */
 int sw100_svf_box(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
-                  const sw100_step* steps, const int32_t* corridor, const int32_t box[4], float* planes,
+                  const sw100_step* steps, int n_steps, const int32_t* corridor, const int32_t box[4], float* planes,
                   uint32_t* bits, void* workspace, int64_t workspace_bytes, void* stream);
 
 /* Bounding box of the cells whose march rasters (dsm, vegdsm, vegdsm2,
@@ -363,7 +363,7 @@ typedef struct {
   float* state;                 /* 6 * npix thermal state, carried across calls */
   float* outputs;               /* popcount(out_mask) * n_t * npix */
   uint32_t out_mask;
-  int32_t pad;
+  int32_t svf_steps;            /* entries of the step table `steps` */
 } sw100_batch_site;
 
 /* Tile list entry {site index, tile column, tile row, daytime row}: the

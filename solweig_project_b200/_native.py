@@ -164,8 +164,8 @@ def load(path: str = LIB_PATH):
         "sw100_svf_window": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp,
                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32), vp, vp, vp, C.c_int64, vp]),
         "sw100_diff_bbox_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
-        "sw100_svf_box": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, vp, C.POINTER(C.c_int32), vp, vp,
-                                    vp, C.c_int64, vp]),
+        "sw100_svf_box": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, C.POINTER(C.c_int32),
+                                    vp, vp, vp, C.c_int64, vp]),
         "sw100_batch_validate": (C.c_int, [vp, C.c_int]),
         "sw100_utci_steps": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_int64, vp, vp]),
         "sw100_nn_conv3x3_tc": (C.c_int, [vp] + [C.c_int] * 6 + [vp, vp, C.c_int, vp] + [C.c_int] * 4 + [vp, vp]),

@@ -46,7 +46,7 @@ class BatchSite(C.Structure):
         ("site", N.SitePlanes), ("rows", C.c_int32), ("cols", C.c_int32), ("plan", C.c_void_p),
         ("steps", C.c_void_p), ("series", N.Series), ("svf_planes", C.c_void_p), ("svf_bits", C.c_void_p),
         ("src4", C.c_void_p), ("bflags", C.c_void_p), ("gsrc", C.c_void_p), ("state", C.c_void_p),
-        ("outputs", C.c_void_p), ("out_mask", C.c_uint32), ("pad", C.c_int32),
+        ("outputs", C.c_void_p), ("out_mask", C.c_uint32), ("svf_steps", C.c_int32),
     ]
 
 
@@ -162,6 +162,7 @@ class SiteBatch:
             b.svf_planes, b.svf_bits = m.planes.data_ptr(), m.bits.data_ptr()
             b.src4, b.bflags, b.gsrc = m.src4.data_ptr(), m.bflags.data_ptr(), m.gsrc.data_ptr()
             b.state, b.outputs, b.out_mask = m.site.state.data_ptr(), m.outputs.data_ptr(), mask
+            b.svf_steps = m.n_steps
         N.call("sw100_batch_validate", C.cast(host, C.c_void_p), len(self.members))
         raw = np.frombuffer(bytes(host), np.uint8).copy()
         self.sites_dev = torch.from_numpy(raw).to(self.device)

@@ -22,12 +22,12 @@ namespace sw100 {
 __global__ void pack4_kernel(const float* a, const float* b, const float* c, const float* d, size_t n, float4* out);
 __global__ void svf_sweep_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                  const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
-                                 uint32_t* bits);
+                                 uint32_t* bits, int n_steps);
 __global__ void svf_window_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                   const sw100_step* steps, const int32_t* corridor, float vmax, int4 rect, int4 win,
-                                  float* out, uint32_t* bits);
+                                  float* out, uint32_t* bits, int n_steps);
 __global__ void svf_box_pairs_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
-                                     const sw100_step* steps, float vmax, int4 box, uint32_t* bits);
+                                     const sw100_step* steps, float vmax, int4 box, uint32_t* bits, int n_steps);
 __global__ void diff_bbox_kernel(const float4* a, const float4* b, int rows, int cols, int* box);
 __global__ void box_init_kernel(int* box);
 __global__ void pack_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
@@ -36,13 +36,13 @@ __global__ void svf_sweep_batch_kernel(const sw100_batch_site* sites, const sw10
 __global__ void sun_march_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void time_loop_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void svf_bush_flags_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
-                                      const sw100_step* steps, uint32_t* flags);
+                                      const sw100_step* steps, uint32_t* flags, int n_steps);
 __global__ void sun_march_kernel(const float4* src4, SitePlanes site, int rows, int cols,
                                  const sw100_sun_step* sun_steps, const sw100_time_step* tsteps,
                                  const sw100_step* table, float vmax, float4* gsrc, float* debug8);
 __global__ void time_loop_kernel(SitePlanes site, int rows, int cols, const sw100_time_step* tsteps, int n_t,
                                  const sw100_patch_step* patch_steps, int n_patches,
-                                 const sw100_gvf_azimuth* gvf_az, const float4* gsrc, float* state,
+                                 const sw100_gvf_azimuth* gvf_az, const float4* gsrc, int n_day, float* state,
                                  uint32_t out_mask, float* outputs);
 __global__ void pack_cubes_kernel(const float* sh, const float* veg, const float* vb, size_t npix, int n_patches,
                                   Single5 single, uint32_t* bits);
@@ -220,11 +220,11 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
   if (site->bush_any) {
     cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)n_steps * 4, st);
     if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
-    svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags);
+    svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags, n_steps);
     if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
   }
   svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                           site->vmax, out_planes, out_bits);
+                                           site->vmax, out_planes, out_bits, n_steps);
   return check_launch("svf_sweep_kernel");
 }
 
@@ -264,14 +264,15 @@ int sw100_svf_window(const sw100_site_planes* site, int rows, int cols, const sw
   dim3 grid((w3 - w2 + 1 + 31) / 32, (w1 - w0 + 1 + 3) / 4);
   svf_window_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, corridor, site->vmax,
                                             make_int4(rect[0], rect[1], rect[2], rect[3]),
-                                            make_int4(w0, w1, w2, w3), planes, bits);
+                                            make_int4(w0, w1, w2, w3), planes, bits, n_steps);
   return check_launch("svf_window_kernel");
 }
 
 int sw100_svf_box(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
-                  const sw100_step* steps, const int32_t* corridor, const int32_t box[4], float* planes,
+                  const sw100_step* steps, int n_steps, const int32_t* corridor, const int32_t box[4], float* planes,
                   uint32_t* bits, void* workspace, int64_t workspace_bytes, void* stream) {
   int rc;
+  if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
   if ((rc = check_grid(rows, cols))) return rc;
   if ((rc = validate_site_march(site))) return rc;
   if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(corridor, "corridor")) ||
@@ -289,13 +290,13 @@ int sw100_svf_box(const sw100_site_planes* site, int rows, int cols, const sw100
   const int4 b4 = make_int4(box[0], box[1], box[2], box[3]);
   const int64_t pairs = (int64_t)(box[1] - box[0] + 1) * (box[3] - box[2] + 1) * SW100_MAX_PATCHES;
   const int blocks = (int)std::min<int64_t>((pairs + 127) / 128, 148 * 32);
-  svf_box_pairs_kernel<<<blocks, 128, 0, st>>>(src4, rows, cols, plan, steps, site->vmax, b4, bits);
+  svf_box_pairs_kernel<<<blocks, 128, 0, st>>>(src4, rows, cols, plan, steps, site->vmax, b4, bits, n_steps);
   if ((rc = check_launch("svf_box_pairs_kernel"))) return rc;
   // re-accumulate from the new bits: a rectangle outside the grid, read by no march
   dim3 block(32, 4);
   dim3 grid((box[3] - box[2] + 1 + 31) / 32, (box[1] - box[0] + 1 + 3) / 4);
   svf_window_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, corridor, site->vmax,
-                                            make_int4(-4, -4, -4, -4), b4, planes, bits);
+                                            make_int4(-4, -4, -4, -4), b4, planes, bits, n_steps);
   return check_launch("svf_window_kernel");
 }
 
@@ -343,6 +344,7 @@ int sw100_batch_validate(const sw100_batch_site* host_sites, int n_sites) {
     for (int k = 0; k < 6; ++k)
       if (!ptrs[k]) return fail(SW100_E_ARG, "site %d: %s must not be NULL", i, names[k]);
     if (b.site.bush_any && !b.bflags) return fail(SW100_E_ARG, "site %d: bflags must not be NULL with bush", i);
+    if (b.svf_steps < 0) return fail(SW100_E_ARG, "site %d: svf_steps must be >= 0", i);
     if ((rc = validate_series(&b.series))) return fail(rc, "site %d: %s", i, g_last_error.c_str());
     if (b.series.n_day > 0 && !b.gsrc) return fail(SW100_E_ARG, "site %d: gsrc must not be NULL", i);
     if (b.out_mask & ~0x7Fu) return fail(SW100_E_ARG, "site %d: unknown output bits 0x%x", i, b.out_mask);
@@ -485,7 +487,8 @@ int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw1
   dim3 block(32, 4);
   dim3 grid((cols + 31) / 32, (rows + 3) / 4);
   time_loop_kernel<<<grid, block, 0, st>>>(make_site(*site), rows, cols, series->steps, series->n_t, series->patch,
-                                           series->n_patches, series->gvf, gsrc, state, out_mask, outputs);
+                                           series->n_patches, series->gvf, gsrc, series->n_day, state, out_mask,
+                                           outputs);
   return check_launch("time_loop_kernel");
 }
 
@@ -503,7 +506,7 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
   dim3 grid((cols + 31) / 32, (rows + 3) / 4);
   time_loop_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
-      reinterpret_cast<const float4*>(gsrc), state, out_mask, outputs);
+      reinterpret_cast<const float4*>(gsrc), series->n_day, state, out_mask, outputs);
   return check_launch("time_loop_kernel");
 }
 
@@ -580,11 +583,11 @@ extern "C" int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, 
   if (site->bush_any) {
     cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)n_steps * 4, st);
     if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
-    svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags);
+    svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags, n_steps);
     if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
   }
   svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                           site->vmax, out_planes, out_bits);
+                                           site->vmax, out_planes, out_bits, n_steps);
   return check_launch("svf_sweep_kernel");
 }
 

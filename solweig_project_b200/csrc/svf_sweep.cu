@@ -239,11 +239,35 @@ __device__ __forceinline__ void svf_finish(SvfAcc& A, const sw100_svf_plan& plan
   }
 }
 
-__device__ __forceinline__ void load_plan(const sw100_svf_plan* __restrict__ plan_g, sw100_svf_plan& plan) {
+// A patch's steps clamped into the step table of n_steps entries (a plan
+// built by the host library is always inside; a malformed plan from another
+// caller then reads no memory outside the table).
+__device__ __forceinline__ void clamp_patch(int off, int cnt, int n_steps, int& o, int& n) {
+  o = min(max(off, 0), n_steps);
+  n = min(max(cnt, 0), n_steps - o);
+}
+
+// Copies the plan into shared memory and clamps every index it holds
+// (patch count, ring and annulus counts, step ranges) to the arrays they
+// index.  Every thread of the block calls it; it ends with a barrier.
+__device__ __forceinline__ void load_plan(const sw100_svf_plan* __restrict__ plan_g, sw100_svf_plan& plan,
+                                          int n_steps) {
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
   const int* s = reinterpret_cast<const int*>(plan_g);
   int* d = reinterpret_cast<int*>(&plan);
   const int nw = sizeof(sw100_svf_plan) / 4;
-  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < nw; i += blockDim.x * blockDim.y) d[i] = s[i];
+  for (int i = tid; i < nw; i += nthr) d[i] = s[i];
+  __syncthreads();
+  if (tid == 0) plan.n_patches = min(max(plan.n_patches, 0), SW100_MAX_PATCHES);
+  for (int q = tid; q < SW100_MAX_PATCHES; q += nthr) {
+    int o, n;
+    clamp_patch(plan.step_offset[q], plan.step_count[q], n_steps, o, n);
+    plan.step_offset[q] = o;
+    plan.step_count[q] = n;
+    plan.ring[q] = min(max(plan.ring[q], 0), SW100_MAX_RINGS - 1);
+  }
+  for (int r = tid; r < SW100_MAX_RINGS; r += nthr) plan.ring_annuli[r] = min(max(plan.ring_annuli[r], 0), SW100_MAX_ANNULI);
+  __syncthreads();
 }
 
 // The 153 patch marches, the sums and the outputs of pixel (r, c).
@@ -281,10 +305,9 @@ __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4,
 __global__ void __launch_bounds__(128) svf_sweep_kernel(
     const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
     const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
-    float* __restrict__ out, uint32_t* __restrict__ bits) {
+    float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps) {
   __shared__ sw100_svf_plan plan;
-  load_plan(plan_g, plan);
-  __syncthreads();
+  load_plan(plan_g, plan, n_steps);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = blockIdx.y * blockDim.y + threadIdx.y;
   if (r >= rows || c >= cols) return;
@@ -307,8 +330,7 @@ __global__ void __launch_bounds__(128) svf_sweep_batch_kernel(const sw100_batch_
     const sw100_tile T = tiles[i];
     const sw100_batch_site& S = sites[T.site];
     __syncthreads();  // the previous tile is done with the shared plan
-    load_plan(S.plan, plan);
-    __syncthreads();
+    load_plan(S.plan, plan, S.svf_steps);
     int r, c;
     if (batch_pixel(S, T, r, c))
       svf_sweep_pixel(reinterpret_cast<const float4*>(S.src4), S.rows, S.cols, plan, S.steps,
@@ -343,9 +365,10 @@ __global__ void __launch_bounds__(128) svf_bush_flags_batch_kernel(const sw100_b
     const float4 self = src4[(size_t)r * S.cols + c];
     if (!(self.w > 0.f)) continue;
     const sw100_svf_plan* plan = S.plan;
-    const int np = plan->n_patches;
+    const int np = min(max(plan->n_patches, 0), SW100_MAX_PATCHES);
     for (int q = 0; q < np; ++q) {
-      const int off = plan->step_offset[q], n = plan->step_count[q];
+      int off, n;
+      clamp_patch(plan->step_offset[q], plan->step_count[q], S.svf_steps, off, n);
       for (int k = 0; k < n; ++k) {
         const sw100_step st = S.steps[off + k];
         const int sr = r + st.dx, sc = c + st.dy;
@@ -397,10 +420,9 @@ __device__ __forceinline__ bool svf_in_corridor(int tr, int tc, const sw100_step
 __global__ void __launch_bounds__(128) svf_window_kernel(
     const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
     const sw100_step* __restrict__ steps, const int32_t* __restrict__ corridor, float vmax, int4 rect, int4 win,
-    float* __restrict__ out, uint32_t* __restrict__ bits) {
+    float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps) {
   __shared__ sw100_svf_plan plan;
-  load_plan(plan_g, plan);
-  __syncthreads();
+  load_plan(plan_g, plan, n_steps);
   const int c = win.z + blockIdx.x * blockDim.x + threadIdx.x;
   const int r = win.x + blockIdx.y * blockDim.y + threadIdx.y;
   if (r > win.y || c > win.w) return;
@@ -456,9 +478,9 @@ __global__ void box_init_kernel(int* box) {
 // new bits in the sweep's order.  Rasters without bush only.
 __global__ void __launch_bounds__(128) svf_box_pairs_kernel(
     const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan,
-    const sw100_step* __restrict__ steps, float vmax, int4 box, uint32_t* __restrict__ bits) {
+    const sw100_step* __restrict__ steps, float vmax, int4 box, uint32_t* __restrict__ bits, int n_steps) {
   const int bw = box.w - box.z + 1, bh = box.y - box.x + 1;
-  const int np = plan->n_patches;
+  const int np = min(max(plan->n_patches, 0), SW100_MAX_PATCHES);
   const int64_t total = (int64_t)bw * bh * np;
   const size_t npix = (size_t)rows * cols;
   const bool finite = plan->all_finite != 0;
@@ -468,7 +490,8 @@ __global__ void __launch_bounds__(128) svf_box_pairs_kernel(
     const int r = box.x + (int)(px / bw), c = box.z + (int)(px % bw);
     const size_t p = (size_t)r * cols + c;
     const float4 self = src4[p];
-    const int off = plan->step_offset[q], n = plan->step_count[q];
+    int off, n;
+    clamp_patch(plan->step_offset[q], plan->step_count[q], n_steps, off, n);
     float sh, veg, vb;
     if (finite)
       march_patch_fast(src4, rows, cols, r, c, self.x, self.z, steps + off, n, vmax, sh, veg, vb);
@@ -516,16 +539,17 @@ __global__ void diff_bbox_kernel(const float4* __restrict__ a, const float4* __r
 // flag the steps at which any pixel with bush > 0 sees vegetation above it.
 __global__ void svf_bush_flags_kernel(const float4* __restrict__ src4, int rows, int cols,
                                       const sw100_svf_plan* __restrict__ plan, const sw100_step* __restrict__ steps,
-                                      uint32_t* __restrict__ flags) {
+                                      uint32_t* __restrict__ flags, int n_steps) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = blockIdx.y * blockDim.y + threadIdx.y;
   if (r >= rows || c >= cols) return;
   const float4 self = src4[(size_t)r * cols + c];
   if (!(self.w > 0.f)) return;
   const float a = self.x;
-  const int np = plan->n_patches;
+  const int np = min(max(plan->n_patches, 0), SW100_MAX_PATCHES);
   for (int q = 0; q < np; ++q) {
-    const int off = plan->step_offset[q], n = plan->step_count[q];
+    int off, n;
+    clamp_patch(plan->step_offset[q], plan->step_count[q], n_steps, off, n);
     for (int k = 0; k < n; ++k) {
       const sw100_step st = steps[off + k];
       const int sr = r + st.dx, sc = c + st.dy;

@@ -39,7 +39,7 @@ __host__ inline SitePlanes make_site(const sw100_site_planes& s) {
 template <class Site>
 __device__ __forceinline__ float ground_temperature(const Site& site, const sw100_time_step& P, size_t p) {
   const float tgamp = site.tgk[p] * P.altmax32 + site.tstart[p];
-  float tg = tgamp * P.tg_factor[site.class_idx[p]];
+  float tg = tgamp * P.tg_factor[min((int)site.class_idx[p], SW100_MAX_CLASSES - 1)];
   tg = tg * P.cig;
   if (P.landcover) tg = tmax(tg, 0.f);
   return tg;

@@ -197,8 +197,8 @@ template <class Site>
 __device__ __forceinline__ void time_loop_tile(
     const Site& site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
-    const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, float* __restrict__ state,
-    uint32_t out_mask, float* __restrict__ outputs, int bx, int by) {
+    const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
+    float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs, int bx, int by) {
   // PP is filled with 16-byte vector stores: the array must be 16-byte
   // aligned (the struct itself only requires 8)
   __shared__ __align__(16) sw100_time_step P;
@@ -280,7 +280,10 @@ __device__ __forceinline__ void time_loop_tile(
     float shadow = 0.f, Lup, LupE, LupS, LupW, LupN;
     float Kdown = 0.f, Kup = 0.f, KupE = 0.f, KupS = 0.f, KupW = 0.f, KupN = 0.f;
     float Kside = 0.f, ksideI = 0.f, albF_day = 0.f;
-    if (P.is_day) {
+    // a daytime step reads its row of sun-march records (a row outside the
+    // n_day rows written is treated as night: nothing outside is read)
+    const bool is_day = P.is_day != 0 && (unsigned)P.day_row < (unsigned)n_day;
+    if (is_day) {
       const float4* G = gsrc + (size_t)P.day_row * npix;
       const float4 own = G[p];
       shadow = own.x;
@@ -288,7 +291,7 @@ __device__ __forceinline__ void time_loop_tile(
       const float tg = ground_temperature(site, P, p);
       // ---------------- ground view factors (18 azimuths)
       GvfSums S = {};
-      const int second_i = (int)P.second;
+      const int second_i = min((int)P.second, SW100_MAX_GVF_STEPS);  // walk tables hold 64 steps
       const float second = P.second;
       StepDiv D;
       D.first = P.first;
@@ -384,7 +387,7 @@ __device__ __forceinline__ void time_loop_tile(
     float ksideD = 0.f, kref_sun = 0.f, kref_sh = 0.f, kref_veg = 0.f, anilum = 0.f;
     float ld_sky = 0.f, ld_veg = 0.f, ld_sh = 0.f, ld_sun = 0.f, ld_ref = 0.f;
     float ls_sky = 0.f, ls_veg = 0.f, ls_sh = 0.f, ls_sun = 0.f, ls_ref = 0.f;
-    const bool day = P.is_day != 0;
+    const bool day = is_day;
     // dense: sky-visible longwave (sh == 1 & vegsh == 1); by day the diffuse
     // Kside term and the anisotropic luminance, indexed by (sh, vegsh)
 #pragma unroll
@@ -513,9 +516,9 @@ __device__ __forceinline__ void time_loop_tile(
 __global__ void __launch_bounds__(128, 5) time_loop_kernel(
     SitePlanes site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
-    const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, float* __restrict__ state,
-    uint32_t out_mask, float* __restrict__ outputs) {
-  time_loop_tile(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, state, out_mask, outputs,
+    const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
+    float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs) {
+  time_loop_tile(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day, state, out_mask, outputs,
                  blockIdx.x, blockIdx.y);
 }
 
@@ -527,7 +530,8 @@ __global__ void __launch_bounds__(128, 5) time_loop_batch_kernel(const sw100_bat
     const sw100_batch_site& S = sites[T.site];
     __syncthreads();  // the previous tile is done with the shared tables
     time_loop_tile(S.site, S.rows, S.cols, S.series.steps, S.series.n_t, S.series.patch, S.series.n_patches,
-                   S.series.gvf, reinterpret_cast<const float4*>(S.gsrc), S.state, S.out_mask, S.outputs, T.tx,
+                   S.series.gvf, reinterpret_cast<const float4*>(S.gsrc), S.series.n_day, S.state, S.out_mask,
+                   S.outputs, T.tx,
                    T.ty);
   }
 }

@@ -292,7 +292,7 @@ class DeviceSite:
         """Exact SVF planes and bits of the box's own pixels after an edit
         of the rasters inside it, one thread per (pixel, patch) march
         (sw100_svf_box); pixels outside keep what they hold."""
-        plan_d, steps_d, _, _, _ = self.svf_tables(patch_option)
+        plan_d, steps_d, n_steps, _, _ = self.svf_tables(patch_option)
         _, desc_d, _ = self._corridor(patch_option)
         key = ("window_ws",)
         if key not in self._cache:
@@ -302,7 +302,7 @@ class DeviceSite:
         r = self.svf_result
         site = self.site_struct()
         box = (r0, r0 + h - 1, c0, c0 + w - 1)
-        N.call("sw100_svf_box", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), _ptr(desc_d),
+        N.call("sw100_svf_box", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), n_steps, _ptr(desc_d),
                (C.c_int32 * 4)(*box), _ptr(r.planes), _ptr(r.bits), _ptr(wws), wws.numel(), _stream())
         return {"mode": "box", "rect": box, "window": box, "pixels": h * w}
 

@@ -22,7 +22,8 @@ namespace sw100 {
 __global__ void pack4_kernel(const float* a, const float* b, const float* c, const float* d, size_t n, float4* out);
 __global__ void svf_sweep_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                  const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
-                                 uint32_t* bits, int n_steps);
+                                 uint32_t* bits, int n_steps, const float* skipmap);
+__global__ void svf_skipmap_kernel(const float4* src4, int rows, int cols, float* m, int crow, int ccol);
 __global__ void svf_window_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                   const sw100_step* steps, const int32_t* corridor, float vmax, int4 rect, int4 win,
                                   float* out, uint32_t* bits, int n_steps);
@@ -195,7 +196,8 @@ int sw100_svf_workspace_bytes(int rows, int cols, int n_steps, int64_t* bytes) {
   if ((rc = check_grid(rows, cols))) return rc;
   if ((rc = check_ptr(bytes, "bytes"))) return rc;
   if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
-  *bytes = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4);
+  *bytes = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4) +
+           align_up((int64_t)((rows + 7) / 8) * ((cols + 7) / 8) * 4);
   return 0;
 }
 
@@ -223,8 +225,13 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
     svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags, n_steps);
     if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
   }
+  // skip map after the bush flags
+  const int crow = (rows + 7) / 8, ccol = (cols + 7) / 8;
+  float* skipmap = reinterpret_cast<float*>(reinterpret_cast<char*>(flags) + align_up((int64_t)n_steps * 4));
+  svf_skipmap_kernel<<<(crow * ccol + 127) / 128, 128, 0, st>>>(src4, rows, cols, skipmap, crow, ccol);
+  if ((rc = check_launch("svf_skipmap_kernel"))) return rc;
   svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                           site->vmax, out_planes, out_bits, n_steps);
+                                           site->vmax, out_planes, out_bits, n_steps, skipmap);
   return check_launch("svf_sweep_kernel");
 }
 
@@ -565,8 +572,9 @@ extern "C" int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, 
   if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(out_planes, "out_planes")) ||
       (rc = check_ptr(out_bits, "out_bits")))
     return rc;
-  int64_t need = 0;
-  if ((rc = sw100_svf_workspace_bytes(rows, cols, n_steps, &need))) return rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
+  const int64_t need = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4);
   if (need > (int64_t)SW100_SVF_NOALLOC_SCRATCH_BYTES)
     return fail(SW100_E_SIZE,
                 "grid %d x %d with %d steps needs %lld scratch bytes; the allocation-free sweep has %lld "
@@ -587,7 +595,7 @@ extern "C" int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, 
     if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
   }
   svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                           site->vmax, out_planes, out_bits, n_steps);
+                                           site->vmax, out_planes, out_bits, n_steps, nullptr);
   return check_launch("svf_sweep_kernel");
 }
 

@@ -110,9 +110,22 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
 // then zeroes the vegetation state for good, so the march ends there.
 // vegsh and the "vbshvegsh ever counted" flag are booleans.  Returns final
 // (sh, vegsh, vbshvegsh) with values as march_patch.
+// Coarse bound on the march sources for skipping steps: m[b] is the largest
+// of dsm, vegdsm and vegdsm2 over the 8 x 8 cell block b and its eight
+// neighbours (crow x ccol blocks).  A march step moves at most one cell per
+// axis, so from a cell of block b the next 8 steps stay inside that 3 x 3
+// neighbourhood; when m - dz <= a at the first of them (dz grows along a
+// patch with positive altitude), none of the 8 can shade the pixel or add
+// vegetation.  m == nullptr: no skipping.
+struct SkipMap {
+  const float* m;
+  int ccol;
+};
+
 __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4, int rows, int cols, int r, int c,
                                                  float a, float veg2_p, const sw100_step* __restrict__ steps, int n,
-                                                 float vmax, float& sh_out, float& veg_out, float& vb_out) {
+                                                 float vmax, float& sh_out, float& veg_out, float& vb_out,
+                                                 SkipMap skip = SkipMap{nullptr, 0}) {
   bool sh = false, vegsh = false, vb_any = false;
   if (n > 0) {
     // first step (index 1 of shadow.py): the trunk-zone rule of :288-293
@@ -134,6 +147,7 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
     if (sh) {
       if (n > 1) vegsh = false;  // the next step zeroes it under building shadow
     } else {
+      const bool can_skip = skip.m != nullptr && a >= 0.f;
       for (int k = 1; k < n; ++k) {
         const sw100_step sk = load_step(&steps[k]);
         const int rr = r + sk.dx, cc = c + sk.dy;
@@ -142,6 +156,11 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
           if (0.f > a) { sh = true; vegsh = false; }
           else vb_any = vb_any || vegsh;
           break;
+        }
+        if (can_skip && sk.dz >= 0.f && __fsub_rn(__ldg(&skip.m[(rr >> 3) * skip.ccol + (cc >> 3)]), sk.dz) <= a) {
+          vb_any = vb_any || vegsh;  // all each of the 8 skipped steps would do
+          k += 7;
+          continue;
         }
         const float4 v = __ldg(&src4[(size_t)rr * cols + cc]);
         if (__fsub_rn(v.x, sk.dz) > a) { sh = true; vegsh = false; break; }
@@ -274,7 +293,8 @@ __device__ __forceinline__ void load_plan(const sw100_svf_plan* __restrict__ pla
 __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4, int rows, int cols,
                                                 const sw100_svf_plan& plan, const sw100_step* __restrict__ steps,
                                                 const uint32_t* __restrict__ bflags, float vmax,
-                                                float* __restrict__ out, uint32_t* __restrict__ bits, int r, int c) {
+                                                float* __restrict__ out, uint32_t* __restrict__ bits, int r, int c,
+                                                SkipMap skip = SkipMap{nullptr, 0}) {
   const size_t npix = (size_t)rows * cols;
   const size_t p = (size_t)r * cols + c;
   const float4 self = src4[p];
@@ -292,7 +312,7 @@ __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4,
     const int n = plan.step_count[q];
     float sh, veg, vb;
     if (fast)
-      march_patch_fast(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb);
+      march_patch_fast(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip);
     else
       march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, n,
                   bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);
@@ -302,16 +322,34 @@ __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4,
   svf_finish(A, plan, veg2_p, p, npix, wsh, wveg, wvb, out, bits);
 }
 
+// The skip map of a site: for each 8 x 8 block, the largest source height
+// (dsm, vegdsm, vegdsm2) over the block and its neighbours.
+__global__ void svf_skipmap_kernel(const float4* __restrict__ src4, int rows, int cols, float* __restrict__ m,
+                                   int crow, int ccol) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= crow * ccol) return;
+  const int br = b / ccol, bc = b % ccol;
+  const int r0 = max(0, (br - 1) * 8), r1 = min(rows, (br + 2) * 8);
+  const int c0 = max(0, (bc - 1) * 8), c1 = min(cols, (bc + 2) * 8);
+  float v = -INFINITY;
+  for (int r = r0; r < r1; ++r)
+    for (int c = c0; c < c1; ++c) {
+      const float4 s = src4[(size_t)r * cols + c];
+      v = fmaxf(v, fmaxf(s.x, fmaxf(s.y, s.z)));
+    }
+  m[b] = v;
+}
+
 __global__ void __launch_bounds__(128) svf_sweep_kernel(
     const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
     const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
-    float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps) {
+    float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps, const float* __restrict__ skipmap) {
   __shared__ sw100_svf_plan plan;
   load_plan(plan_g, plan, n_steps);
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = blockIdx.y * blockDim.y + threadIdx.y;
   if (r >= rows || c >= cols) return;
-  svf_sweep_pixel(src4, rows, cols, plan, steps, bflags, vmax, out, bits, r, c);
+  svf_sweep_pixel(src4, rows, cols, plan, steps, bflags, vmax, out, bits, r, c, SkipMap{skipmap, (cols + 7) / 8});
 }
 
 // ------------------------------------------------------------- batches

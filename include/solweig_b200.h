@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define SW100_ABI_VERSION 1
+#define SW100_ABI_VERSION 2
 
 #define SW100_MAX_PATCHES 160   /* patch option 2 uses 153 */
 #define SW100_MAX_RINGS 16
@@ -65,12 +65,18 @@ extern "C" {
 
 /* One executed step of a march: source offset (dx rows, dy cols) and the
  * float32 height drop dz, built on the host with the reference's float32
- * trigonometry so that the executed sequence is bit-identical. */
+ * trigonometry so that the executed sequence is bit-identical.  flags bit 0
+ * (SW100_STEP_SKIP8) is the host's proof that steps k .. k+7 of the same march
+ * (those that exist) each move at most one cell per axis from the step
+ * before and that dz does not decrease from step k-1 through k+7: the
+ * kernels then may test those 8 steps at once against a coarse height bound
+ * (an exact shortcut).  0 is always valid. */
+#define SW100_STEP_SKIP8 1
 typedef struct {
   int32_t dx;
   int32_t dy;
   float dz;
-  int32_t pad;
+  int32_t flags;
 } sw100_step;
 
 /* ------------------------------------------------------- site planes -- */
@@ -364,6 +370,9 @@ typedef struct {
   float* outputs;               /* popcount(out_mask) * n_t * npix */
   uint32_t out_mask;
   int32_t svf_steps;            /* entries of the step table `steps` */
+  float* skipmap;               /* ((rows + 7) / 8) * ((cols + 7) / 8) source bounds of the SVF
+                                   sweep, written by sw100_batch_skipmap after the pack; NULL:
+                                   march every step */
 } sw100_batch_site;
 
 /* Tile list entry {site index, tile column, tile row, daytime row}: the
@@ -387,6 +396,10 @@ int sw100_batch_pack(const sw100_batch_site* sites, const sw100_tile* tiles, int
                      int block_y, int grid, void* stream);
 int sw100_batch_bush_flags(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
                            int block_y, int grid, void* stream);
+/* Source-height bounds of 8 x 8 cell blocks (the step shortcut of the SVF
+ * sweep) for every site of `sites` (device array of n_sites) whose skipmap
+ * is not NULL; runs after the pack. */
+int sw100_batch_skipmap(const sw100_batch_site* sites, int n_sites, void* stream);
 int sw100_batch_svf(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x, int block_y,
                     int grid, void* stream);
 int sw100_batch_sun_march(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,

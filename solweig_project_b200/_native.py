@@ -31,14 +31,15 @@ OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDO
             "ldown": OUT_LDOWN, "shadow": OUT_SHADOW}
 
 # Exported symbols (checked by the CPU tests against include/solweig_b200.h)
-SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noalloc", "sw100_pack_cubes", "sw100_sun_march_workspace_bytes",
-           "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop", "sw100_flux_loop", "sw100_utci",
-           "sw100_abi_version", "sw100_last_error", "sw100_launch_count", "sw100_svf_window_workspace_bytes",
-           "sw100_svf_window", "sw100_diff_bbox_workspace_bytes", "sw100_diff_bbox", "sw100_batch_validate",
-           "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
-           "sw100_batch_flux_loop", "sw100_utci_steps", "sw100_nn_conv3x3_wgrad",
-           "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2", "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam",
-           "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc")
+SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noalloc", "sw100_pack_cubes",
+           "sw100_sun_march_workspace_bytes", "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop",
+           "sw100_flux_loop", "sw100_utci", "sw100_abi_version", "sw100_last_error", "sw100_launch_count",
+           "sw100_svf_window_workspace_bytes", "sw100_svf_window", "sw100_diff_bbox_workspace_bytes",
+           "sw100_diff_bbox", "sw100_batch_validate", "sw100_batch_pack", "sw100_batch_bush_flags",
+           "sw100_batch_skipmap", "sw100_batch_svf", "sw100_batch_sun_march", "sw100_batch_flux_loop",
+           "sw100_utci_steps", "sw100_nn_conv3x3_wgrad", "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2",
+           "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc")
+ABI_VERSION = 2  # SW100_ABI_VERSION of include/solweig_b200.h
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
 
@@ -57,7 +58,8 @@ class NativeError(RuntimeError):
 
 
 # ----------------------------------------------------------- numpy tables
-STEP_DTYPE = np.dtype([("dx", "<i4"), ("dy", "<i4"), ("dz", "<f4"), ("pad", "<i4")], align=True)
+STEP_DTYPE = np.dtype([("dx", "<i4"), ("dy", "<i4"), ("dz", "<f4"), ("flags", "<i4")], align=True)
+STEP_SKIP8 = 1
 
 SVF_PLAN_DTYPE = np.dtype([
     ("n_patches", "<i4"), ("n_rings", "<i4"), ("bush_any", "<i4"), ("all_finite", "<i4"),
@@ -181,6 +183,7 @@ def load(path: str = LIB_PATH):
         **{name: (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]) for name in (
             "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
             "sw100_batch_flux_loop")},
+        "sw100_batch_skipmap": (C.c_int, [vp, C.c_int, vp]),
         "sw100_diff_bbox": (C.c_int, [C.POINTER(SitePlanes), C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp,
                                       C.c_int64, vp]),
     }
@@ -188,8 +191,8 @@ def load(path: str = LIB_PATH):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.sw100_abi_version() != 1:
-        raise NativeUnavailable(f"{path} has ABI version {lib.sw100_abi_version()}, expected 1")
+    if lib.sw100_abi_version() != ABI_VERSION:
+        raise NativeUnavailable(f"{path} has ABI version {lib.sw100_abi_version()}, expected {ABI_VERSION}")
     _LIB = lib
     return lib
 

@@ -46,7 +46,7 @@ class BatchSite(C.Structure):
         ("site", N.SitePlanes), ("rows", C.c_int32), ("cols", C.c_int32), ("plan", C.c_void_p),
         ("steps", C.c_void_p), ("series", N.Series), ("svf_planes", C.c_void_p), ("svf_bits", C.c_void_p),
         ("src4", C.c_void_p), ("bflags", C.c_void_p), ("gsrc", C.c_void_p), ("state", C.c_void_p),
-        ("outputs", C.c_void_p), ("out_mask", C.c_uint32), ("svf_steps", C.c_int32),
+        ("outputs", C.c_void_p), ("out_mask", C.c_uint32), ("svf_steps", C.c_int32), ("skipmap", C.c_void_p),
     ]
 
 
@@ -113,6 +113,7 @@ class _Member:
     gsrc: torch.Tensor
     outputs: torch.Tensor
     n_steps: int
+    skipmap: torch.Tensor
 
 
 class SiteBatch:
@@ -149,7 +150,8 @@ class SiteBatch:
                 bflags=torch.zeros(max(1, n_steps), dtype=torch.int32, device=d),
                 gsrc=torch.empty((n_day, npix, 4), dtype=torch.float32, device=d),
                 outputs=torch.empty((len(self.names), s_struct.n_t, rows, cols), dtype=torch.float32, device=d),
-                n_steps=n_steps))
+                n_steps=n_steps,
+                skipmap=torch.empty(-(-rows // 8) * -(-cols // 8), dtype=torch.float32, device=d)))
             site._plan_steps = (plan_d, steps_d)
         self.mask = mask
         host = (BatchSite * len(self.members))()
@@ -163,6 +165,7 @@ class SiteBatch:
             b.src4, b.bflags, b.gsrc = m.src4.data_ptr(), m.bflags.data_ptr(), m.gsrc.data_ptr()
             b.state, b.outputs, b.out_mask = m.site.state.data_ptr(), m.outputs.data_ptr(), mask
             b.svf_steps = m.n_steps
+            b.skipmap = m.skipmap.data_ptr()
         N.call("sw100_batch_validate", C.cast(host, C.c_void_p), len(self.members))
         raw = np.frombuffer(bytes(host), np.uint8).copy()
         self.sites_dev = torch.from_numpy(raw).to(self.device)
@@ -219,6 +222,9 @@ class SiteBatch:
                 m.site.state.zero_()
         for st in STAGES:
             self.launch(st)
+            if st == "pack":
+                N.call("sw100_batch_skipmap", C.c_void_p(self.sites_dev.data_ptr()), len(self.members),
+                       E._stream())
 
     def capture(self):
         """Record :meth:`run` in a CUDA graph (tile lists and descriptors are

@@ -35,6 +35,7 @@ __global__ void pack_batch_kernel(const sw100_batch_site* sites, const sw100_til
 __global__ void svf_bush_flags_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void svf_sweep_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void sun_march_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
+__global__ void skipmap_batch_kernel(const sw100_batch_site* sites);
 __global__ void time_loop_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void svf_bush_flags_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
                                       const sw100_step* steps, uint32_t* flags, int n_steps);
@@ -171,6 +172,15 @@ int validate_series(const sw100_series* s) {
   return 0;
 }
 
+// Bytes of a site's skip map (one float per 8 x 8 cell block), aligned.
+int64_t skipmap_bytes(int rows, int cols) { return align_up((int64_t)((rows + 7) / 8) * ((cols + 7) / 8) * 4); }
+
+int launch_skipmap(const float4* src4, int rows, int cols, float* skipmap, cudaStream_t st) {
+  const int crow = (rows + 7) / 8, ccol = (cols + 7) / 8;
+  svf_skipmap_kernel<<<(crow * ccol + 127) / 128, 128, 0, st>>>(src4, rows, cols, skipmap, crow, ccol);
+  return check_launch("svf_skipmap_kernel");
+}
+
 int launch_sun_march(const sw100_site_planes& site, int rows, int cols, const sw100_series& ser, const float4* src4,
                      float4* gsrc, float* debug8, cudaStream_t st) {
   if (ser.n_day == 0) return 0;
@@ -196,8 +206,7 @@ int sw100_svf_workspace_bytes(int rows, int cols, int n_steps, int64_t* bytes) {
   if ((rc = check_grid(rows, cols))) return rc;
   if ((rc = check_ptr(bytes, "bytes"))) return rc;
   if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
-  *bytes = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4) +
-           align_up((int64_t)((rows + 7) / 8) * ((cols + 7) / 8) * 4);
+  *bytes = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4) + skipmap_bytes(rows, cols);
   return 0;
 }
 
@@ -226,10 +235,8 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
     if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
   }
   // skip map after the bush flags
-  const int crow = (rows + 7) / 8, ccol = (cols + 7) / 8;
   float* skipmap = reinterpret_cast<float*>(reinterpret_cast<char*>(flags) + align_up((int64_t)n_steps * 4));
-  svf_skipmap_kernel<<<(crow * ccol + 127) / 128, 128, 0, st>>>(src4, rows, cols, skipmap, crow, ccol);
-  if ((rc = check_launch("svf_skipmap_kernel"))) return rc;
+  if ((rc = launch_skipmap(src4, rows, cols, skipmap, st))) return rc;
   svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
                                            site->vmax, out_planes, out_bits, n_steps, skipmap);
   return check_launch("svf_sweep_kernel");
@@ -400,6 +407,15 @@ int sw100_batch_bush_flags(const sw100_batch_site* sites, const sw100_tile* tile
                            int block_y, int grid, void* stream) {
   return launch_batch(svf_bush_flags_batch_kernel, "svf_bush_flags_batch_kernel", sites, tiles, n_tiles, block_x,
                       block_y, grid, stream);
+}
+
+int sw100_batch_skipmap(const sw100_batch_site* sites, int n_sites, void* stream) {
+  int rc;
+  if (n_sites < 0 || n_sites > 65535) return fail(SW100_E_ARG, "n_sites must be in [0, 65535]");
+  if (n_sites == 0) return 0;
+  if ((rc = check_ptr(sites, "sites"))) return rc;
+  skipmap_batch_kernel<<<dim3(64, n_sites), 128, 0, static_cast<cudaStream_t>(stream)>>>(sites);
+  return check_launch("skipmap_batch_kernel");
 }
 
 int sw100_batch_svf(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x, int block_y,

@@ -28,6 +28,13 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
   float shvoveg = vegdem_p;
   float dzprev = 0.f;
   const float wallbol = walls_p > 0.f ? 1.f : 0.f;
+  // Building shadow settles a pixel that is not a wall (walls exactly +0)
+  // on finite rasters (vmax finite: no NaN or +inf source): from then on sh
+  // stays 1, vegsh ends every step at 0 and vbsh gains nothing; f and
+  // shvoveg only reach the outputs through the wall tail, where with walls
+  // +0 they decide nothing but the sign of the zero (shvoveg - a) * 0,
+  // which stays +0 once shvoveg - a is +0 or positive.
+  const bool shade_exit = __float_as_uint(walls_p) == 0u && isfinite(vmax);
   for (int k = 0; k < n; ++k) {
     const sw100_step st = load_step(&steps[k]);
     const int sr = r + st.dx, sc = c + st.dy;
@@ -56,9 +63,10 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
     // grid (it stays out and reads zeros), or every later source height
     // minus a larger drop stays at or below the pixel, its running building
     // maximum and its running vegetation maximum.  Zeros are covered by
-    // a >= 0 and shvoveg >= 0.
+    // nonneg(a) and nonneg(shvoveg).
     const float top = __fsub_rn(vmax, dz);
-    if (a >= 0.f && shvoveg >= 0.f && (!inb || (top <= a && top <= shvoveg))) break;
+    if (nonneg(a) && nonneg(shvoveg) && (!inb || (top <= a && top <= shvoveg))) break;
+    if (shade_exit && f > a && nonneg(__fsub_rn(shvoveg, a))) break;
   }
   MarchOut o;
   float facesh;

@@ -110,18 +110,9 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
 // then zeroes the vegetation state for good, so the march ends there.
 // vegsh and the "vbshvegsh ever counted" flag are booleans.  Returns final
 // (sh, vegsh, vbshvegsh) with values as march_patch.
-// Coarse bound on the march sources for skipping steps: m[b] is the largest
-// of dsm, vegdsm and vegdsm2 over the 8 x 8 cell block b and its eight
-// neighbours (crow x ccol blocks).  A march step moves at most one cell per
-// axis, so from a cell of block b the next 8 steps stay inside that 3 x 3
-// neighbourhood; when m - dz <= a at the first of them (dz grows along a
-// patch with positive altitude), none of the 8 can shade the pixel or add
-// vegetation.  m == nullptr: no skipping.
-struct SkipMap {
-  const float* m;
-  int ccol;
-};
-
+// Steps flagged SW100_STEP_SKIP8 whose 8-step source bound minus the step's
+// drop is at or below the pixel cannot shade it or add vegetation: they are
+// passed over 8 at a time (SkipMap, sw_common.cuh).
 __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4, int rows, int cols, int r, int c,
                                                  float a, float veg2_p, const sw100_step* __restrict__ steps, int n,
                                                  float vmax, float& sh_out, float& veg_out, float& vb_out,
@@ -157,7 +148,8 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
           else vb_any = vb_any || vegsh;
           break;
         }
-        if (can_skip && sk.dz >= 0.f && __fsub_rn(__ldg(&skip.m[(rr >> 3) * skip.ccol + (cc >> 3)]), sk.dz) <= a) {
+        if (can_skip && (sk.flags & SW100_STEP_SKIP8) && sk.dz >= 0.f &&
+            __fsub_rn(skip_bound(skip, rr, cc), sk.dz) <= a) {
           vb_any = vb_any || vegsh;  // all each of the 8 skipped steps would do
           k += 7;
           continue;
@@ -323,11 +315,10 @@ __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4,
 }
 
 // The skip map of a site: for each 8 x 8 block, the largest source height
-// (dsm, vegdsm, vegdsm2) over the block and its neighbours.
-__global__ void svf_skipmap_kernel(const float4* __restrict__ src4, int rows, int cols, float* __restrict__ m,
-                                   int crow, int ccol) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= crow * ccol) return;
+// (dsm, vegdsm, vegdsm2) over the block and its neighbours; NaN propagates
+// (a NaN bound never passes the skip test).
+__device__ __forceinline__ void skipmap_block(const float4* __restrict__ src4, int rows, int cols,
+                                              float* __restrict__ m, int ccol, int b) {
   const int br = b / ccol, bc = b % ccol;
   const int r0 = max(0, (br - 1) * 8), r1 = min(rows, (br + 2) * 8);
   const int c0 = max(0, (bc - 1) * 8), c1 = min(cols, (bc + 2) * 8);
@@ -335,9 +326,16 @@ __global__ void svf_skipmap_kernel(const float4* __restrict__ src4, int rows, in
   for (int r = r0; r < r1; ++r)
     for (int c = c0; c < c1; ++c) {
       const float4 s = src4[(size_t)r * cols + c];
-      v = fmaxf(v, fmaxf(s.x, fmaxf(s.y, s.z)));
+      v = tmax(v, tmax(s.x, tmax(s.y, s.z)));
     }
   m[b] = v;
+}
+
+__global__ void svf_skipmap_kernel(const float4* __restrict__ src4, int rows, int cols, float* __restrict__ m,
+                                   int crow, int ccol) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= crow * ccol) return;
+  skipmap_block(src4, rows, cols, m, ccol, b);
 }
 
 __global__ void __launch_bounds__(128) svf_sweep_kernel(
@@ -372,8 +370,19 @@ __global__ void __launch_bounds__(128) svf_sweep_batch_kernel(const sw100_batch_
     int r, c;
     if (batch_pixel(S, T, r, c))
       svf_sweep_pixel(reinterpret_cast<const float4*>(S.src4), S.rows, S.cols, plan, S.steps,
-                      S.site.bush_any ? S.bflags : nullptr, S.site.vmax, S.svf_planes, S.svf_bits, r, c);
+                      S.site.bush_any ? S.bflags : nullptr, S.site.vmax, S.svf_planes, S.svf_bits, r, c,
+                      SkipMap{S.skipmap, (S.cols + 7) / 8});
   }
+}
+
+// Skip maps of the sites of a batch: grid.y = site, blocks stride over the
+// site's 8 x 8 cell blocks.
+__global__ void __launch_bounds__(128) skipmap_batch_kernel(const sw100_batch_site* __restrict__ sites) {
+  const sw100_batch_site& S = sites[blockIdx.y];
+  if (S.skipmap == nullptr) return;
+  const int ccol = (S.cols + 7) / 8, nb = ((S.rows + 7) / 8) * ccol;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+    skipmap_block(reinterpret_cast<const float4*>(S.src4), S.rows, S.cols, S.skipmap, ccol, b);
 }
 
 // Packs {dsm, vegdsm, vegdsm2, bush} of every site of a batch.

@@ -40,6 +40,28 @@ struct Single5 {
   uint32_t w[SW100_CUBE_WORDS];
 };
 
+// +0 or a positive number (+inf included); false for -0, negatives and NaN.
+// The march shortcuts that stop or skip steps require their thresholds to
+// be non-negative so that an out-of-grid zero source changes nothing, and
+// exclude -0 so that no later +0 source would have replaced a -0 maximum.
+__device__ __forceinline__ bool nonneg(float x) { return __float_as_uint(x) <= 0x7f800000u; }
+
+// Coarse bound on the march sources for skipping steps: m[b] is the largest
+// of dsm, vegdsm and vegdsm2 over the 8 x 8 cell block b and its eight
+// neighbours (row-major, ccol blocks per row), NaN when any of them is NaN.
+// Under SW100_STEP_SKIP8 at step k, steps k .. k+7 move at most one cell per
+// axis each and so stay inside the 3 x 3 blocks around step k's cell; with
+// dz not decreasing, m - dz(k) bounds every source height minus drop they
+// compute.  m == nullptr: no skipping.
+struct SkipMap {
+  const float* m;
+  int ccol;
+};
+
+__device__ __forceinline__ float skip_bound(const SkipMap& s, int r, int c) {
+  return __ldg(&s.m[(size_t)(r >> 3) * s.ccol + (c >> 3)]);
+}
+
 // Read-only cached load of one march step (16 bytes).
 __device__ __forceinline__ sw100_step load_step(const sw100_step* p) {
   const int4 v = __ldg(reinterpret_cast<const int4*>(p));
@@ -47,7 +69,7 @@ __device__ __forceinline__ sw100_step load_step(const sw100_step* p) {
   s.dx = v.x;
   s.dy = v.y;
   s.dz = __int_as_float(v.z);
-  s.pad = 0;
+  s.flags = v.w;
   return s;
 }
 

@@ -124,6 +124,32 @@ def _executed(dx, dy, dz, amax, rows, cols):
     return int(bad[0]) + 1 if bad.size else len(dz)
 
 
+def step_skip_flags(dx, dy, dz) -> np.ndarray:
+    """SW100_STEP_SKIP8 flags of one march's executed steps.  Step k >= 1 is
+    flagged when each of the steps k+1 .. k+7 that exist moves at most one
+    cell per axis from the step before, and dz does not decrease over the
+    steps k-1 .. k+7 (a NaN counts as a decrease).  The kernels' 8-step
+    shortcut -- one look-up in a block maximum of the sources over the 3 x 3
+    blocks of 8 x 8 cells around step k's cell -- is exact under these two
+    facts only; a march whose tables break them is marched step by step."""
+    n = len(dz)
+    flags = np.zeros(n, np.int32)
+    if n < 2:
+        return flags
+    dx, dy = np.asarray(dx, np.int64), np.asarray(dy, np.int64)
+    dz = np.asarray(dz, F32)
+    bad_mv = np.zeros(n + 8, np.int64)
+    bad_dz = np.zeros(n + 8, np.int64)
+    bad_mv[1:n] = (np.abs(np.diff(dx)) > 1) | (np.abs(np.diff(dy)) > 1)
+    bad_dz[1:n] = ~(dz[1:] >= dz[:-1])
+    cm = np.concatenate([[0], np.cumsum(bad_mv)])  # cm[b] = bad_mv[:b].sum()
+    cz = np.concatenate([[0], np.cumsum(bad_dz)])
+    k = np.arange(1, n)
+    ok = (cm[k + 8] - cm[k + 1] == 0) & (cz[k + 8] - cz[k] == 0)
+    flags[1:] = np.where(ok, N.STEP_SKIP8, 0)
+    return flags
+
+
 def _trig(az, alt):
     sin_a, cos_a, tan_a = torch.sin(az), torch.cos(az), torch.tan(az)
     return (F32(torch.sign(sin_a).item()), F32(torch.sign(cos_a).item()), F32(tan_a.item()),
@@ -247,6 +273,7 @@ def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03, 
             n = len(dz)
             t = np.zeros(n, N.STEP_DTYPE)
             t["dx"], t["dy"], t["dz"] = dx, dy, dz
+            t["flags"] = step_skip_flags(dx, dy, dz)
             chunks.append(t)
             plan["step_offset"][0, q] = off
             plan["step_count"][0, q] = n

@@ -1,0 +1,136 @@
+"""Early exits of the SVF sweep and the sun march.
+
+Host side: the SW100_STEP_SKIP8 flags certify, per step, that the next 8
+steps move at most one cell per axis each and that dz does not decrease
+(checked against a direct restatement on random and real tables).  Device
+side, on a city with tall buildings, one with NaN sources and one with
+negative heights: a sweep with the flags cleared (every step marched)
+equals the sweep with the 8-step shortcut bit for bit, and the sun march
+(which stops at settled building shadow and when nothing can reach the
+pixel any more) equals the oracle's full march bit for bit.
+"""
+import numpy as np
+import pytest
+
+from solweig_project_b200 import _native as N
+from solweig_project_b200 import tables as T
+
+
+def _flags_direct(dx, dy, dz):
+    n = len(dz)
+    out = np.zeros(n, np.int32)
+    for k in range(1, n):
+        ok = True
+        for j in range(k, min(k + 8, n)):
+            if not (dz[j] >= dz[j - 1]):
+                ok = False
+            if j > k and (abs(int(dx[j]) - int(dx[j - 1])) > 1 or abs(int(dy[j]) - int(dy[j - 1])) > 1):
+                ok = False
+        out[k] = N.STEP_SKIP8 if ok else 0
+    return out
+
+
+def test_skip_flags_match_direct_definition():
+    rng = np.random.default_rng(5)
+    for trial in range(200):
+        n = int(rng.integers(0, 40))
+        dx = np.cumsum(rng.choice([-1, 0, 1, 2], n, p=[0.2, 0.4, 0.35, 0.05])).astype(np.int32)
+        dy = np.cumsum(rng.choice([-2, -1, 0, 1], n, p=[0.05, 0.35, 0.4, 0.2])).astype(np.int32)
+        dz = np.cumsum(rng.choice([-0.5, 0.0, 1.0, 2.0], n, p=[0.05, 0.1, 0.6, 0.25])).astype(np.float32)
+        if n > 3 and trial % 7 == 0:
+            dz[n // 2] = np.nan
+        np.testing.assert_array_equal(T.step_skip_flags(dx, dy, dz), _flags_direct(dx, dy, dz))
+
+
+def test_real_tables_are_mostly_skippable():
+    plan, steps, _ = T.svf_plan(300, 300, 1.0, 60.0, False, 2)
+    for q in range(0, 153, 17):
+        o, n = int(plan["step_offset"][0, q]), int(plan["step_count"][0, q])
+        t = steps[o:o + n]
+        np.testing.assert_array_equal(t["flags"], _flags_direct(t["dx"], t["dy"], t["dz"]))
+    assert (steps["flags"] != 0).mean() > 0.9
+    for az, alt in ((95.0, 20.0), (180.0, 60.0), (272.5, 8.0), (45.0, 35.0)):
+        dx, dy, dz, _ = T.sun_table(az, alt, 1.0, 60.0, 300, 300)
+        f = T.step_skip_flags(dx, dy, dz)
+        np.testing.assert_array_equal(f, _flags_direct(dx, dy, dz))
+        assert f[0] == 0 and (len(f) < 2 or f[1:].mean() > 0.9)
+
+
+# ------------------------------------------------------------------- GPU
+def _city(kind):
+    from solweig_project_b200 import synthetic
+    c = synthetic.make_city(160, 144, seed=31, h_max=90.0, n_buildings=30, n_trees=40)
+    dsm, trees, dem = c.dsm.copy(), c.trees.copy(), c.dem.copy()
+    if kind == "nan":
+        dsm[40:43, 50:52] = np.nan
+        trees[100, 20] = np.nan
+    elif kind == "negative":
+        dem = dem - np.float32(3.0)
+        dsm = dsm - np.float32(3.0)
+    return c, dsm, trees, dem
+
+
+def _clear_flags(table_dev):
+    """Zero the flags word of every step of an uploaded step table."""
+    import torch
+    table_dev.view(torch.int32).view(-1, 4)[:, 3] = 0
+
+
+def _site(kind):
+    from solweig_project_b200 import synthetic
+    from solweig_project_b200.engine import DeviceSite
+    c, dsm, trees, dem = _city(kind)
+    # a fixed amaxvalue: with NaN sources the derived one is NaN and no
+    # march runs at all
+    return c, DeviceSite(dsm, trees, dem, c.walls, c.aspect, c.scale, landcover=c.landcover,
+                         lc_class=synthetic.default_lc_class(), amaxvalue=90.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["plain", "nan", "negative"])
+def test_svf_shortcut_is_exact(cuda, kind):
+    import torch
+
+    def run(clear):
+        _, s = _site(kind)
+        if clear:
+            _clear_flags(s.svf_tables()[1])
+        res = s.run_svf()
+        torch.cuda.synchronize()
+        return res.planes.cpu().numpy().view(np.uint32), res.bits.cpu().numpy()
+
+    fast, slow = run(False), run(True)
+    for name, a, b in zip(("planes", "bits"), fast, slow):
+        assert np.array_equal(a, b), (kind, name, int((a != b).sum()))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["plain", "nan", "negative"])
+def test_sun_march_exits_are_exact(cuda, kind):
+    import torch
+    from oracle import march as om
+    from solweig_project_b200 import synthetic
+    c, s = _site(kind)
+    s.run_svf()
+    geo = synthetic.load_sun_geometry("single")
+    ser = s.build_series(synthetic.make_met(7), geo["altitude"], geo["azimuth"], geo["zen"], geo["jday"],
+                         geo["dectime"], geo["altmax"], dict(synthetic.DEFAULT_LOCATION))
+    _, dbg = s.run_sun_march(ser)
+    dbg = dbg.cpu().numpy()
+    assert dbg.shape[0] >= 4
+    h = s.host
+    vegdsm, vegdsm2 = (s.t[k].cpu().numpy() for k in ("vegdsm", "vegdsm2"))
+    bush = s.t["bush"].cpu().numpy() if s.t["bush"] is not None else np.zeros_like(vegdsm)
+    asp = om.aspect_radians(c.aspect)
+    names = ("vegsh", "sh", "vbshvegsh", "wallsh", "wallsun", "wallshve", "facesh", "facesun")
+    for d in range(0, dbg.shape[0], 3):
+        i = int(ser.sun["t"][d])
+        az = torch.tensor(geo["azimuth"][0][i]).item()
+        alt = torch.tensor(geo["altitude"][0][i]).item()
+        want = om.wallheight_23(h["dsm"], vegdsm, vegdsm2, az, alt, float(c.scale), 90.0, bush, c.walls, asp)
+        for k, name in enumerate(names):
+            got, ref = dbg[d, k], np.asarray(want[k], np.float32)
+            # bit-equal, NaN payloads aside (the GPU's NaN is canonical, the
+            # host's keeps the operand's payload)
+            same = (got.view(np.uint32) == ref.view(np.uint32)) | (np.isnan(got) & np.isnan(ref))
+            assert same.all(), (kind, d, name, int((~same).sum()))

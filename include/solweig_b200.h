@@ -107,6 +107,56 @@ typedef struct {
   uint32_t single_step[SW100_CUBE_WORDS];
 } sw100_site_planes;
 
+/* ------------------------------------------------- site preparation -- */
+/* Maxima the host needs after sw100_prepare_site, by index into
+ * sw100_site_stats.max_key. */
+#define SW100_STAT_DSM 0          /* dsm */
+#define SW100_STAT_VEGDEM 1       /* canopy (clipped at 0) + dem: amaxvalue with the dsm maximum */
+#define SW100_STAT_VEGDSM 2       /* vegdsm, vegdsm2: the march bound with the dsm maximum */
+#define SW100_STAT_VEGDSM2 3
+#define SW100_STAT_ABS_DSM 4      /* |dsm|, |vegdsm|, |vegdsm2| */
+#define SW100_STAT_ABS_VEGDSM 5
+#define SW100_STAT_ABS_VEGDSM2 6
+#define SW100_STAT_BUSH 7         /* bush: the bush flag is "maximum > 0" */
+#define SW100_N_SITE_STATS 8
+
+/* Reductions of sw100_prepare_site (device memory, cleared by the call).
+ * A maximum x is stored as its order-preserving key k: k = bits | 2^31
+ * for x >= +0, k = ~bits for x <= -0 (so -0 < +0); NaN inputs set their
+ * bit in nan_mask instead, and the maximum is then NaN, as numpy's is. */
+typedef struct {
+  uint32_t max_key[SW100_N_SITE_STATS];
+  uint32_t nan_mask;        /* bit s: maximum s met a NaN */
+  uint32_t nonfinite;       /* a NaN or infinity in dsm, vegdsm or vegdsm2 */
+  uint32_t codes;           /* bit c: cleaned land-cover code c (1..7) occurs */
+  uint32_t bad_codes;       /* a cleaned land-cover value has no class row */
+} sw100_site_stats;
+
+/* Land-cover classes by cleaned code 1..7 (landcoverclasses_2016a rows):
+ * float32 TgK, Tstart, albedo, emissivity; bit c of `valid` set when code c
+ * has exactly one class row. */
+typedef struct {
+  float tgk[8];
+  float tstart[8];
+  float alb[8];
+  float emis[8];
+  uint32_t valid;
+} sw100_class_table;
+
+/* The rasters the chain derives from a site's inputs, all on the device in
+ * one pass (replaces the host preparation of utci_process.py:667-681,
+ * :733-766, :1377-1385 and solweig.py:2083): vegdsm, vegdsm2, bush,
+ * buildings, aspect in radians, the land-cover property planes and per
+ * pixel the cleaned land-cover code (class_idx; 0 without land cover), plus
+ * the maxima of sw100_site_stats.  Inputs and outputs are npix device
+ * planes; `landcover` may be NULL (default properties), `classes` is a host
+ * pointer, required with land cover. */
+int sw100_prepare_site(const float* dsm, const float* trees, const float* dem, const float* aspect_deg,
+                       const float* landcover, const sw100_class_table* classes, int rows, int cols,
+                       float* vegdsm, float* vegdsm2, float* bush, float* buildings, float* aspect_rad, float* tgk,
+                       float* tstart, float* alb, float* emis, uint8_t* class_idx, sw100_site_stats* stats,
+                       void* stream);
+
 /* ---------------------------------------------------------------- SVF -- */
 typedef struct {
   int32_t n_patches;                          /* 153 */

@@ -38,7 +38,8 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noal
            "sw100_diff_bbox", "sw100_batch_validate", "sw100_batch_pack", "sw100_batch_bush_flags",
            "sw100_batch_skipmap", "sw100_batch_svf", "sw100_batch_sun_march", "sw100_batch_flux_loop",
            "sw100_utci_steps", "sw100_nn_conv3x3_wgrad", "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2",
-           "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc")
+           "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc",
+           "sw100_prepare_site")
 ABI_VERSION = 2  # SW100_ABI_VERSION of include/solweig_b200.h
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
@@ -119,6 +120,27 @@ class SitePlanes(C.Structure):
     ]
 
 
+class ClassTable(C.Structure):
+    """sw100_class_table: land-cover properties by cleaned code."""
+    _fields_ = [("tgk", C.c_float * 8), ("tstart", C.c_float * 8), ("alb", C.c_float * 8), ("emis", C.c_float * 8),
+                ("valid", C.c_uint32)]
+
+
+N_SITE_STATS = 8
+STAT_DSM, STAT_VEGDEM, STAT_VEGDSM, STAT_VEGDSM2, STAT_ABS_DSM, STAT_ABS_VEGDSM, STAT_ABS_VEGDSM2, STAT_BUSH = range(8)
+SITE_STATS_WORDS = N_SITE_STATS + 4   # sw100_site_stats as uint32 words
+
+
+def stat_value(stats: np.ndarray, s: int) -> np.float32:
+    """Maximum s of a sw100_site_stats read back as uint32 words: NaN when a
+    NaN entered it, else the float whose order-preserving key is stored."""
+    if (int(stats[N_SITE_STATS]) >> s) & 1:
+        return np.float32(np.nan)
+    k = int(stats[s])
+    u = (k & 0x7fffffff) if k & 0x80000000 else (~k & 0xffffffff)
+    return np.array([u], np.uint32).view(np.float32)[0]
+
+
 class Series(C.Structure):
     _fields_ = [
         ("steps", C.c_void_p), ("n_t", C.c_int32), ("n_day", C.c_int32), ("sun", C.c_void_p),
@@ -184,6 +206,7 @@ def load(path: str = LIB_PATH):
             "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
             "sw100_batch_flux_loop")},
         "sw100_batch_skipmap": (C.c_int, [vp, C.c_int, vp]),
+        "sw100_prepare_site": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(ClassTable), C.c_int, C.c_int] + [vp] * 12),
         "sw100_diff_bbox": (C.c_int, [C.POINTER(SitePlanes), C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp,
                                       C.c_int64, vp]),
     }

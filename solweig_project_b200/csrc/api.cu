@@ -58,6 +58,11 @@ __global__ void nn_conv3x3_tc_kernel(const __nv_bfloat16* X, int N, int H, int W
 __global__ void nn_wgrad_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
                                 const __nv_bfloat16* dY, int Cout, int dstride, int dcoff, float* dW, float* dbias,
                                 int rows_per_block);
+__global__ void prepare_site_kernel(const float* dsm, const float* trees, const float* dem, const float* aspect_deg,
+                                    const float* landcover, sw100_class_table classes, size_t npix, float* vegdsm,
+                                    float* vegdsm2, float* bush, float* buildings, float* aspect_rad, float* tgk,
+                                    float* tstart, float* alb, float* emis, uint8_t* class_idx,
+                                    sw100_site_stats* stats);
 __global__ void nn_weights_kernel(const float* Wm, int Cin, int Cout, __nv_bfloat16* Wf, __nv_bfloat16* Wd);
 __global__ void nn_relu_bwd_kernel(__nv_bfloat16* dY, const __nv_bfloat16* Y, int64_t npix, int C, int dstride,
                                    int dcoff, int ystride, int ycoff);
@@ -434,6 +439,34 @@ int sw100_batch_flux_loop(const sw100_batch_site* sites, const sw100_tile* tiles
                           int block_y, int grid, void* stream) {
   return launch_batch(time_loop_batch_kernel, "time_loop_batch_kernel", sites, tiles, n_tiles, block_x, block_y,
                       grid, stream);
+}
+
+int sw100_prepare_site(const float* dsm, const float* trees, const float* dem, const float* aspect_deg,
+                       const float* landcover, const sw100_class_table* classes, int rows, int cols,
+                       float* vegdsm, float* vegdsm2, float* bush, float* buildings, float* aspect_rad, float* tgk,
+                       float* tstart, float* alb, float* emis, uint8_t* class_idx, sw100_site_stats* stats,
+                       void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  const void* in[] = {dsm, trees, dem, aspect_deg, vegdsm, vegdsm2, bush, buildings, aspect_rad, tgk, tstart, alb,
+                      emis, class_idx, stats};
+  const char* names[] = {"dsm", "trees", "dem", "aspect_deg", "vegdsm", "vegdsm2", "bush", "buildings",
+                         "aspect_rad", "tgk", "tstart", "alb", "emis", "class_idx", "stats"};
+  for (int k = 0; k < 15; ++k)
+    if ((rc = check_ptr(in[k], names[k]))) return rc;
+  sw100_class_table table = {};
+  if (landcover) {
+    if ((rc = check_ptr(classes, "classes"))) return rc;
+    table = *classes;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(stats, 0, sizeof(sw100_site_stats), st);
+  if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+  const size_t npix = (size_t)rows * cols;
+  const int grid = (int)std::min<size_t>((npix + 255) / 256, 148 * 8);
+  prepare_site_kernel<<<grid, 256, 0, st>>>(dsm, trees, dem, aspect_deg, landcover, table, npix, vegdsm, vegdsm2,
+                                            bush, buildings, aspect_rad, tgk, tstart, alb, emis, class_idx, stats);
+  return check_launch("prepare_site_kernel");
 }
 
 int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbshvegshmat, int rows, int cols,

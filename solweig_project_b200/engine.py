@@ -59,8 +59,15 @@ def _table(arr: np.ndarray, device) -> torch.Tensor:
 
 
 def to_host(t: torch.Tensor) -> np.ndarray:
+    """Device tensor -> numpy array in page-locked host memory (torch's
+    caching host allocator: a repeated call of the same size reuses the
+    buffer once the previous result is released)."""
     TRANSFER["d2h"] += t.numel() * t.element_size()
-    return t.cpu().numpy()
+    if t.device.type == "cpu":
+        return t.numpy()
+    out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    out.copy_(t)
+    return out.numpy()
 
 
 def _ptr(t):
@@ -129,26 +136,53 @@ class DeviceSite:
         self.rows, self.cols = a.shape
         if self.rows * self.cols >= 2 ** 31:
             raise ValueError("grid too large")
-        vegdsm, vegdsm2, bush, amax, buildings = march_inputs(a, trees, dem)
-        self.amax_fixed = amaxvalue is not None
-        self.amax = F32(amaxvalue) if amaxvalue is not None else amax
-        self._set_march_stats(a, vegdsm, vegdsm2, bush)
-        # host copies of the edited inputs (block edits update them in place)
-        self.host = {"dsm": a.copy(), "trees": np.asarray(trees, F32).copy(), "dem": np.asarray(dem, F32).copy()}
+        for name, x in (("trees", trees), ("dem", dem), ("walls", walls), ("aspect", aspect_deg),
+                        ("landcover", landcover), ("windcoeff", windcoeff)):
+            if x is not None and np.shape(x) != a.shape:
+                raise ValueError(f"{name} must have the shape of the DSM {a.shape}")
+        if landcover is not None and lc_class is None:
+            raise ValueError("landcover needs lc_class (the land-cover class table)")
         self.scale = float(scale)
         d = self.device
-        self.t = {
-            "dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
-            "bush": _dev(bush, d) if self.bush_any else None, "buildings": _dev(buildings, d),
-            "dem": _dev(np.asarray(dem, F32), d),
-            "walls": _dev(np.asarray(walls, F32), d),
-            "aspect_rad": _dev((np.asarray(aspect_deg, F32) * F32(np.pi)) / F32(180.), d),
-            "windcoeff": _dev(np.ones((self.rows, self.cols), F32) if windcoeff is None else
-                              np.asarray(windcoeff, F32), d),
-        }
-        self.props = TS.landcover_props(landcover, lc_class, self.rows, self.cols)
-        for k in ("tgk", "tstart", "alb", "emis"):
-            self.t[k] = _dev(getattr(self.props, k), d)
+        # the input rasters go up as they are; everything derived from them
+        # is computed on the device (sw100_prepare_site)
+        self.t = {"dsm": _dev(a, d), "trees": _dev(trees, d), "dem": _dev(dem, d), "walls": _dev(walls, d)}
+        aspect_d = _dev(aspect_deg, d)
+        lc_d = _dev(landcover, d) if landcover is not None else None
+        plane = lambda dtype=torch.float32: torch.empty((self.rows, self.cols), dtype=dtype, device=d)  # noqa: E731
+        for k in ("vegdsm", "vegdsm2", "bush", "buildings", "aspect_rad", "tgk", "tstart", "alb", "emis"):
+            self.t[k] = plane()
+        self.t["class_idx"] = plane(torch.uint8)
+        self.t["windcoeff"] = (torch.ones((self.rows, self.cols), dtype=torch.float32, device=d) if windcoeff is None
+                               else _dev(windcoeff, d))
+        table = N.ClassTable()
+        if landcover is not None:
+            tab, valid = TS.class_table(lc_class)
+            for k in ("tgk", "tstart", "alb", "emis"):
+                getattr(table, k)[:] = [float(v) for v in tab[k]]
+            table.valid = valid
+        stats = torch.empty(N.SITE_STATS_WORDS, dtype=torch.int32, device=d)
+        t = self.t
+        N.call("sw100_prepare_site", _ptr(t["dsm"]), _ptr(t["trees"]), _ptr(t["dem"]), _ptr(aspect_d), _ptr(lc_d),
+               C.byref(table), self.rows, self.cols, _ptr(t["vegdsm"]), _ptr(t["vegdsm2"]), _ptr(t["bush"]),
+               _ptr(t["buildings"]), _ptr(t["aspect_rad"]), _ptr(t["tgk"]), _ptr(t["tstart"]), _ptr(t["alb"]),
+               _ptr(t["emis"]), _ptr(t["class_idx"]), _ptr(stats), _stream())
+        st = to_host(stats).view(np.uint32)
+        if st[N.N_SITE_STATS + 3]:
+            raise ValueError("landcover holds a code without a row in lc_class")
+        v = {s: N.stat_value(st, s) for s in range(N.N_SITE_STATS)}
+        # the host computation's reductions, Python max() quirks with NaN included
+        amax = F32(max(v[N.STAT_DSM], v[N.STAT_VEGDEM]))
+        self.amax_fixed = amaxvalue is not None
+        self.amax = F32(amaxvalue) if amaxvalue is not None else amax
+        self.bush_any = bool(v[N.STAT_BUSH] > 0)
+        self.vmax = F32(max(v[N.STAT_DSM], v[N.STAT_VEGDSM], v[N.STAT_VEGDSM2]))
+        self.all_finite = not st[N.N_SITE_STATS + 1]
+        self.hmax = float(max(v[N.STAT_ABS_DSM], v[N.STAT_ABS_VEGDSM], v[N.STAT_ABS_VEGDSM2]))
+        if not self.bush_any:
+            self.t["bush"] = None
+        self.props = TS.device_props(lc_class if landcover is not None else None, st[N.N_SITE_STATS + 2])
+        self._host = None        # host copies of dsm / trees / dem, made on first use by an edit
         self.svf_result: SvfResult | None = None
         self.state = torch.zeros((6, self.rows, self.cols), dtype=torch.float32, device=d)
         self._keep = []
@@ -170,7 +204,7 @@ class DeviceSite:
         self.amax = F32(amaxvalue)
         self.amax_fixed = True
         self._set_march_stats(a, vegdsm, vegdsm2, bush)
-        self.host = None
+        self._host = None
         self.scale = float(scale)
         d = self.device
         self.t = {"dsm": _dev(a, d), "vegdsm": _dev(vegdsm, d), "vegdsm2": _dev(vegdsm2, d),
@@ -181,6 +215,19 @@ class DeviceSite:
         self._keep = []
         self._cache = {}
         return self
+
+    @property
+    def host(self):
+        """Host copies of the edited inputs (dsm, trees, dem), read back from
+        the device on first use; block edits update them in place.  None for
+        a site built from march rasters."""
+        if self._host is None and "trees" in self.t:
+            self._host = {k: to_host(self.t[k]).reshape(self.rows, self.cols).copy() for k in ("dsm", "trees", "dem")}
+        return self._host
+
+    @host.setter
+    def host(self, value):
+        self._host = value
 
     def _set_march_stats(self, a, vegdsm, vegdsm2, bush):
         self.bush_any = bool(bush.max() > 0)
@@ -438,7 +485,8 @@ class DeviceSite:
                               amax=self.amax, rows=self.rows, cols=self.cols, props=self.props,
                               params=self.params, time_start=time_start, time_stop=time_stop,
                               initial_scalars=initial_scalars)
-        self.t["class_idx"] = _upload(torch.from_numpy(ser.class_idx), self.device)
+        if ser.class_idx is not None:
+            self.t["class_idx"] = _upload(torch.from_numpy(ser.class_idx), self.device)
         return ser
 
     def upload_series(self, ser: TS.Series):

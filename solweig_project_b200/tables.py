@@ -263,30 +263,66 @@ def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03, 
     plan["tail"] = F32(3.0459e-004)
     plan["trans"] = F32(0.03)
     plan["trans_veg"] = F32(trans_veg)
-    chunks = []
-    off = 0
+    ring = np.repeat(np.arange(len(altint)), nband)[:P]
+    steps, counts = _svf_steps_all(azs[:P], np.asarray(altint)[ring], scale, amax, rows, cols)
     single = np.zeros(N.CUBE_WORDS, np.uint32)
-    q = 0
-    for i in range(len(altint)):
-        for _ in range(nband[i]):
-            dx, dy, dz = svf_patch_table(azs[q], altint[i], scale, amax, rows, cols)
-            n = len(dz)
-            t = np.zeros(n, N.STEP_DTYPE)
-            t["dx"], t["dy"], t["dz"] = dx, dy, dz
-            t["flags"] = step_skip_flags(dx, dy, dz)
-            chunks.append(t)
-            plan["step_offset"][0, q] = off
-            plan["step_count"][0, q] = n
-            plan["ring"][0, q] = i
-            a = float(azs[q])
-            plan["dir_flags"][0, q] = ((1 if 0 <= a < 180 else 0) | (2 if 90 <= a < 270 else 0) |
-                                       (4 if 180 <= a < 360 else 0) | (8 if (a >= 270 or a < 90) else 0))
-            if n <= 1:
-                single[q >> 5] |= np.uint32(1 << (q & 31))
-            off += n
-            q += 1
-    steps = np.concatenate(chunks) if chunks else np.zeros(0, N.STEP_DTYPE)
+    offsets = np.concatenate([[0], np.cumsum(counts)[:-1]]) if P else np.zeros(0, np.int64)
+    plan["step_offset"][0, :P] = offsets
+    plan["step_count"][0, :P] = counts
+    plan["ring"][0, :P] = ring
+    for q in range(P):
+        a = float(azs[q])
+        plan["dir_flags"][0, q] = ((1 if 0 <= a < 180 else 0) | (2 if 90 <= a < 270 else 0) |
+                                   (4 if 180 <= a < 360 else 0) | (8 if (a >= 270 or a < 90) else 0))
+        if counts[q] <= 1:
+            single[q >> 5] |= np.uint32(1 << (q & 31))
     return plan, steps, single
+
+
+def _svf_steps_all(azs, alts, scale, amax, rows, cols):
+    """Executed steps of every patch march at once (svf_patch_table applied
+    patch by patch gives the same float32 values: each element is the same
+    chain of float32 operations), concatenated in patch order with their
+    SW100_STEP_SKIP8 flags; returns (steps, counts)."""
+    P = len(azs)
+    trig = [_svf_patch_trig(float(a), int(h)) for a, h in zip(azs, alts)]
+    branch_y = np.array([t[0] for t in trig])[:, None]
+    ssin = np.array([t[1] for t in trig], F32)[:, None]
+    scos = np.array([t[2] for t in trig], F32)[:, None]
+    tan_a = np.array([t[3] for t in trig], F32)[:, None]
+    ds = np.array([t[4] for t in trig], F32)[:, None]
+    tanalt = np.array([F32(t[5] / F32(scale)) for t in trig], F32)[:, None]
+    fi = np.arange(1, max(rows, cols) + 3).astype(F32)[None, :]
+    m_scos = F32(-1.) * scos
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        dy = np.where(branch_y, ssin * fi, ssin * np.abs(np.rint(fi * tan_a))).astype(F32)
+        dx = np.where(branch_y, m_scos * np.abs(np.rint(fi / tan_a)), m_scos * fi).astype(F32)
+        dz = ((ds * fi) * tanalt).astype(F32)
+    L = fi.shape[1]
+    ok = (F32(amax) >= dz) & (np.abs(dx) < rows) & (np.abs(dy) < cols)
+    first_bad = np.where(ok.all(axis=1), L, np.argmin(ok, axis=1) + 1)
+    counts = first_bad if F32(amax) >= F32(0.) else np.zeros(P, np.int64)
+    counts = np.minimum(counts, L).astype(np.int64)
+    L = int(counts.max()) if P else 0          # no patch executes beyond this
+    dx, dy, dz = dx[:, :L], dy[:, :L], dz[:, :L]
+    live = np.arange(L)[None, :] < counts[:, None]
+    dxi, dyi = dx.astype(np.int32), dy.astype(np.int32)
+    # SW100_STEP_SKIP8: per row, over the steps that exist
+    bad_mv = np.zeros((P, L + 8), np.int64)
+    bad_dz = np.zeros((P, L + 8), np.int64)
+    both = live[:, 1:] & live[:, :-1]
+    bad_mv[:, 1:L] = both & ((np.abs(np.diff(dxi.astype(np.int64), axis=1)) > 1) |
+                             (np.abs(np.diff(dyi.astype(np.int64), axis=1)) > 1))
+    bad_dz[:, 1:L] = both & ~(dz[:, 1:] >= dz[:, :-1])
+    cm = np.concatenate([np.zeros((P, 1), np.int64), np.cumsum(bad_mv, axis=1)], axis=1)
+    cz = np.concatenate([np.zeros((P, 1), np.int64), np.cumsum(bad_dz, axis=1)], axis=1)
+    # flag k: no bad move in k+1 .. k+7, no decreasing dz in k .. k+7
+    flag_ok = (cm[:, 8:8 + L] - cm[:, 1:1 + L] == 0) & (cz[:, 8:8 + L] - cz[:, 0:L] == 0) & \
+        (np.arange(L)[None, :] >= 1)
+    steps = np.zeros(int(counts.sum()), N.STEP_DTYPE)
+    steps["dx"], steps["dy"], steps["dz"] = dxi[live], dyi[live], dz[live]
+    steps["flags"] = np.where(flag_ok, N.STEP_SKIP8, 0).astype(np.int32)[live]
+    return steps, counts
 
 
 # ------------------------------------------- windowed SVF recompute

@@ -236,23 +236,56 @@ def _steradians_uncached(palt):
     return ster
 
 
+_LSKY_CACHE: dict = {}
+_THR_CACHE: dict = {}
+
+
+def _thr_bounds(palt):
+    """atan_degree_bounds of every patch altitude, as two float32 vectors."""
+    key = palt.numpy().tobytes()
+    hit = _THR_CACHE.get(key)
+    if hit is None:
+        b = np.array([T.atan_degree_bounds(float(pa)) for pa in palt.numpy()], F32).reshape(-1, 2)
+        hit = _THR_CACHE.setdefault(key, (b[:, 0].copy(), b[:, 1].copy()))
+    return hit
+
+
+def _lsky_geometry(palt):
+    """The step-independent part of _lsky for a patch-altitude vector: the
+    distinct altitudes u, the band exponential of each, the patch -> u index,
+    the solid angles and sin / cos of each altitude (0-dim evaluations, as
+    the per-altitude loop makes them), rounded to the planes' dtype."""
+    key = (palt.numpy().tobytes(), str(palt.dtype))
+    hit = _LSKY_CACHE.get(key)
+    if hit is None:
+        deg2rad = torch.tensor(np.pi / 180)
+        u, _ = torch.unique(palt, return_counts=True)
+        expo = torch.exp(0.308 * (1.7 - (1 / torch.cos((90 - u) * deg2rad))))
+        idx = torch.searchsorted(u, palt.contiguous())
+        sin_u = torch.stack([torch.sin(alt * deg2rad) for alt in u])
+        cos_u = torch.stack([torch.cos(alt * deg2rad) for alt in u])
+        hit = _LSKY_CACHE.setdefault(key, (u, expo, idx, _steradians(palt), sin_u, cos_u))
+    return hit
+
+
 def _lsky(esky, palt, Ta64):
     """Sky longwave per patch on horizontal / vertical surfaces with the
-    Martin & Berdahl band emissivities (model2, solweig.py:1394-1413, 1725-1737)."""
-    deg2rad = torch.tensor(np.pi / 180)
+    Martin & Berdahl band emissivities (model2, solweig.py:1394-1413, 1725-1737).
+    Per distinct altitude: base = (band * sbc * Ta^4) / pi, then per patch
+    base * ster * sin(alt) (cos for the vertical); evaluated here as whole
+    vectors, each element by the same float32 operations."""
+    u, expo, idx, ster, sin_u, cos_u = _lsky_geometry(palt)
     sbc = torch.tensor(SBC)
-    u, _ = torch.unique(palt, return_counts=True)
-    band = 1 - (1 - esky) * torch.exp(0.308 * (1.7 - (1 / torch.cos((90 - u) * deg2rad))))
-    ster = _steradians(palt)
+    band = 1 - (1 - esky) * expo
+    ta4 = (Ta64 + 273.15) ** 4
+    base = ((band * sbc * ta4) / torch.tensor(np.pi))[idx]
+    bs = base * ster
+    dt = bs.dtype
     ld = torch.zeros(palt.shape[0])
     ls = torch.zeros(palt.shape[0])
-    ta4 = (Ta64 + 273.15) ** 4
-    for alt in u:
-        msk = palt == alt
-        base = (band[u == alt] * sbc * ta4) / torch.tensor(np.pi)
-        ld[msk] = base * ster[msk] * torch.sin(alt * deg2rad)
-        ls[msk] = base * ster[msk] * torch.cos(alt * deg2rad)
-    return ld, ls, ster
+    ld[:] = bs * sin_u[idx].to(dt)
+    ls[:] = bs * cos_u[idx].to(dt)
+    return ld, ls, ster.clone()
 
 
 def utci_pow(x, p: int) -> np.float32:
@@ -331,6 +364,51 @@ class LandCoverProps:
     tstart_wall: object
     tmaxlst_wall: object
     landcover: int
+    # Sites prepared on the device (sw100_prepare_site) keep no property
+    # rasters on the host: their pixels carry the cleaned land-cover code,
+    # `codes` has bit c set when code c occurs and `code_tmax[c]` is that
+    # class's TmaxLST.
+    codes: int = 0
+    code_tmax: np.ndarray | None = None
+    device_classes: bool = False
+
+
+_PROP_COLS = {"tstart": 4, "alb": 1, "emis": 2, "tmax": 5, "tgk": 3}
+
+
+def class_table(lc_class):
+    """Per cleaned land-cover code 1..7 the float32 TgK, Tstart, albedo,
+    emissivity and TmaxLST of its class row, and the mask of codes that have
+    exactly one row (landcover_props gives every pixel of such a code that
+    row's values; a code without its row is refused)."""
+    lc_class = np.asarray(lc_class)
+    tab = {k: np.zeros(8, F32) for k in _PROP_COLS}
+    valid = 0
+    for c in range(1, 8):
+        hit = np.flatnonzero(lc_class[:, 0] == c)
+        if len(hit) == 1:
+            valid |= 1 << c
+            for k, j in _PROP_COLS.items():
+                tab[k][c] = F32(lc_class[hit[0], j])
+    return tab, valid
+
+
+def wall_class(lc_class):
+    """TgK, Tstart and TmaxLST of the wall class (code 99)."""
+    lc_class = np.asarray(lc_class)
+    wall = np.where(lc_class[:, 0] == 99)
+    return (np.asarray(lc_class[wall, 3], F32), np.asarray(lc_class[wall, 4], F32),
+            np.asarray(lc_class[wall, 5], F32))
+
+
+def device_props(lc_class, codes) -> LandCoverProps:
+    """Land-cover description of a device-prepared site (no host rasters);
+    lc_class None: the default properties."""
+    if lc_class is None:
+        return LandCoverProps(None, None, None, None, None, 0.37, -3.41, 15., 0, device_classes=True)
+    tab, _ = class_table(lc_class)
+    return LandCoverProps(None, None, None, None, None, *wall_class(lc_class), 1, codes=int(codes),
+                          code_tmax=tab["tmax"], device_classes=True)
 
 
 def landcover_props(lc_grid, lc_class, rows, cols) -> LandCoverProps:
@@ -363,7 +441,7 @@ class Series:
     patch: np.ndarray         # PATCH_STEP_DTYPE (n_t, P)
     gvf: np.ndarray           # GVF_AZ_DTYPE (18)
     final: dict               # carried scalars after the last step
-    class_idx: np.ndarray     # uint8 per pixel
+    class_idx: np.ndarray     # uint8 per pixel (None: the site's device plane holds the classes)
 
 
 def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, scale, amax, rows, cols,
@@ -404,15 +482,24 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         firstdaytime = float(initial_scalars["firstdaytime"])
         CI = float(initial_scalars["CI"])
 
-    # pixel classes of the ground temperature wave
-    if props.landcover:
+    # pixel classes of the ground temperature wave: the distinct TmaxLST
+    # values in ascending order (np.unique of the raster); a device-prepared
+    # site indexes tg_factor by land-cover code instead, each code's slot
+    # holding its TmaxLST value's factor
+    code_slot = None
+    if props.landcover and props.device_classes:
+        present = [c for c in range(1, 8) if (props.codes >> c) & 1]
+        tvals = np.unique(np.asarray(props.code_tmax, F32)[present])
+        code_slot = {c: int(np.searchsorted(tvals, props.code_tmax[c])) for c in present}
+        class_idx = None
+    elif props.landcover:
         tvals, class_idx = np.unique(props.tmaxlst, return_inverse=True)
         if len(tvals) > N.MAX_CLASSES:
             raise ValueError(f"more than {N.MAX_CLASSES} distinct TmaxLST classes")
         class_idx = class_idx.reshape(rows, cols).astype(np.uint8)
     else:
         tvals = np.array([15.], F32)
-        class_idx = np.zeros((rows, cols), np.uint8)
+        class_idx = None if props.device_classes else np.zeros((rows, cols), np.uint8)
 
     P = int(sum(T.PATCH_LAYOUT[patch_option][3]))
     steps = np.zeros(n_t, N.TIME_STEP_DTYPE)
@@ -499,7 +586,12 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             else:
                 fac = torch.tensor([float(F32(torch.sin((phase / (15. / 24 - SNUP / 24)) * np.pi / 2).item()))])
                 tgwall = (0.37 * altmax64 + -3.41) * torch.sin((phase / (15. / 24 - SNUP / 24)) * np.pi / 2)
-            S["tg_factor"][:len(tvals)] = fac.numpy().astype(F32)
+            fac_n = fac.numpy().astype(F32)
+            if code_slot is None:
+                S["tg_factor"][:len(tvals)] = fac_n
+            else:
+                for code, k in code_slot.items():
+                    S["tg_factor"][code] = fac_n[k]
             tgwall = torch.maximum(tgwall, torch.tensor(0))
             tgwall = tgwall * CI_TgG
             lwall = sbc_t * ewall_t * (tgwall + Ta64 + 273.15) ** 4 - sbc_t * ewall_t * (Ta64 + 273.15) ** 4
@@ -585,8 +677,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         Q["sh_sin"] = Q["veg_sin"]
         Q["sun_cos"] = (sun_surf * ster_l.numpy()) * cos_l.numpy()
         Q["sun_sin"] = (sun_surf * ster_l.numpy()) * sin_l.numpy()
-        for k, pa in enumerate(palt_l.numpy()):
-            Q["thr_sun"][k], Q["thr_shd"][k] = T.atan_degree_bounds(float(pa))
+        Q["thr_sun"], Q["thr_shd"] = _thr_bounds(palt_l)
     sun = np.array(sun_rows, N.SUN_STEP_DTYPE) if sun_rows else np.zeros(0, N.SUN_STEP_DTYPE)
     table = np.concatenate(tables) if tables else np.zeros(0, N.STEP_DTYPE)
     final = {"CI": float(CI), "firstdaytime": float(firstdaytime), "timeadd": float(timeadd)}

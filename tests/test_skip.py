@@ -134,3 +134,24 @@ def test_sun_march_exits_are_exact(cuda, kind):
             # host's keeps the operand's payload)
             same = (got.view(np.uint32) == ref.view(np.uint32)) | (np.isnan(got) & np.isnan(ref))
             assert same.all(), (kind, d, name, int((~same).sum()))
+
+
+@pytest.mark.parametrize("rows,cols,scale,amax", [(36, 36, 1.0, 12.5), (24, 40, 0.5, 9.0), (1, 16, 1.0, 3.0),
+                                                   (300, 120, 2.0, 88.6), (64, 64, 1.0, 0.0), (64, 64, 1.0, -1.0),
+                                                   (50, 50, 1.0, float("nan"))])
+def test_plan_equals_per_patch_tables(rows, cols, scale, amax):
+    """svf_plan builds every patch's steps at once; each patch's rows equal
+    svf_patch_table's, and its flags the direct definition."""
+    plan, steps, single = T.svf_plan(rows, cols, scale, np.float32(amax), False, 2)
+    _, altint, _, nband = T.PATCH_LAYOUT[2]
+    azs = T.sweep_azimuths(2)
+    ring = np.repeat(np.arange(len(altint)), nband)
+    for q in range(153):
+        dx, dy, dz = T.svf_patch_table(azs[q], altint[ring[q]], scale, np.float32(amax), rows, cols)
+        o, n = int(plan["step_offset"][0, q]), int(plan["step_count"][0, q])
+        assert n == len(dz)
+        t = steps[o:o + n]
+        assert np.array_equal(t["dx"], dx) and np.array_equal(t["dy"], dy)
+        assert np.array_equal(t["dz"].view(np.uint32), dz.view(np.uint32))
+        assert np.array_equal(t["flags"], _flags_direct(dx, dy, dz))
+        assert bool((int(single[q >> 5]) >> (q & 31)) & 1) == (n <= 1)

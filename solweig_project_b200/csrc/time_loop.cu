@@ -398,12 +398,12 @@ __device__ __forceinline__ void time_loop_tile(
       if (day) {
         for (int j = 0; j < nq; ++j) {
           const sw100_patch_step& Q = PP[q0 + j];
-          const bool sh = (sw >> j) & 1u, veg = (vw >> j) & 1u;
-          const float4 kd = *reinterpret_cast<const float4*>(Q.kside_d);
-          const float4 an = *reinterpret_cast<const float4*>(Q.anilum);
-          ksideD = ksideD + (sh ? (veg ? kd.w : kd.z) : (veg ? kd.y : kd.x));
-          anilum = anilum + (sh ? (veg ? an.w : an.z) : (veg ? an.y : an.x));
-          if (sh && veg) { ld_sky = ld_sky + Q.ld_sky; ls_sky = ls_sky + Q.ls_sky; }
+          // the (sh, vegsh) code indexes the patch's four increments: lanes
+          // read different words of one 16-byte group, no bank conflict
+          const int code = (int)((sw >> j) & 1u) * 2 + (int)((vw >> j) & 1u);
+          ksideD = ksideD + Q.kside_d[code];
+          anilum = anilum + Q.anilum[code];
+          if (code == 3) { ld_sky = ld_sky + Q.ld_sky; ls_sky = ls_sky + Q.ls_sky; }
         }
       } else {
         for (int j = 0; j < nq; ++j) {

@@ -88,6 +88,8 @@ def _utci_terms():
 
 
 _TERMS = _utci_terms()
+_TERM_C = np.array([F32(c) for c, _, _, _, _ in _TERMS], F32)      # coefficient of each term
+_TERM_PT = np.array([pt for _, pt, _, _, _ in _TERMS], np.int64)  # its power of Ta
 _ES_G = (-2.8365744E3, -6.028076559E3, 1.954263612E1, -2.737830188E-2, 1.6261698E-5, 7.0229056E-10,
          -1.8680009E-13, 2.7150305)
 
@@ -161,10 +163,28 @@ def _diffuse(radG, altitude, Kt, Ta, RH):
     return radI, radD
 
 
+_PEREZ_GEOM: dict = {}
+_PEREZ_CO: dict = {}
+
+
+def _perez_geometry():
+    """Patch angles of the Perez distribution and their step-independent
+    trigonometry (the same tensors every step evaluates)."""
+    if not _PEREZ_GEOM:
+        deg2rad = torch.tensor(np.pi / 180)
+        rad2deg = torch.tensor(180 / np.pi)
+        alt_p, azi_p = (torch.from_numpy(v) for v in T.sky_patches(2))
+        skyzen = (90 - alt_p) * deg2rad
+        skyalt = alt_p * deg2rad
+        skyazi = azi_p * deg2rad
+        _PEREZ_GEOM.update(skyazi=skyazi, sin_alt=torch.sin(skyalt), cos_alt=torch.cos(skyalt),
+                           cos_zen=torch.cos(skyzen), alt_deg=skyalt * rad2deg, azi_deg=skyazi * rad2deg)
+    return _PEREZ_GEOM
+
+
 def _perez(zen_deg, azimuth_deg, radD, radI, jday):
     """Perez_v3 with patchchoice 1 (solweig.py:1227-1356): (P, 3) float32."""
     deg2rad = torch.tensor(np.pi / 180)
-    rad2deg = torch.tensor(180 / np.pi)
     zen = torch.tensor(zen_deg) * deg2rad
     azimuth = torch.tensor(azimuth_deg) * deg2rad
     altitude = torch.tensor(90 - zen_deg) * deg2rad
@@ -184,7 +204,9 @@ def _perez(zen_deg, azimuth_deg, radD, radI, jday):
     if radD <= 10:
         bright = torch.tensor(0.0)
     ic = next((j for j, b in enumerate(_CLEAR_BINS) if clearness < b), 7)
-    co = {k: torch.tensor(v[ic]) for k, v in _PEREZ.items()}
+    co = _PEREZ_CO.get(ic)
+    if co is None:
+        co = _PEREZ_CO.setdefault(ic, {k: torch.tensor(v[ic]) for k, v in _PEREZ.items()})
 
     def lin(c):
         return c[0] + c[1] * zen + bright * (c[2] + c[3] * zen)
@@ -196,16 +218,13 @@ def _perez(zen_deg, azimuth_deg, radD, radI, jday):
         c, d = co["c"], co["d"]
         m_c = torch.exp(torch.pow(bright * (c[0] + c[1] * zen), c[2])) - 1
         m_d = -torch.exp(bright * (d[0] + d[1] * zen)) + d[2] + bright * d[3] * bright
-    alt_p, azi_p = (torch.from_numpy(v) for v in T.sky_patches(2))
-    skyzen = (90 - alt_p) * deg2rad
-    skyalt = alt_p * deg2rad
-    skyazi = azi_p * deg2rad
-    cs = torch.sin(skyalt) * torch.sin(altitude) + torch.cos(altitude) * torch.cos(skyalt) * \
-        torch.cos(torch.abs(skyazi - azimuth))
-    lv = (1 + m_a * torch.exp(m_b / torch.cos(skyzen))) * ((1 + m_c * torch.exp(m_d * torch.arccos(cs)) +
-                                                          m_e * cs * cs))
+    g = _perez_geometry()
+    cs = g["sin_alt"] * torch.sin(altitude) + torch.cos(altitude) * g["cos_alt"] * \
+        torch.cos(torch.abs(g["skyazi"] - azimuth))
+    lv = (1 + m_a * torch.exp(m_b / g["cos_zen"])) * ((1 + m_c * torch.exp(m_d * torch.arccos(cs)) +
+                                                      m_e * cs * cs))
     lv = lv / torch.sum(lv)
-    return torch.stack([skyalt * rad2deg, skyazi * rad2deg, lv], dim=1)
+    return torch.stack([g["alt_deg"], g["azi_deg"], lv], dim=1)
 
 
 _STER_CACHE: dict = {}
@@ -329,7 +348,8 @@ def _utci_table(ta_mat: np.float32, rh32: np.float32):
     pa = utci_vapour_pressure(ta_mat, rh32)
     pa_pows = np.array([utci_pow(pa, p) for p in range(1, 7)], F32)
     ta_pows = [F32(1)] + [utci_pow(ta_mat, p) for p in range(1, 7)]
-    k = np.array([F32(c) * ta_pows[pt] if pt else F32(c) for c, pt, _, _, _ in _TERMS], F32)
+    # c * Ta^pt per term in float32 (c * 1 for the Ta-free terms is c itself)
+    k = _TERM_C * np.array(ta_pows, F32)[_TERM_PT]
     return pa_pows, k
 
 

@@ -93,28 +93,84 @@ def make_workload(name, rank, side=None):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clock and throttle-reason samples during the timed region: an NVML
+    polling thread (every ~2 ms, the first sample taken before the region
+    starts), nvidia-smi as the fallback when NVML is unavailable."""
 
     FIELDS = ("clocks.sm", "clocks.max.sm", "clocks_event_reasons.active", "clocks_event_reasons.hw_slowdown",
               "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
               "clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index):
         self.path = tempfile.mktemp(suffix=".csv")
         self.proc = None
         self.gpu = gpu_index
+        self.rows = []
+        self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.gpu)
+        bus = getattr(props, "pci_bus_id", None)
+        if bus is not None:
+            dom, dev = getattr(props, "pci_domain_id", 0), getattr(props, "pci_device_id", 0)
+            try:
+                return pynvml.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dev:02x}.0")
+            except pynvml.NVMLError:
+                pass
+        uuid = str(getattr(props, "uuid", ""))
+        if uuid:
+            try:
+                return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except pynvml.NVMLError:
+                pass
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in vis.split(",") if v.strip()]
+        idx = int(ids[self.gpu]) if ids and ids[self.gpu].strip().isdigit() else self.gpu
+        return pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _poll(self, handle, ready):
+        import pynvml
+        bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+        mx = pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM)
+        while True:
+            sm = pynvml.nvmlDeviceGetClockInfo(handle, pynvml.NVML_CLOCK_SM)
+            r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+            self.rows.append((float(sm), float(mx), {k for k, b in bits.items() if r & b}))
+            ready.set()
+            if self.stop.wait(0.002):
+                return
 
     def __enter__(self):
+        import threading
+        try:
+            handle = self._nvml_handle()
+            self.stop, ready = threading.Event(), threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(handle, ready), daemon=True)
+            self.thread.start()
+            ready.wait(2.0)
+            return self
+        except Exception:  # noqa: BLE001 - any NVML trouble: fall back to nvidia-smi
+            self.thread = None
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + ",".join(self.FIELDS),
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -124,16 +180,21 @@ class ClockSampler:
             self.fh.close()
 
     def summary(self):
+        if self.thread is not None:
+            sm = [r[0] for r in self.rows]
+            mx = [r[1] for r in self.rows]
+            reasons = sorted(set().union(*[r[2] for r in self.rows])) if self.rows else []
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml"}
         try:
             rows = [[c.strip() for c in line.split(",")] for line in open(self.path) if line.strip()]
         except OSError:
             rows = []
         sm = [float(r[0]) for r in rows if r and r[0].replace(".", "").isdigit()]
         mx = [float(r[1]) for r in rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        reasons = sorted({self.REASONS[i] for r in rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(sm)}
+                "reasons": reasons, "samples": len(sm), "source": "nvidia-smi"}
 
 
 def cpu_baseline(city, met, geo, lc_class, crop=64):

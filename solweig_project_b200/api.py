@@ -172,11 +172,10 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
     if initial_state is not None:
         init_scalars = _validate_state(initial_state, rows, cols, time_start, out_window)
         site.load_state(initial_state)
-    ser = site.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                            time_start=time_start, time_stop=time_stop, initial_scalars=init_scalars)
     gpu_vars = [k for k in N.OUT_BITS if k in requested]
-    out = site.run_time_loop(ser, requested=gpu_vars)
-    outputs = {k: E.to_host(v) for k, v in out.items()}
+    outputs, final_scalars = site.run_chain_chunked(met_file, altitude, azimuth, zen, jday, dectime, altmax,
+                                                    location, requested=gpu_vars, time_start=time_start,
+                                                    time_stop=time_stop, initial_scalars=init_scalars)
     n_t = time_stop - time_start
     if "ta" in requested:
         uh = met_file[:, 24] if met_file.shape[1] > 24 else np.zeros(met_file.shape[0])
@@ -193,8 +192,8 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
         return outputs
     st = site.state_dict()
     final = {k: (v[r0:r1, c0:c1].clone() if out_window is not None else v) for k, v in st.items()}
-    final.update(CI=ser.final["CI"], firstdaytime=ser.final["firstdaytime"], timeadd=ser.final["timeadd"],
-                 Twater=None, next_step=int(time_stop))
+    final.update(CI=final_scalars["CI"], firstdaytime=final_scalars["firstdaytime"],
+                 timeadd=final_scalars["timeadd"], Twater=None, next_step=int(time_stop))
     return outputs, final
 
 
@@ -282,8 +281,10 @@ def run_exact_chain(*, dsm, trees, dem, walls, aspect, scale, met_file, altitude
     site = E.DeviceSite(dsm, trees, dem, walls, aspect, scale, landcover=landcover, lc_class=lc_class,
                         windcoeff=windcoeff, params=_model_params(model_parameters))
     site.run_svf()
-    ser = site.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location)
-    out = site.run_time_loop(ser, requested=[k for k in N.OUT_BITS if k in requested])
     if return_device:
-        return out
-    return {k: E.to_host(v) for k, v in out.items()}
+        ser = site.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location)
+        return site.run_time_loop(ser, requested=[k for k in N.OUT_BITS if k in requested])
+    # host tables of later steps are built while the GPU runs earlier ones
+    out, _ = site.run_chain_chunked(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
+                                    requested=requested)
+    return out

@@ -548,6 +548,41 @@ class DeviceSite:
         N.call("sw100_flux_loop", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc),
                _ptr(self.state), out_mask, _ptr(outputs), _stream())
 
+    def run_chain_chunked(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
+                          requested=("utci",), time_start=0, time_stop=None, initial_scalars=None, chunk_steps=6):
+        """The time loop of steps [time_start, time_stop) with the host tables
+        built chunk by chunk while the GPU works: the tables of `chunk_steps`
+        steps are built, their sun march and flux loop launched and their
+        outputs copied asynchronously into page-locked host arrays; then the
+        next chunk's tables are built while those run.  The thermal state
+        (device planes) and the carried scalars (CI, timeadd, firstdaytime)
+        pass from chunk to chunk exactly as between the reference's
+        consecutive windows, so the result equals one launch over all steps
+        bit for bit.  Returns ({name: (T, rows, cols) float32 ndarray},
+        final carried scalars)."""
+        if self.svf_result is None:
+            raise RuntimeError("run_svf() (or set_svf()) must come before the time loop")
+        if time_stop is None:
+            time_stop = met_file.shape[0]
+        if chunk_steps < 1:
+            raise ValueError("chunk_steps must be >= 1")
+        names = [k for k in N.OUT_BITS if k in requested]
+        n_t = time_stop - time_start
+        host = {k: torch.empty((n_t, self.rows, self.cols), dtype=torch.float32, pin_memory=True) for k in names}
+        scalars, keep = initial_scalars, []
+        for t0 in range(time_start, time_stop, chunk_steps):
+            t1 = min(time_stop, t0 + chunk_steps)
+            ser = self.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
+                                    time_start=t0, time_stop=t1, initial_scalars=scalars)
+            scalars = ser.final
+            out = self.run_time_loop(ser, requested=names)
+            for k in names:
+                host[k][t0 - time_start:t1 - time_start].copy_(out[k], non_blocking=True)
+                TRANSFER["d2h"] += out[k].numel() * out[k].element_size()
+            keep.append((out, self._keep))
+        torch.cuda.current_stream().synchronize()
+        return {k: v.numpy() for k, v in host.items()}, scalars
+
     def load_state(self, state: dict):
         for k, name in enumerate(STATE_NAMES):
             v = state[name]

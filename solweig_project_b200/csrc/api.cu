@@ -182,7 +182,8 @@ int64_t skipmap_bytes(int rows, int cols) { return align_up((int64_t)((rows + 7)
 
 int launch_skipmap(const float4* src4, int rows, int cols, float* skipmap, cudaStream_t st) {
   const int crow = (rows + 7) / 8, ccol = (cols + 7) / 8;
-  svf_skipmap_kernel<<<(crow * ccol + 127) / 128, 128, 0, st>>>(src4, rows, cols, skipmap, crow, ccol);
+  const long long threads = (long long)crow * ccol * 32;  // one warp per 8 x 8 block
+  svf_skipmap_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(src4, rows, cols, skipmap, crow, ccol);
   return check_launch("svf_skipmap_kernel");
 }
 
@@ -419,7 +420,7 @@ int sw100_batch_skipmap(const sw100_batch_site* sites, int n_sites, void* stream
   if (n_sites < 0 || n_sites > 65535) return fail(SW100_E_ARG, "n_sites must be in [0, 65535]");
   if (n_sites == 0) return 0;
   if ((rc = check_ptr(sites, "sites"))) return rc;
-  skipmap_batch_kernel<<<dim3(64, n_sites), 128, 0, static_cast<cudaStream_t>(stream)>>>(sites);
+  skipmap_batch_kernel<<<dim3(256, n_sites), 128, 0, static_cast<cudaStream_t>(stream)>>>(sites);
   return check_launch("skipmap_batch_kernel");
 }
 

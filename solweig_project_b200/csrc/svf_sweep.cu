@@ -316,26 +316,30 @@ __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4,
 
 // The skip map of a site: for each 8 x 8 block, the largest source height
 // (dsm, vegdsm, vegdsm2) over the block and its neighbours; NaN propagates
-// (a NaN bound never passes the skip test).
-__device__ __forceinline__ void skipmap_block(const float4* __restrict__ src4, int rows, int cols,
-                                              float* __restrict__ m, int ccol, int b) {
+// (a NaN bound never passes the skip test; the sign of a zero maximum does
+// not matter to the test).  One warp per block: the lanes stride over the
+// (up to) 24 x 24 cells and reduce with shuffles.
+__device__ __forceinline__ void skipmap_block_warp(const float4* __restrict__ src4, int rows, int cols,
+                                                   float* __restrict__ m, int ccol, int b, int lane) {
   const int br = b / ccol, bc = b % ccol;
   const int r0 = max(0, (br - 1) * 8), r1 = min(rows, (br + 2) * 8);
   const int c0 = max(0, (bc - 1) * 8), c1 = min(cols, (bc + 2) * 8);
+  const int w = c1 - c0, n = (r1 - r0) * w;
   float v = -INFINITY;
-  for (int r = r0; r < r1; ++r)
-    for (int c = c0; c < c1; ++c) {
-      const float4 s = src4[(size_t)r * cols + c];
-      v = tmax(v, tmax(s.x, tmax(s.y, s.z)));
-    }
-  m[b] = v;
+  for (int i = lane; i < n; i += 32) {
+    const float4 s = src4[(size_t)(r0 + i / w) * cols + (c0 + i % w)];
+    v = tmax(v, tmax(s.x, tmax(s.y, s.z)));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = tmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  if (lane == 0) m[b] = v;
 }
 
 __global__ void svf_skipmap_kernel(const float4* __restrict__ src4, int rows, int cols, float* __restrict__ m,
                                    int crow, int ccol) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= crow * ccol) return;
-  skipmap_block(src4, rows, cols, m, ccol, b);
+  const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (b >= crow * ccol) return;  // whole warps: the block count is a multiple of 32 threads
+  skipmap_block_warp(src4, rows, cols, m, ccol, b, threadIdx.x & 31);
 }
 
 __global__ void __launch_bounds__(128) svf_sweep_kernel(
@@ -381,8 +385,10 @@ __global__ void __launch_bounds__(128) skipmap_batch_kernel(const sw100_batch_si
   const sw100_batch_site& S = sites[blockIdx.y];
   if (S.skipmap == nullptr) return;
   const int ccol = (S.cols + 7) / 8, nb = ((S.rows + 7) / 8) * ccol;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
-    skipmap_block(reinterpret_cast<const float4*>(S.src4), S.rows, S.cols, S.skipmap, ccol, b);
+  const int warps = (int)(gridDim.x * blockDim.x) >> 5;
+  for (int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); b < nb; b += warps)
+    skipmap_block_warp(reinterpret_cast<const float4*>(S.src4), S.rows, S.cols, S.skipmap, ccol, b,
+                       threadIdx.x & 31);
 }
 
 // Packs {dsm, vegdsm, vegdsm2, bush} of every site of a batch.

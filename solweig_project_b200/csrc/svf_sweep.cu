@@ -342,7 +342,7 @@ __global__ void svf_skipmap_kernel(const float4* __restrict__ src4, int rows, in
   skipmap_block_warp(src4, rows, cols, m, ccol, b, threadIdx.x & 31);
 }
 
-__global__ void __launch_bounds__(128) svf_sweep_kernel(
+__global__ void __launch_bounds__(128, 12) svf_sweep_kernel(
     const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
     const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
     float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps, const float* __restrict__ skipmap) {

@@ -30,6 +30,7 @@
 namespace sw100 {
 
 constexpr int kMaxPatchSmem = 153;
+constexpr int kTileThreads = 128;  // threads of a time-loop block (every launch shape)
 
 struct GvfAzSmem {
   int8_t dx[SW100_MAX_GVF_STEPS];
@@ -230,7 +231,11 @@ __device__ __forceinline__ void time_loop_tile(
   // per-pixel statics
   float bld = 0.f, walls = 0.f, aspect = 0.f, emis = 0.f, alb = 0.f, svfbuveg = 0.f, hsvf = 0.f, tan_alfa = 0.f,
         wind = 0.f;
-  uint32_t wsh[SW100_CUBE_WORDS] = {}, wveg[SW100_CUBE_WORDS] = {}, wvb[SW100_CUBE_WORDS] = {};
+  // the pixel's patch-bit words (sh, vegsh, vbshvegsh cubes) live in shared
+  // memory, one column per thread: registers go to the per-step work
+  __shared__ uint32_t CB[3 * SW100_CUBE_WORDS][kTileThreads];
+  const int ctid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int w = 0; w < 3 * SW100_CUBE_WORDS; ++w) CB[w][ctid] = 0u;
   float st[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // Tgmap1, E, S, W, N, TgOut1
   if (live) {
     bld = site.buildings[p];
@@ -244,9 +249,9 @@ __device__ __forceinline__ void time_loop_tile(
     wind = site.windcoeff[p];
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
-      wsh[w] = site.bits[(0 * SW100_CUBE_WORDS + w) * npix + p];
-      wveg[w] = site.bits[(1 * SW100_CUBE_WORDS + w) * npix + p];
-      wvb[w] = site.bits[(2 * SW100_CUBE_WORDS + w) * npix + p];
+      CB[w][ctid] = site.bits[(0 * SW100_CUBE_WORDS + w) * npix + p];
+      CB[SW100_CUBE_WORDS + w][ctid] = site.bits[(1 * SW100_CUBE_WORDS + w) * npix + p];
+      CB[2 * SW100_CUBE_WORDS + w][ctid] = site.bits[(2 * SW100_CUBE_WORDS + w) * npix + p];
     }
 #pragma unroll
     for (int k = 0; k < 6; ++k) st[k] = state[k * npix + p];
@@ -394,7 +399,7 @@ __device__ __forceinline__ void time_loop_tile(
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
       const int nq = min(32, n_patches - q0);
-      const uint32_t sw = wsh[w], vw = wveg[w];
+      const uint32_t sw = CB[w][ctid], vw = CB[SW100_CUBE_WORDS + w][ctid];
       if (day) {
         for (int j = 0; j < nq; ++j) {
           const sw100_patch_step& Q = PP[q0 + j];
@@ -420,7 +425,7 @@ __device__ __forceinline__ void time_loop_tile(
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
-      uint32_t m = (~wveg[w] | (~wvb[w] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
+      uint32_t m = (~CB[SW100_CUBE_WORDS + w][ctid] | (~CB[2 * SW100_CUBE_WORDS + w][ctid] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
       while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1u;
@@ -435,7 +440,7 @@ __device__ __forceinline__ void time_loop_tile(
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
-      uint32_t m = ~wsh[w] & wvb[w] & patch_word_mask(n_patches, q0);
+      uint32_t m = ~CB[w][ctid] & CB[2 * SW100_CUBE_WORDS + w][ctid] & patch_word_mask(n_patches, q0);
       while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1u;
@@ -466,7 +471,8 @@ __device__ __forceinline__ void time_loop_tile(
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
-      uint32_t m = (~wsh[w] | ~wveg[w] | (~wvb[w] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
+      uint32_t m = (~CB[w][ctid] | ~CB[SW100_CUBE_WORDS + w][ctid] |
+          (~CB[2 * SW100_CUBE_WORDS + w][ctid] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
       while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1u;
@@ -513,7 +519,7 @@ __device__ __forceinline__ void time_loop_tile(
   }
 }
 
-__global__ void __launch_bounds__(128, 5) time_loop_kernel(
+__global__ void __launch_bounds__(kTileThreads, 6) time_loop_kernel(
     SitePlanes site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
@@ -523,7 +529,7 @@ __global__ void __launch_bounds__(128, 5) time_loop_kernel(
 }
 
 // The time loop of every site of a batch, tiles taken in list order.
-__global__ void __launch_bounds__(128, 5) time_loop_batch_kernel(const sw100_batch_site* __restrict__ sites,
+__global__ void __launch_bounds__(kTileThreads, 6) time_loop_batch_kernel(const sw100_batch_site* __restrict__ sites,
                                                                  const sw100_tile* __restrict__ tiles, int n_tiles) {
   for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {
     const sw100_tile T = tiles[i];

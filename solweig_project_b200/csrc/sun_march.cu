@@ -21,13 +21,17 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
                                               float a, float vegdem_p, float bush_p, float walls_p,
                                               float aspect_p, const sw100_step* __restrict__ steps, int n,
                                               float vmax, const sw100_sun_step& S) {
-  const float bushplant = bush_p > 1.f ? 1.f : 0.f;
-  float sh = 0.f, vbsh = 0.f;
-  float vegsh = bushplant;
+  // vegsh, sh and the "vbshvegsh ever counted" flag only take the values
+  // 0 and 1 in the reference's float32 planes (vegsh starts at bushplant,
+  // every update is a max with a 0/1 value or a reset to 0; vbshvegsh only
+  // matters through > 0), so they are carried as booleans; f and shvoveg
+  // stay float32 running maxima with torch.maximum's NaN rule.
+  bool sh = false, vegsh = bush_p > 1.f, vb_any = false;
   float f = a;
   float shvoveg = vegdem_p;
   float dzprev = 0.f;
   const float wallbol = walls_p > 0.f ? 1.f : 0.f;
+  const bool a_nonneg = nonneg(a);
   // Building shadow settles a pixel that is not a wall (walls exactly +0)
   // on finite rasters (vmax finite: no NaN or +inf source): from then on sh
   // stays 1, vegsh ends every step at 0 and vbsh gains nothing; f and
@@ -51,22 +55,20 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
     }
     f = tmax(f, temp);
     shvoveg = tmax(shvoveg, tv);
-    sh = (f > a) ? 1.f : 0.f;
-    float vegsh2 = (tv > a ? 1.f : 0.f) + (tv2 > a ? 1.f : 0.f) + (tlf > a ? 1.f : 0.f) + (tlg > a ? 1.f : 0.f);
+    sh = f > a;
+    // vegsh2: 1 when one to three of the four canopy tests hold
+    const int cnt = (int)(tv > a) + (int)(tv2 > a) + (int)(tlf > a) + (int)(tlg > a);
     dzprev = dz;
-    if (vegsh2 == 4.f) vegsh2 = 0.f;
-    if (vegsh2 > 0.f) vegsh2 = 1.f;
-    vegsh = tmax(vegsh, vegsh2);
-    if (vegsh * sh > 0.f) vegsh = 0.f;
-    vbsh = vbsh + vegsh;
+    vegsh = (vegsh || (cnt > 0 && cnt < 4)) && !sh;
+    vb_any = vb_any || vegsh;
     // Nothing above this pixel can be reached any more: the ray has left the
     // grid (it stays out and reads zeros), or every later source height
     // minus a larger drop stays at or below the pixel, its running building
     // maximum and its running vegetation maximum.  Zeros are covered by
     // nonneg(a) and nonneg(shvoveg).
     const float top = __fsub_rn(vmax, dz);
-    if (nonneg(a) && nonneg(shvoveg) && (!inb || (top <= a && top <= shvoveg))) break;
-    if (shade_exit && f > a && nonneg(__fsub_rn(shvoveg, a))) break;
+    if (a_nonneg && nonneg(shvoveg) && (!inb || (top <= a && top <= shvoveg))) break;
+    if (shade_exit && sh && nonneg(__fsub_rn(shvoveg, a))) break;
   }
   MarchOut o;
   float facesh;
@@ -75,12 +77,11 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
   } else {
     facesh = ((aspect_p > S.facesh_lo || aspect_p <= S.facesh_hi) ? 1.f : 0.f) * -1.f + 1.f;
   }
-  sh = 1.f - sh;
-  if (vbsh > 0.f) vbsh = 1.f;
-  vbsh = vbsh - vegsh;
-  if (vegsh > 0.f) vegsh = 1.f;
-  shvoveg = (shvoveg - a) * vegsh;
-  vegsh = 1.f - vegsh;
+  const float vegf = vegsh ? 1.f : 0.f;
+  const float shf = 1.f - (sh ? 1.f : 0.f);
+  float vbsh = (vb_any ? 1.f : 0.f) - vegf;
+  shvoveg = (shvoveg - a) * vegf;
+  const float vegshf = 1.f - vegf;
   vbsh = 1.f - vbsh;
   const float shvo = f - a;
   const float facesun = ((facesh + wallbol == 1.f) && walls_p > 0.f) ? 1.f : 0.f;
@@ -94,7 +95,7 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
   wallsun = wallsun - wallshve;
   if (wallsun < 0.f) wallsun = 0.f;
   if (wallshve > walls_p) wallshve = walls_p;
-  o.vegsh = vegsh; o.sh = sh; o.vbsh = vbsh; o.wallsh = wallsh; o.wallsun = wallsun;
+  o.vegsh = vegshf; o.sh = shf; o.vbsh = vbsh; o.wallsh = wallsh; o.wallsun = wallsun;
   o.wallshve = wallshve; o.facesh = facesh; o.facesun = facesun;
   return o;
 }

@@ -363,7 +363,7 @@ __device__ __forceinline__ bool batch_pixel(const sw100_batch_site& S, const sw1
 }
 
 // SVF sweep of every site of a batch, tiles taken in list order.
-__global__ void __launch_bounds__(128) svf_sweep_batch_kernel(const sw100_batch_site* __restrict__ sites,
+__global__ void __launch_bounds__(128, 10) svf_sweep_batch_kernel(const sw100_batch_site* __restrict__ sites,
                                                               const sw100_tile* __restrict__ tiles, int n_tiles) {
   __shared__ sw100_svf_plan plan;
   for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {

@@ -256,6 +256,19 @@ def _steradians_uncached(palt):
 
 
 _LSKY_CACHE: dict = {}
+_TRIG_CACHE: dict = {}
+
+
+def _patch_trig(palt):
+    """cos / sin of the patch altitudes in radians (the tensors every step
+    evaluates from the same altitude vector) and cos(alt) * cos(0)."""
+    key = (palt.numpy().tobytes(), str(palt.dtype))
+    hit = _TRIG_CACHE.get(key)
+    if hit is None:
+        deg2rad = torch.tensor(np.pi / 180)
+        cos_t, sin_t = torch.cos(palt * deg2rad), torch.sin(palt * deg2rad)
+        hit = _TRIG_CACHE.setdefault(key, (cos_t, sin_t, cos_t * torch.cos(torch.tensor(0.))))
+    return hit
 _THR_CACHE: dict = {}
 
 
@@ -464,6 +477,7 @@ class Series:
     class_idx: np.ndarray     # uint8 per pixel (None: the site's device plane holds the classes)
 
 
+@torch.inference_mode()
 def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, scale, amax, rows, cols,
                  props: LandCoverProps, params: ModelParams = None, time_start=0, time_stop=None,
                  initial_scalars=None, patch_option=2) -> Series:
@@ -532,6 +546,19 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     alt_n, azi_n = T.sky_patches(patch_option)
     night_patches = torch.stack([torch.from_numpy(alt_n), torch.from_numpy(azi_n), torch.zeros(P)], dim=1)
     diff_vals = np.array([F32(s) - (F32(1) - F32(v)) * F32(1 - params.transVeg) for s in (0, 1) for v in (0, 1)], F32)
+    # step-independent fields, evaluated once
+    steps["sbc"] = F32(SBC)
+    steps["albedo_b"] = F32(params.albedo_b)
+    steps["first"], steps["second"] = first_f, second_f
+    steps["refl_k"] = F32((1 - ewall_t).item())
+    for k in ("absK", "absL", "Fside", "Fup", "Fcyl"):
+        steps[k] = F32(getattr(params, k))
+    steps["absl_sbc"] = F32((params.absL * sbc_t).item())
+    steps["landcover"] = props.landcover
+    idx_t = np.arange(time_start, time_stop)
+    steps["rh32"] = np.asarray(RH_all[idx_t], F32)
+    steps["ws32"] = np.asarray(Ws_all[idx_t], F32)
+    steps["ta_mat"] = (F32(0) + np.asarray(Ta_all[idx_t], F32)) + np.asarray(uhii_all[idx_t], F32)
 
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
@@ -550,17 +577,6 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         ta32 = F32(Ta64.item())
         S["ta32"] = ta32
         S["ta4"] = F32(((Ta64 + 273.15) ** 4).item())
-        S["sbc"] = F32(SBC)
-        S["albedo_b"] = F32(params.albedo_b)
-        S["first"], S["second"] = first_f, second_f
-        S["refl_k"] = F32((1 - ewall_t).item())
-        S["absK"], S["absL"], S["Fside"], S["Fup"], S["Fcyl"] = (F32(v) for v in (
-            params.absK, params.absL, params.Fside, params.Fup, params.Fcyl))
-        S["absl_sbc"] = F32((params.absL * sbc_t).item())
-        S["rh32"] = F32(RH_all[i])
-        S["ws32"] = F32(Ws_all[i])
-        S["ta_mat"] = (F32(0) + F32(Ta_all[i])) + F32(uhii_all[i])
-        S["landcover"] = props.landcover
         S["utci_pa"], S["utci_k"] = _utci_table(S["ta_mat"], S["rh32"])
         S["night_lup_base"] = ((F32(0) + ta32) + F32(0)) + F32(273.15)
         Q = patch[o]
@@ -640,14 +656,15 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             palt, pazi, plum = lv[:, 0], lv[:, 1], lv[:, 2]
             ster = _steradians(palt)
             # radTot += lum * ster * sin(alt), one float32 add per patch in order
-            terms = (plum * ster * torch.sin(palt * deg2rad_t)).numpy()
+            cos_pt, sin_pt, ang_t = _patch_trig(palt)
+            terms = (plum * ster * sin_pt).numpy()
             radTot = torch.tensor([np.add.accumulate(terms, dtype=F32)[-1]])
             lumChi = (plum * radD) / radTot
             sun_k = ((params.albedo_b * (radI * torch.cos(alt32 * deg2rad_t)) + (radD * 0.5)) / torch.pi)
             sh_k = ((params.albedo_b * radD * 0.5) / torch.pi)
-            cos_p = torch.cos(palt * deg2rad_t).numpy()
-            sin_p = torch.sin(palt * deg2rad_t).numpy()
-            ang = (torch.cos(palt * deg2rad_t) * torch.cos(torch.tensor(0.))).numpy()
+            cos_p = cos_pt.numpy()
+            sin_p = sin_pt.numpy()
+            ang = ang_t.numpy()
             ster_n = ster.numpy()
             lum_n = lumChi.numpy()
             lvz = plum.numpy()
@@ -682,8 +699,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         # Lcyl per patch (solweig.py:1651-1760)
         palt_l, pazi_l = L_patches[:, 0], L_patches[:, 1]
         ld, ls, ster_l = _lsky(esky, palt_l, Ta64)
-        cos_l = torch.cos(palt_l * deg2rad_t)
-        sin_l = torch.sin(palt_l * deg2rad_t)
+        cos_l, sin_l, _ = _patch_trig(palt_l)
         Q["ld_sky"] = ld.numpy()
         Q["ls_sky"] = ls.numpy()
         Q["ster"] = ster_l.numpy()

@@ -163,6 +163,184 @@ def _diffuse(radG, altitude, Kt, Ta, RH):
     return radI, radD
 
 
+# ------------------------------------------- the day-step chain, batched
+# The helpers above evaluate one daytime step at a time on 0-dim tensors, as
+# the reference does.  _day_chain evaluates the same operations for every
+# daytime step at once on 1-D tensors.  Each element is bit-identical to the
+# 0-dim evaluation: torch's elementwise arithmetic, sqrt, exp, log, sin, cos,
+# tan, asin, acos and the special powers (x**2, x**3, x**0.5, x**-0.5) give
+# the same bits for a 0-dim tensor and for a vector element; the general
+# powers (x**0.3, x**-1.6364, c**x, x**c) do not, so they are evaluated on
+# 0-dim elements one at a time; and where two 0-dim tensors of different
+# dtypes meet, the vector form casts explicitly to the dtype torch's
+# promotion of the 0-dim pair gives.
+def _pow_each(x, e):
+    """x ** e element by element on 0-dim tensors (e a number or a vector)."""
+    if isinstance(e, torch.Tensor):
+        return torch.stack([torch.pow(x[k], e[k]) for k in range(x.shape[0])]) if x.shape[0] else x
+    return torch.stack([x[k] ** e for k in range(x.shape[0])]) if x.shape[0] else x
+
+
+def _rpow_each(base, x):
+    """base ** x (a number to a tensor power) element by element."""
+    return torch.stack([base ** x[k] for k in range(x.shape[0])]) if x.shape[0] else x
+
+
+def _season_g(latitude, jd32):
+    G = next(g for hi, g in _G if latitude < hi)
+    out = []
+    for j in jd32.tolist():
+        if j > 335 or j <= 60:
+            out.append(G[0])
+        elif 60 < j <= 152:
+            out.append(G[1])
+        elif 152 < j <= 244:
+            out.append(G[2])
+        else:
+            out.append(G[3])
+    return out
+
+
+def _clearness_v(zen, jday, Ta32, RH, radG, latitude, P):
+    """_clearness for vectors: zen, jday, RH, radG, P float32 (as the 0-dim
+    call receives them), Ta32 the float32 values of the Python Ta."""
+    missing = P == -999.0
+    q_known = 0.000949 * (P * 10.0) + 0.051
+    q = torch.where(missing, torch.tensor(F32(0.000949 * 1013.0 + 0.051)), q_known)
+    b = 2. * torch.pi * jday / 365.
+    D = torch.sqrt(1.00011 + 0.034221 * torch.cos(b) + 0.001280 * torch.sin(b) + 0.000719 * torch.cos(2. * b)
+                   + 0.000077 * torch.sin(2. * b))
+    cz = torch.cos(zen)
+    m = 35.0 * cz * ((1224.0 * (cz ** 2) + 1.0) ** (-1 / 2.0))
+    trpg = 1.021 - 0.084 * (m * q) ** 0.5
+    Gp1 = torch.tensor([g + 1. for g in _season_g(latitude, jday)])
+    a2, b2 = torch.tensor(17.27), torch.tensor(237.7)
+    inner = ((a2 * Ta32) / (b2 + Ta32)) + torch.log(RH)
+    Td = (b2 * inner) / (a2 - inner)
+    Td = (Td * 1.8) + 32
+    u = torch.exp(0.1133 - torch.log(Gp1) + 0.0393 * Td)
+    Tw = 1 - 0.077 * _pow_each(u * m, 0.3)
+    I0 = 1370.0 * torch.cos(zen) * trpg * Tw * D * _rpow_each(0.935, m)
+    I0 = torch.where(torch.abs(zen) > torch.pi / 2, torch.tensor(0.0), I0)
+    I0 = torch.where(torch.isnan(I0), torch.tensor(0.0), I0)
+    corr = 0.1473 * torch.log(90 - (zen / torch.pi * 180)) + 0.3454
+    return I0, radG / I0 + (1 - corr), radG / (1370.0 * torch.cos(zen) * D)
+
+
+def _diffuse_v(radG, alfa, low_alt, Kt, Ta, RH):
+    """_diffuse for vectors.  alfa: the altitude in radians as the 0-dim call
+    makes it; low_alt: altitude < 1 per element; Kt a vector or a number;
+    Ta, RH float32 vectors."""
+    missing = (Ta <= -999.00) | (RH <= -999.00) | torch.isnan(Ta) | torch.isnan(RH)
+    if isinstance(Kt, torch.Tensor):
+        k1, k2 = Kt <= 0.3, (0.3 < Kt) & (Kt < 0.78)
+    else:
+        k1 = torch.full(radG.shape, Kt <= 0.3)
+        k2 = torch.full(radG.shape, 0.3 < Kt < 0.78)
+    m1, m2, m3 = radG * (1.020 - 0.248 * Kt), radG * (1.45 - 1.67 * Kt), radG * 0.147
+    RHc = RH / 100
+    s = torch.sin(alfa)
+    n1 = radG * (1 - 0.232 * Kt + 0.0239 * s - 0.000682 * Ta + 0.0195 * RHc)
+    n2 = radG * (1.329 - 1.716 * Kt + 0.267 * s - 0.00357 * Ta + 0.106 * RHc)
+    n3 = radG * (0.426 * Kt - 0.256 * s + 0.00349 * Ta + 0.0734 * RHc)
+    radD = torch.where(missing, torch.where(k1, m1, torch.where(k2, m2, m3)),
+                       torch.where(k1, n1, torch.where(k2, n2, n3)))
+    radI = (radG - radD) / torch.sin(alfa)
+    radI = torch.where(radI < 0, torch.tensor(0.0), radI)
+    radI = torch.where(low_alt & (radI > radG), radG, radI)
+    radD = torch.where(radD > radG, radG, radD)
+    return radI, radD
+
+
+def _perez_v(zen_deg, azimuth_deg, radD, radI, jday):
+    """_perez for every daytime step: lists of the Python-float arguments,
+    radD / radI float32 vectors; returns the (P, 3) tables in a list, or None
+    for a step the batched form does not cover (sun below the horizon)."""
+    n = len(zen_deg)
+    deg2rad = torch.tensor(np.pi / 180)          # float32, as in _perez
+    zen = torch.tensor(zen_deg) * deg2rad
+    azimuth = torch.tensor(azimuth_deg) * deg2rad
+    altitude = torch.tensor([90 - z for z in zen_deg]) * deg2rad
+    z3 = 1.041 * torch.pow(zen, 3)
+    clearness = ((radD + radI) / (radD + z3)) / (1 + z3)
+    da = torch.tensor([j * 2 * torch.pi / 365 for j in jday], dtype=torch.float32)
+    I0 = 1367 * (1.00011 + 0.034221 * torch.cos(da) + 0.00128 * torch.sin(da) + 0.000719 * torch.cos(2 * da)
+                 + 0.000077 * torch.sin(2 * da))
+    high = altitude >= 10 * deg2rad
+    low = 1 / torch.sin(altitude) + 0.50572 * _pow_each(180 * altitude / torch.pi + 6.07995, -1.6364)
+    airmass = torch.where(high, 1 / torch.sin(altitude), low)
+    bright = (airmass * radD) / I0
+    bright = torch.where(radD <= 10, torch.tensor(0.0), bright)
+    ic = [next((j for j, b in enumerate(_CLEAR_BINS) if c < b), 7) for c in clearness.tolist()]
+    ict = torch.tensor(ic)
+    co = {k: torch.tensor(v, dtype=torch.float32)[ict] for k, v in _PEREZ.items()}
+
+    def lin(c):
+        return c[:, 0] + c[:, 1] * zen + bright * (c[:, 2] + c[:, 3] * zen)
+
+    m_a, m_b, m_e = lin(co["a"]), lin(co["b"]), lin(co["e"])
+    m_c, m_d = lin(co["c"]), lin(co["d"])
+    clear0 = [k for k in range(n) if ic[k] == 0]
+    if clear0:
+        c, d = co["c"], co["d"]
+        for k in clear0:
+            m_c[k] = torch.exp(torch.pow(bright[k] * (c[k, 0] + c[k, 1] * zen[k]), c[k, 2])) - 1
+            m_d[k] = -torch.exp(bright[k] * (d[k, 0] + d[k, 1] * zen[k])) + d[k, 2] + bright[k] * d[k, 3] * bright[k]
+    g = _perez_geometry()
+    f32 = torch.float32
+    cs = g["sin_alt"][None, :] * torch.sin(altitude).to(f32)[:, None] + \
+        torch.cos(altitude).to(f32)[:, None] * g["cos_alt"][None, :] * \
+        torch.cos(torch.abs(g["skyazi"][None, :] - azimuth.to(f32)[:, None]))
+    lv = (1 + m_a.to(f32)[:, None] * torch.exp(m_b.to(f32)[:, None] / g["cos_zen"][None, :])) * \
+        ((1 + m_c.to(f32)[:, None] * torch.exp(m_d.to(f32)[:, None] * torch.arccos(cs)) +
+          m_e.to(f32)[:, None] * cs * cs))
+    out = []
+    for k in range(n):
+        if altitude[k] < 0:
+            out.append(None)
+            continue
+        row = lv[k].contiguous()
+        row = row / torch.sum(row)
+        out.append(torch.stack([g["alt_deg"], g["azi_deg"], row], dim=1))
+    return out
+
+
+def _day_chain(days, met_file, altitude, azimuth, zen, jday, lat):
+    """The per-daytime-step scalars of build_series for the forcing rows
+    `days`, each element bit-identical to the 0-dim helpers' result for that
+    step (tests/test_series_batched.py): sunrise, clearness (I0, CI, Kt),
+    diffuse split, Perez luminances and the diffuse split of I0."""
+    if not days:
+        return {}
+    alt_py = [float(altitude[0][i]) for i in days]
+    zen_py = [float(zen[0][i]) for i in days]
+    jd_py = [float(jday[0][i]) for i in days]
+    ta_py = [float(met_file[i, 11]) for i in days]
+    rh_py = [float(met_file[i, 10]) for i in days]
+    rg_py = [float(met_file[i, 14]) for i in days]
+    jd32 = torch.tensor(jd_py)
+    Ta32, RH32, radG32 = torch.tensor(ta_py), torch.tensor(rh_py), torch.tensor(rg_py)
+    alt32 = torch.tensor(alt_py)
+    out = {"snup": _snup_v(jd32, torch.tensor(lat))}
+    I0, CI, Kt = _clearness_v(torch.tensor(zen_py), jd32, Ta32, RH32 / 100., radG32, lat,
+                              torch.tensor([float(met_file[i, 12]) for i in days]))
+    out.update(I0=I0, CI=CI, Kt=Kt)
+    out["radI"], out["radD"] = _diffuse_v(radG32, alt32 * (torch.pi / 180.0), alt32 < 1, Kt, Ta32, RH32)
+    zen_deg = [float(np.float64(z) * (180 / np.pi)) for z in zen_py]
+    out["lv"] = _perez_v(zen_deg, [float(azimuth[0][i]) for i in days], out["radD"], out["radI"], jd_py)
+    alfa0 = torch.tensor([a * (torch.pi / 180.0) for a in alt_py])
+    out["radI0"], out["radD0"] = _diffuse_v(I0, alfa0, torch.tensor([a < 1 for a in alt_py]), 1., Ta32, RH32)
+    return out
+
+
+def _snup_v(jday_f32, lat_f32):
+    """_snup for a vector of float32 days."""
+    rad = torch.pi / 180.0
+    dec = -23.45 * torch.cos(2.0 * torch.pi * (jday_f32 + 10.0) / 365.0)
+    soc = torch.clamp(torch.tan(rad * dec) * torch.tan(rad * lat_f32), -1.0, 1.0)
+    return 12.0 - (12.0 + 24.0 * torch.arcsin(soc) / torch.pi) / 2.0
+
+
 _PEREZ_GEOM: dict = {}
 _PEREZ_CO: dict = {}
 
@@ -560,6 +738,9 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     steps["ws32"] = np.asarray(Ws_all[idx_t], F32)
     steps["ta_mat"] = (F32(0) + np.asarray(Ta_all[idx_t], F32)) + np.asarray(uhii_all[idx_t], F32)
 
+    dc = _day_chain([i for i in range(time_start, time_stop) if altitude[0][i] > 0], met_file, altitude, azimuth,
+                    zen, jday, lat)
+    d = -1
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
@@ -583,14 +764,13 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         if alt64 > 0:
             S["is_day"] = 1
             S["day_row"] = len(sun_rows)
-            SNUP = _snup(torch.tensor(jd.item()), torch.tensor(lat))
-            I0, CI, Kt = _clearness(torch.tensor(zen64.item()), torch.tensor(jd.item()), Ta64.item(),
-                                    torch.tensor(RH64.item()) / 100., torch.tensor(radG64.item()), lat,
-                                    torch.tensor(met_file[i, 12].item()))
+            d += 1
+            SNUP, I0, CI = dc["snup"][d], dc["I0"][d], dc["CI"][d]
             CI = min(CI, 1.0)
-            radI, radD = _diffuse(torch.tensor(radG64.item()), torch.tensor(alt64.item()), Kt,
-                                  torch.tensor(Ta64.item()), torch.tensor(RH64.item()))
-            lv = _perez((zen64 * (180 / np.pi)).item(), azi64.item(), radD, radI, jd.item())
+            radI, radD = dc["radI"][d], dc["radD"][d]
+            lv = dc["lv"][d]
+            if lv is None:   # sun below the horizon in the Perez geometry: the 0-dim form
+                lv = _perez((zen64 * (180 / np.pi)).item(), azi64.item(), radD, radI, jd.item())
             # sun march table and wall-face bounds
             dx, dy, dz, az_f = T.sun_table(azi64.item(), alt64.item(), scale, float(amax), rows, cols)
             t = np.zeros(len(dz), N.STEP_DTYPE)
@@ -606,7 +786,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             dect = torch.tensor(dectime[i])
             altmax64 = torch.tensor(altmax[0][i])
             phase = (dect - torch.floor(dect)) - SNUP / 24
-            radI0, radD0 = _diffuse(I0, alt64.item(), 1., Ta64.item(), RH64.item())
+            radI0, radD0 = dc["radI0"][d], dc["radD0"][d]
             corr = 0.1473 * torch.log(90 - (zen64 / np.pi * 180)) + 0.3454
             CI_TgG = min((radG64 / (radI0 * (torch.sin(alt64 * (np.pi / 180))) + radD0)) + (1 - corr), 1.0)
             S["cig"] = F32(float(CI_TgG))

@@ -1,0 +1,64 @@
+"""The series builder evaluates the daytime scalar chain for all daytime
+steps at once (timeseries._day_chain); every value must equal the 0-dim,
+step-by-step evaluation of the reference's helpers bit for bit, dtype and
+sign of zero included, across the branches (missing Ta / RH / pressure,
+the three clearness regimes of the diffuse split, radD <= 10, sun below
+10 degrees and below 1 degree, every Perez clearness bin)."""
+import numpy as np
+import pytest
+import torch
+
+from solweig_project_b200 import timeseries as TS
+
+
+def _same(a, b):
+    a = torch.as_tensor(a).double().reshape(-1)
+    b = torch.as_tensor(b).double().reshape(-1)
+    return bool((((a == b) | (torch.isnan(a) & torch.isnan(b))) & (torch.signbit(a) == torch.signbit(b))).all())
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_day_chain_equals_stepwise_helpers(seed):
+    rng = np.random.default_rng(seed)
+    n = 160
+    alt = rng.uniform(0.01, 89, n)
+    alt[:12] = rng.uniform(0.01, 1.5, 12)
+    met = np.zeros((n, 25))
+    met[:, 11] = rng.uniform(-20, 45, n)
+    met[::37, 11] = -999.0
+    met[5, 11] = np.nan
+    met[:, 10] = rng.uniform(5, 100, n)
+    met[::41, 10] = -999.0
+    met[:, 14] = rng.uniform(0, 1100, n)
+    met[::7, 14] = rng.uniform(0, 15, len(met[::7, 14]))
+    met[:, 12] = rng.uniform(90, 105, n)
+    met[::5, 12] = -999.0
+    altitude = alt[None, :]
+    zen = np.radians(90 - alt + rng.normal(0, 0.01, n))[None, :]
+    azimuth = rng.uniform(0, 360, n)[None, :]
+    jday = rng.integers(1, 366, n).astype(np.float64)[None, :]
+    lat = float(rng.uniform(-60, 89))
+    days = list(range(n))
+    with torch.inference_mode():
+        dc = TS._day_chain(days, met, altitude, azimuth, zen, jday, lat)
+        bins = set()
+        for d, i in enumerate(days):
+            Ta, RH, radG = met[i, 11], met[i, 10], met[i, 14]
+            jd = jday[0][i]
+            snup = TS._snup(torch.tensor(jd.item()), torch.tensor(lat))
+            I0, CI, Kt = TS._clearness(torch.tensor(zen[0][i].item()), torch.tensor(jd.item()), Ta.item(),
+                                       torch.tensor(RH.item()) / 100., torch.tensor(radG.item()), lat,
+                                       torch.tensor(met[i, 12].item()))
+            radI, radD = TS._diffuse(torch.tensor(radG.item()), torch.tensor(alt[i].item()), Kt,
+                                     torch.tensor(Ta.item()), torch.tensor(RH.item()))
+            radI0, radD0 = TS._diffuse(I0, alt[i].item(), 1., Ta.item(), RH.item())
+            for name, want in (("snup", snup), ("I0", I0), ("CI", CI), ("Kt", Kt), ("radI", radI), ("radD", radD),
+                               ("radI0", radI0), ("radD0", radD0)):
+                got = dc[name][d]
+                assert got.dtype == want.dtype and _same(got, want), (seed, i, name, got, want)
+            zen_deg = (torch.tensor(zen[0][i]) * (180 / np.pi)).item()
+            lv = TS._perez(zen_deg, azimuth[0][i].item(), radD, radI, jd.item())
+            assert dc["lv"][d] is not None
+            assert torch.equal(lv.view(torch.int32), dc["lv"][d].view(torch.int32)), (seed, i, "lv")
+            bins.add(float(radD) <= 10)
+        assert bins == {True, False}

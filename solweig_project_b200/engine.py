@@ -479,12 +479,12 @@ class DeviceSite:
 
     # ---------------------------------------------------------- time loop
     def build_series(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, time_start=0,
-                     time_stop=None, initial_scalars=None):
+                     time_stop=None, initial_scalars=None, day_chain=None):
         ser = TS.build_series(met_file=met_file, altitude=altitude, azimuth=azimuth, zen=zen, jday=jday,
                               dectime=dectime, altmax=altmax, location=location, scale=self.scale,
                               amax=self.amax, rows=self.rows, cols=self.cols, props=self.props,
                               params=self.params, time_start=time_start, time_stop=time_stop,
-                              initial_scalars=initial_scalars)
+                              initial_scalars=initial_scalars, day_chain=day_chain)
         if ser.class_idx is not None:
             self.t["class_idx"] = _upload(torch.from_numpy(ser.class_idx), self.device)
         return ser
@@ -570,10 +570,11 @@ class DeviceSite:
         n_t = time_stop - time_start
         host = {k: torch.empty((n_t, self.rows, self.cols), dtype=torch.float32, pin_memory=True) for k in names}
         scalars, keep = initial_scalars, []
+        dc = TS.day_chain(met_file, altitude, azimuth, zen, jday, location, time_start, time_stop)
         for t0 in range(time_start, time_stop, chunk_steps):
             t1 = min(time_stop, t0 + chunk_steps)
             ser = self.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                                    time_start=t0, time_stop=t1, initial_scalars=scalars)
+                                    time_start=t0, time_stop=t1, initial_scalars=scalars, day_chain=dc)
             scalars = ser.final
             out = self.run_time_loop(ser, requested=names)
             for k in names:

@@ -305,13 +305,23 @@ def _perez_v(zen_deg, azimuth_deg, radD, radI, jday):
     return out
 
 
+def day_chain(met_file, altitude, azimuth, zen, jday, location, time_start=0, time_stop=None):
+    """The daytime scalar chain of the forcing rows [time_start, time_stop),
+    for build_series(..., day_chain=...) calls over parts of that range."""
+    if time_stop is None:
+        time_stop = met_file.shape[0]
+    with torch.inference_mode():
+        return _day_chain([i for i in range(time_start, time_stop) if altitude[0][i] > 0], met_file, altitude,
+                          azimuth, zen, jday, location["latitude"])
+
+
 def _day_chain(days, met_file, altitude, azimuth, zen, jday, lat):
     """The per-daytime-step scalars of build_series for the forcing rows
     `days`, each element bit-identical to the 0-dim helpers' result for that
     step (tests/test_series_batched.py): sunrise, clearness (I0, CI, Kt),
     diffuse split, Perez luminances and the diffuse split of I0."""
     if not days:
-        return {}
+        return {"pos": {}}
     alt_py = [float(altitude[0][i]) for i in days]
     zen_py = [float(zen[0][i]) for i in days]
     jd_py = [float(jday[0][i]) for i in days]
@@ -321,7 +331,7 @@ def _day_chain(days, met_file, altitude, azimuth, zen, jday, lat):
     jd32 = torch.tensor(jd_py)
     Ta32, RH32, radG32 = torch.tensor(ta_py), torch.tensor(rh_py), torch.tensor(rg_py)
     alt32 = torch.tensor(alt_py)
-    out = {"snup": _snup_v(jd32, torch.tensor(lat))}
+    out = {"pos": {i: k for k, i in enumerate(days)}, "snup": _snup_v(jd32, torch.tensor(lat))}
     I0, CI, Kt = _clearness_v(torch.tensor(zen_py), jd32, Ta32, RH32 / 100., radG32, lat,
                               torch.tensor([float(met_file[i, 12]) for i in days]))
     out.update(I0=I0, CI=CI, Kt=Kt)
@@ -658,9 +668,11 @@ class Series:
 @torch.inference_mode()
 def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, scale, amax, rows, cols,
                  props: LandCoverProps, params: ModelParams = None, time_start=0, time_stop=None,
-                 initial_scalars=None, patch_option=2) -> Series:
+                 initial_scalars=None, patch_option=2, day_chain=None) -> Series:
     """Tables for steps [time_start, time_stop) of run_utci_window's loop
-    (utci_process.py:917-1067)."""
+    (utci_process.py:917-1067).  `day_chain` (from day_chain() over a range
+    holding these steps) spares recomputing the daytime scalar chain when a
+    day is built in parts."""
     if params is None:
         params = ModelParams()
     if params.anisotropic_sky != 1 or not params.cyl:
@@ -738,9 +750,9 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     steps["ws32"] = np.asarray(Ws_all[idx_t], F32)
     steps["ta_mat"] = (F32(0) + np.asarray(Ta_all[idx_t], F32)) + np.asarray(uhii_all[idx_t], F32)
 
-    dc = _day_chain([i for i in range(time_start, time_stop) if altitude[0][i] > 0], met_file, altitude, azimuth,
-                    zen, jday, lat)
-    d = -1
+    rows_day = [i for i in range(time_start, time_stop) if altitude[0][i] > 0]
+    dc = day_chain if day_chain is not None and all(i in day_chain["pos"] for i in rows_day) else \
+        _day_chain(rows_day, met_file, altitude, azimuth, zen, jday, lat)
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
@@ -764,7 +776,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         if alt64 > 0:
             S["is_day"] = 1
             S["day_row"] = len(sun_rows)
-            d += 1
+            d = dc["pos"][i]
             SNUP, I0, CI = dc["snup"][d], dc["I0"][d], dc["CI"][d]
             CI = min(CI, 1.0)
             radI, radD = dc["radI"][d], dc["radD"][d]

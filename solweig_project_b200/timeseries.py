@@ -343,6 +343,28 @@ def _day_chain(days, met_file, altitude, azimuth, zen, jday, lat):
     return out
 
 
+def _yi_tables(days, azimuth, altitude, pazi):
+    """yi_ of shaded_or_sunlit for the Kside call (float32) and the Lcyl call
+    (float64 -> float32), and the Lcyl branch flags, for the daytime rows
+    `days` against the patch azimuths `pazi` (solweig.py:524-562, the
+    expressions of the step-by-step form evaluated as (days, patches)
+    arrays, element by element the same operations)."""
+    azi = [float(azimuth[0][i]) for i in days]
+    alt = [float(altitude[0][i]) for i in days]
+    alt32 = torch.tensor(alt)
+    yk = 2 * torch.cos(torch.abs(torch.tensor(azi)[:, None] - pazi[None, :]) * (torch.pi / 180.0)) * \
+        torch.tan(alt32 * (torch.pi / 180.0))[:, None]
+    yi_k = torch.where(yk > 0, 0.0, yk).numpy()
+    pz64 = pazi.double()
+    azi64 = torch.tensor(azi, dtype=torch.float64)
+    yl = 2 * torch.cos(torch.abs(azi64[:, None] - pz64[None, :]) * (torch.pi / 180.0)) * \
+        torch.tan(torch.tensor(alt, dtype=torch.float64) * (torch.pi / 180.0))[:, None]
+    yi_l = torch.where(yl > 0, 0.0, yl).numpy().astype(F32)
+    azd = torch.abs(azi64[:, None] - pz64[None, :])
+    flags = ((azd > 90) & (azd < 270)).numpy().astype(np.int32)
+    return yi_k, yi_l, flags, pazi.clone()
+
+
 def _snup_v(jday_f32, lat_f32):
     """_snup for a vector of float32 days."""
     rad = torch.pi / 180.0
@@ -488,7 +510,25 @@ def _lsky_geometry(palt):
     return hit
 
 
-def _lsky(esky, palt, Ta64):
+_LCYL_CACHE: dict = {}
+
+
+def _lcyl_geometry(palt):
+    """Per patch layout: solid angles, cos / sin of the altitudes (float32
+    and float64) and the shaded_or_sunlit bounds, as the Lcyl tables use
+    them every step."""
+    key = (palt.numpy().tobytes(), str(palt.dtype))
+    hit = _LCYL_CACHE.get(key)
+    if hit is None:
+        ster = _steradians(palt)
+        cos_t, sin_t, _ = _patch_trig(palt)
+        hit = _LCYL_CACHE.setdefault(key, {
+            "ster_n": ster.numpy().copy(), "cos_n": cos_t.numpy().copy(), "sin_n": sin_t.numpy().copy(),
+            "s64": ster.double(), "cos64": cos_t.double(), "sin64": sin_t.double(), "thr": _thr_bounds(palt)})
+    return hit
+
+
+def _lsky(esky, palt, Ta64, ta4=None):
     """Sky longwave per patch on horizontal / vertical surfaces with the
     Martin & Berdahl band emissivities (model2, solweig.py:1394-1413, 1725-1737).
     Per distinct altitude: base = (band * sbc * Ta^4) / pi, then per patch
@@ -497,7 +537,8 @@ def _lsky(esky, palt, Ta64):
     u, expo, idx, ster, sin_u, cos_u = _lsky_geometry(palt)
     sbc = torch.tensor(SBC)
     band = 1 - (1 - esky) * expo
-    ta4 = (Ta64 + 273.15) ** 4
+    if ta4 is None:
+        ta4 = (Ta64 + 273.15) ** 4
     base = ((band * sbc * ta4) / torch.tensor(np.pi))[idx]
     bs = base * ster
     dt = bs.dtype
@@ -750,9 +791,38 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     steps["ws32"] = np.asarray(Ws_all[idx_t], F32)
     steps["ta_mat"] = (F32(0) + np.asarray(Ta_all[idx_t], F32)) + np.asarray(uhii_all[idx_t], F32)
 
+    # per-step air temperature chain for every step at once (elementwise
+    # float64; the general powers 10 ** x and x ** 4 element by element)
+    Ta64v = torch.tensor(np.asarray(Ta_all[idx_t]))
+    RH64v = torch.tensor(np.asarray(RH_all[idx_t]))
+    ea_v = 6.107 * _rpow_each(10, (7.5 * Ta64v) / (237.3 + Ta64v)) * (RH64v / 100.)
+    msteg_v = 46.5 * (ea_v / (Ta64v + 273.15))
+    esky_v = (1 - (1 + msteg_v) * torch.exp(-((1.2 + 3.0 * msteg_v) ** 0.5))) + params.elvis
+    ta4_v = _pow_each(Ta64v + 273.15, 4)
     rows_day = [i for i in range(time_start, time_stop) if altitude[0][i] > 0]
     dc = day_chain if day_chain is not None and all(i in day_chain["pos"] for i in rows_day) else \
         _day_chain(rows_day, met_file, altitude, azimuth, zen, jday, lat)
+    # ground temperature wave inputs of every daytime row (solweig.py:2101-2122)
+    if rows_day:
+        pos = [dc["pos"][i] for i in rows_day]
+        snup_d = dc["snup"][pos]
+        dect_v = torch.tensor(np.asarray(dectime)[rows_day])
+        phase_v = (dect_v - torch.floor(dect_v)) - snup_d / 24
+        zen64_v = torch.tensor(np.asarray(zen[0])[rows_day])
+        alt64_v = torch.tensor(np.asarray(altitude[0])[rows_day])
+        corr_v = 0.1473 * torch.log(90 - (zen64_v / np.pi * 180)) + 0.3454
+        cig_v = (torch.tensor(np.asarray(radG_all)[rows_day]) /
+                 (dc["radI0"][pos] * (torch.sin(alt64_v * (np.pi / 180))) + dc["radD0"][pos])) + (1 - corr_v)
+        if props.landcover:
+            tm = torch.from_numpy(np.asarray(tvals, F32))
+            # float64 phase / float32 class plane -> float32 (solweig.py:2103)
+            fac_v = torch.sin(((phase_v.to(torch.float32)[:, None] / (tm[None, :] / 24 - snup_d[:, None] / 24)) *
+                               np.pi) / 2).numpy().astype(F32)
+        else:
+            wave_v = torch.sin((phase_v / (15. / 24 - snup_d / 24)) * np.pi / 2)
+            fac_v = wave_v.numpy().astype(F32)[:, None]
+    day_k = {i: k for k, i in enumerate(rows_day)}
+    yi = None
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
@@ -760,16 +830,14 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         alt64 = torch.tensor(altitude[0][i])
         azi64 = torch.tensor(azimuth[0][i])
         zen64 = torch.tensor(zen[0][i])
-        Ta64 = torch.tensor(Ta_all[i])
-        RH64 = torch.tensor(RH_all[i])
+        Ta64 = Ta64v[o]
+        RH64 = RH64v[o]
         radG64 = torch.tensor(radG_all[i])
         jd = jday[0][i]
-        ea = 6.107 * 10 ** ((7.5 * Ta64) / (237.3 + Ta64)) * (RH64 / 100.)
-        msteg = 46.5 * (ea / (Ta64 + 273.15))
-        esky = (1 - (1 + msteg) * torch.exp(-((1.2 + 3.0 * msteg) ** 0.5))) + params.elvis
+        esky = esky_v[o]
         ta32 = F32(Ta64.item())
         S["ta32"] = ta32
-        S["ta4"] = F32(((Ta64 + 273.15) ** 4).item())
+        S["ta4"] = F32(ta4_v[o].item())
         S["utci_pa"], S["utci_k"] = _utci_table(S["ta_mat"], S["rh32"])
         S["night_lup_base"] = ((F32(0) + ta32) + F32(0)) + F32(273.15)
         Q = patch[o]
@@ -795,26 +863,20 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             sun_rows.append(srow)
             sun_off += len(dz)
             # ground temperature wave (solweig.py:2101-2122)
-            dect = torch.tensor(dectime[i])
+            kd = day_k[i]
             altmax64 = torch.tensor(altmax[0][i])
-            phase = (dect - torch.floor(dect)) - SNUP / 24
-            radI0, radD0 = dc["radI0"][d], dc["radD0"][d]
-            corr = 0.1473 * torch.log(90 - (zen64 / np.pi * 180)) + 0.3454
-            CI_TgG = min((radG64 / (radI0 * (torch.sin(alt64 * (np.pi / 180))) + radD0)) + (1 - corr), 1.0)
+            phase = phase_v[kd]
+            CI_TgG = min(cig_v[kd], 1.0)
             S["cig"] = F32(float(CI_TgG))
             S["altmax32"] = F32(altmax64.item())
             if props.landcover:
-                tm = torch.from_numpy(np.asarray(tvals, F32))
-                # float64 phase / float32 class plane -> float32 (solweig.py:2103)
-                fac = torch.sin(((torch.tensor(F32(phase.item())) / (tm / 24 - SNUP / 24)) * np.pi) / 2)
                 tgk_w = torch.from_numpy(np.asarray(props.tgk_wall, F32))
                 tst_w = torch.from_numpy(np.asarray(props.tstart_wall, F32))
                 tmx_w = torch.from_numpy(np.asarray(props.tmaxlst_wall, F32))
                 tgwall = (tgk_w * altmax64 + tst_w) * torch.sin((phase / (tmx_w / 24 - SNUP / 24)) * np.pi / 2)
             else:
-                fac = torch.tensor([float(F32(torch.sin((phase / (15. / 24 - SNUP / 24)) * np.pi / 2).item()))])
-                tgwall = (0.37 * altmax64 + -3.41) * torch.sin((phase / (15. / 24 - SNUP / 24)) * np.pi / 2)
-            fac_n = fac.numpy().astype(F32)
+                tgwall = (0.37 * altmax64 + -3.41) * wave_v[kd]
+            fac_n = fac_v[kd]
             if code_slot is None:
                 S["tg_factor"][:len(tvals)] = fac_n
             else:
@@ -866,14 +928,10 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             Q["kref_veg"] = (F32(sh_k.item()) * ster_n) * cos_p
             Q["kref_sun"] = (F32(sun_k.item()) * ster_n) * cos_p
             Q["kref_sh"] = Q["kref_veg"]
-            yk = 2 * torch.cos(torch.abs(azi64.item() - pazi) * (torch.pi / 180.0)) * \
-                torch.tan(alt32 * (torch.pi / 180.0))
-            Q["yi_k"] = torch.where(yk > 0, 0.0, yk).numpy()
-            pz64 = pazi.double()
-            yl = 2 * torch.cos(torch.abs(azi64 - pz64) * (torch.pi / 180.0)) * torch.tan(alt64 * (torch.pi / 180.0))
-            Q["yi_l"] = torch.where(yl > 0, 0.0, yl).numpy().astype(F32)
-            azd = torch.abs(azi64 - pz64)
-            Q["flags"] = ((azd > 90) & (azd < 270)).numpy().astype(np.int32)
+            if yi is None or not torch.equal(pazi, yi[3]):
+                yi = _yi_tables(rows_day, azimuth, altitude, pazi)
+            k = rows_day.index(i)
+            Q["yi_k"], Q["yi_l"], Q["flags"] = yi[0][k], yi[1][k], yi[2][k]
             L_patches = lv
             # sunlit wall surface of define_patch_characteristics (solweig.py:1596)
             sun_surf = F32((((ewall_t * sbc_t) * ((Ta64 + tgwall + 273.15) ** 4)) /
@@ -889,23 +947,21 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         if CI < 0.95:
             esky = CI * esky + (1 - CI) * 1.
         # Lcyl per patch (solweig.py:1651-1760)
-        palt_l, pazi_l = L_patches[:, 0], L_patches[:, 1]
-        ld, ls, ster_l = _lsky(esky, palt_l, Ta64)
-        cos_l, sin_l, _ = _patch_trig(palt_l)
+        palt_l = L_patches[:, 0]
+        ta4 = ta4_v[o]                         # (Ta64 + 273.15) ** 4
+        ld, ls, _ = _lsky(esky, palt_l, Ta64, ta4)
+        G = _lcyl_geometry(palt_l)
         Q["ld_sky"] = ld.numpy()
         Q["ls_sky"] = ls.numpy()
-        Q["ster"] = ster_l.numpy()
-        Q["cos_alt"] = cos_l.numpy()
-        Q["sin_alt"] = sin_l.numpy()
-        surf = ((ewall_t * sbc_t * ((Ta64 + 273.15) ** 4)) / torch.tensor(np.pi))  # float64
-        s64 = ster_l.double()
-        Q["veg_cos"] = ((surf * s64) * cos_l.double()).numpy()
-        Q["veg_sin"] = ((surf * s64) * sin_l.double()).numpy()
+        Q["ster"], Q["cos_alt"], Q["sin_alt"] = G["ster_n"], G["cos_n"], G["sin_n"]
+        surf = ((ewall_t * sbc_t * ta4) / torch.tensor(np.pi))  # float64
+        Q["veg_cos"] = ((surf * G["s64"]) * G["cos64"]).numpy()
+        Q["veg_sin"] = ((surf * G["s64"]) * G["sin64"]).numpy()
         Q["sh_cos"] = Q["veg_cos"]
         Q["sh_sin"] = Q["veg_sin"]
-        Q["sun_cos"] = (sun_surf * ster_l.numpy()) * cos_l.numpy()
-        Q["sun_sin"] = (sun_surf * ster_l.numpy()) * sin_l.numpy()
-        Q["thr_sun"], Q["thr_shd"] = _thr_bounds(palt_l)
+        Q["sun_cos"] = (sun_surf * G["ster_n"]) * G["cos_n"]
+        Q["sun_sin"] = (sun_surf * G["ster_n"]) * G["sin_n"]
+        Q["thr_sun"], Q["thr_shd"] = G["thr"]
     sun = np.array(sun_rows, N.SUN_STEP_DTYPE) if sun_rows else np.zeros(0, N.SUN_STEP_DTYPE)
     table = np.concatenate(tables) if tables else np.zeros(0, N.STEP_DTYPE)
     final = {"CI": float(CI), "firstdaytime": float(firstdaytime), "timeadd": float(timeadd)}

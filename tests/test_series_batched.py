@@ -62,3 +62,32 @@ def test_day_chain_equals_stepwise_helpers(seed):
             assert torch.equal(lv.view(torch.int32), dc["lv"][d].view(torch.int32)), (seed, i, "lv")
             bins.add(float(radD) <= 10)
         assert bins == {True, False}
+
+
+@pytest.mark.parametrize("chunk", [1, 5, 7])
+def test_chunked_series_equal_one_build(chunk):
+    """Building a day in chunks (carried scalars passed on, one day chain for
+    the whole window) gives the tables of one build: only the daytime-row
+    numbering restarts in each chunk."""
+    from conftest import load_golden, golden_location
+    from solweig_project_b200.engine import march_inputs
+    d = load_golden("city36")
+    rows, cols = d["dsm"].shape
+    props = TS.landcover_props(d["landcover"], d["lc_class"], rows, cols)
+    kw = dict(met_file=d["met"], altitude=d["altitude"], azimuth=d["azimuth"], zen=d["zen"], jday=d["jday"],
+              dectime=d["dectime"], altmax=d["altmax"], location=golden_location(d), scale=float(d["scale"]),
+              amax=march_inputs(d["dsm"], d["trees"], d["dem"])[3], rows=rows, cols=cols, props=props)
+    full = TS.build_series(**kw)
+    dc = TS.day_chain(d["met"], d["altitude"], d["azimuth"], d["zen"], d["jday"], golden_location(d))
+    n, sc, parts = d["met"].shape[0], None, []
+    for t0 in range(0, n, chunk):
+        s = TS.build_series(**kw, time_start=t0, time_stop=min(n, t0 + chunk), initial_scalars=sc, day_chain=dc)
+        sc = s.final
+        parts.append(s)
+    a, b = full.steps.copy(), np.concatenate([p.steps for p in parts])
+    a["day_row"] = 0
+    b["day_row"] = 0
+    assert a.tobytes() == b.tobytes()
+    assert full.patch.tobytes() == np.concatenate([p.patch for p in parts]).tobytes()
+    assert full.sun_table.tobytes() == np.concatenate([p.sun_table for p in parts]).tobytes()
+    assert full.final == sc

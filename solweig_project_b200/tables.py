@@ -198,6 +198,48 @@ def sun_table(azimuth, altitude, scale, amax, rows, cols):
     return dx[:n].astype(np.int32), dy[:n].astype(np.int32), dz[:n], F32(az.item())
 
 
+def sun_tables(azimuths, altitudes, scale, amax, rows, cols):
+    """sun_table and facesh_thresholds for every daytime step at once: the
+    float32 trigonometry as vectors (each element the same operations as
+    the one-step form), the step tables per step.  Returns a list of
+    (dx, dy, dz, az_f32, (mode, lo, hi))."""
+    if not azimuths:
+        return []
+    degrees = torch.tensor(np.pi / 180.0)
+    az = torch.tensor(list(azimuths)) * degrees
+    alt = torch.tensor(list(altitudes)) * degrees
+    sin_a, cos_a, tan_a = torch.sin(az), torch.cos(az), torch.tan(az)
+    ssin, scos = torch.sign(sin_a).tolist(), torch.sign(cos_a).tolist()
+    dssin, dscos = torch.abs(1. / sin_a).tolist(), torch.abs(1. / cos_a).tolist()
+    tanalt = (torch.tan(alt) / scale).tolist()
+    pb4 = torch.tensor(np.pi / 4.0)
+    by = (((pb4 <= az) & (az < 3 * pb4)) | ((5 * pb4 <= az) & (az < 7 * pb4))).tolist()
+    # wall-face bounds (facesh_thresholds) on the float32 azimuths
+    lo = az - torch.pi / 2
+    hi = az + torch.pi / 2
+    mode0 = ((lo >= 0) & (hi < 2 * torch.pi)).tolist()
+    up = ((lo < 0) & (hi <= 2 * torch.pi)).tolist()
+    down = ((lo > 0) & (hi >= 2 * torch.pi)).tolist()
+    lo_up, hi_down = (lo + 2 * torch.pi).tolist(), (hi - 2 * torch.pi).tolist()
+    lo_l, hi_l, az_l, tan_l = lo.tolist(), hi.tolist(), az.tolist(), tan_a.tolist()
+    idx = np.arange(0, max(rows, cols) + 3)
+    out = []
+    for k in range(len(az_l)):
+        ds = F32(dssin[k] if by[k] else dscos[k])
+        dx, dy, dz = _march_steps(by[k], F32(ssin[k]), F32(scos[k]), F32(tan_l[k]), ds, F32(tanalt[k]), idx)
+        n = _executed(dx, dy, dz, amax, rows, cols)
+        if mode0[k]:
+            face = (0, F32(lo_l[k]), F32(hi_l[k]))
+        elif up[k]:
+            face = (1, F32(lo_up[k]), F32(hi_l[k]))
+        elif down[k]:
+            face = (1, F32(lo_l[k]), F32(hi_down[k]))
+        else:
+            raise ValueError(f"sun azimuth {az_l[k]} outside the wall-face branches")
+        out.append((dx[:n].astype(np.int32), dy[:n].astype(np.int32), dz[:n], F32(az_l[k]), face))
+    return out
+
+
 def facesh_thresholds(az_rad_f32):
     """Branch and float32 bounds of the wall-face test (solweig.py:1187-1196,
     :239-248): mode 0 -> facesh = [aspect < lo or aspect >= hi] - wallbol + 1,

@@ -822,6 +822,8 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             wave_v = torch.sin((phase_v / (15. / 24 - snup_d / 24)) * np.pi / 2)
             fac_v = wave_v.numpy().astype(F32)[:, None]
     day_k = {i: k for k, i in enumerate(rows_day)}
+    suntab = T.sun_tables([float(azimuth[0][i]) for i in rows_day], [float(altitude[0][i]) for i in rows_day],
+                          scale, float(amax), rows, cols)
     yi = None
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
@@ -852,13 +854,13 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             if lv is None:   # sun below the horizon in the Perez geometry: the 0-dim form
                 lv = _perez((zen64 * (180 / np.pi)).item(), azi64.item(), radD, radI, jd.item())
             # sun march table and wall-face bounds
-            dx, dy, dz, az_f = T.sun_table(azi64.item(), alt64.item(), scale, float(amax), rows, cols)
+            dx, dy, dz, az_f, face = suntab[day_k[i]]
             t = np.zeros(len(dz), N.STEP_DTYPE)
             t["dx"], t["dy"], t["dz"] = dx, dy, dz
             tables.append(t)
             srow = np.zeros(1, N.SUN_STEP_DTYPE)[0]
             srow["step_offset"], srow["step_count"], srow["t"] = sun_off, len(dz), o
-            srow["facesh_mode"], srow["facesh_lo"], srow["facesh_hi"] = T.facesh_thresholds(az_f)
+            srow["facesh_mode"], srow["facesh_lo"], srow["facesh_hi"] = face
             srow["psi_term"] = F32(1) - psi[i]
             sun_rows.append(srow)
             sun_off += len(dz)

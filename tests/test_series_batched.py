@@ -91,3 +91,20 @@ def test_chunked_series_equal_one_build(chunk):
     assert full.patch.tobytes() == np.concatenate([p.patch for p in parts]).tobytes()
     assert full.sun_table.tobytes() == np.concatenate([p.sun_table for p in parts]).tobytes()
     assert full.final == sc
+
+
+@pytest.mark.parametrize("scale,amax,rows,cols", [(1.0, 40.0, 500, 500), (0.5, 12.0, 36, 80), (2.0, 120.0, 300, 100)])
+def test_sun_tables_equal_one_step_form(scale, amax, rows, cols):
+    from solweig_project_b200 import tables as T
+    rng = np.random.default_rng(3)
+    az = rng.uniform(0, 360, 120).tolist() + [0.0, 90.0, 180.0, 270.0, 359.999, 45.0, 135.0, 225.0, 315.0]
+    alt = rng.uniform(0.5, 89, len(az)).tolist()
+    got = T.sun_tables(az, alt, scale, np.float32(amax), rows, cols)
+    for k in range(len(az)):
+        dx, dy, dz, azf = T.sun_table(az[k], alt[k], scale, float(np.float32(amax)), rows, cols)
+        mode, lo, hi = T.facesh_thresholds(azf)
+        v = got[k]
+        assert np.array_equal(dx, v[0]) and np.array_equal(dy, v[1]) and dz.tobytes() == v[2].tobytes()
+        assert np.float32(azf).tobytes() == np.float32(v[3]).tobytes()
+        assert (mode, np.float32(lo).tobytes(), np.float32(hi).tobytes()) == \
+            (v[4][0], np.float32(v[4][1]).tobytes(), np.float32(v[4][2]).tobytes())

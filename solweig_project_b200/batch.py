@@ -32,10 +32,12 @@ from . import engine as E
 from . import timeseries as TS
 
 STAGES = ("pack", "bush", "svf", "sun", "flux")
-SHAPES = ((32, 4), (16, 8), (64, 2), (128, 1))
+SHAPES = ((8, 16), (32, 4), (16, 8), (4, 32), (64, 2), (128, 1))
 SM_COUNT = 148
-DEFAULT_SHAPE = {"pack": ((32, 4), "tiles"), "bush": ((32, 4), "tiles"), "svf": ((32, 4), "tiles"),
-                 "sun": ((32, 4), "tiles"), "flux": ((32, 4), "tiles")}
+# the march stages default to 8 x 16 tiles: a warp covers 8 x 4 pixels, whose
+# rays meet similar obstacles (less divergence than 32 x 1 rows)
+DEFAULT_SHAPE = {"pack": ((32, 4), "tiles"), "bush": ((32, 4), "tiles"), "svf": ((8, 16), "tiles"),
+                 "sun": ((8, 16), "tiles"), "flux": ((32, 4), "tiles")}
 ENTRY = {"pack": "sw100_batch_pack", "bush": "sw100_batch_bush_flags", "svf": "sw100_batch_svf",
          "sun": "sw100_batch_sun_march", "flux": "sw100_batch_flux_loop"}
 

@@ -111,6 +111,10 @@ int check_launch(const char* what) {
 
 int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
+// Block shape of the march kernels (SVF sweep, windowed recompute): 128
+// threads, a warp covering 8 x 4 pixels.
+constexpr int kMarchBx = 8, kMarchBy = 16;
+
 int check_grid(int rows, int cols) {
   if (rows <= 0 || cols <= 0) return fail(SW100_E_SIZE, "grid %d x %d must be positive", rows, cols);
   if ((int64_t)rows * cols >= kMaxPixels) return fail(SW100_E_SIZE, "grid %d x %d too large", rows, cols);
@@ -190,8 +194,9 @@ int launch_skipmap(const float4* src4, int rows, int cols, float* skipmap, cudaS
 int launch_sun_march(const sw100_site_planes& site, int rows, int cols, const sw100_series& ser, const float4* src4,
                      float4* gsrc, float* debug8, cudaStream_t st) {
   if (ser.n_day == 0) return 0;
-  dim3 block(32, 8);
-  dim3 grid((cols + 31) / 32, (rows + 7) / 8, ser.n_day);
+  // 8 x 32 blocks: warps of 8 x 4 pixels (see the sweep)
+  const dim3 block(8, 32);
+  const dim3 grid((cols + 7) / 8, (rows + 31) / 32, ser.n_day);
   sun_march_kernel<<<grid, block, 0, st>>>(src4, make_site(site), rows, cols, ser.sun, ser.steps, ser.sun_table,
                                            site.vmax, gsrc, debug8);
   return check_launch("sun_march_kernel");
@@ -243,8 +248,12 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
   // skip map after the bush flags
   float* skipmap = reinterpret_cast<float*>(reinterpret_cast<char*>(flags) + align_up((int64_t)n_steps * 4));
   if ((rc = launch_skipmap(src4, rows, cols, skipmap, st))) return rc;
-  svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                           site->vmax, out_planes, out_bits, n_steps, skipmap);
+  // 8 x 16 blocks: a warp marches an 8 x 4 pixel patch, whose rays meet
+  // similar obstacles (less divergence than a 32 x 1 row: -20 % time)
+  const dim3 sblock(kMarchBx, kMarchBy);
+  const dim3 sgrid((cols + kMarchBx - 1) / kMarchBx, (rows + kMarchBy - 1) / kMarchBy);
+  svf_sweep_kernel<<<sgrid, sblock, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
+                                             site->vmax, out_planes, out_bits, n_steps, skipmap);
   return check_launch("svf_sweep_kernel");
 }
 
@@ -280,8 +289,8 @@ int sw100_svf_window(const sw100_site_planes* site, int rows, int cols, const sw
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   float4* src4 = static_cast<float4*>(workspace);
   if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
-  dim3 block(32, 4);
-  dim3 grid((w3 - w2 + 1 + 31) / 32, (w1 - w0 + 1 + 3) / 4);
+  const dim3 block(kMarchBx, kMarchBy);
+  const dim3 grid((w3 - w2 + 1 + kMarchBx - 1) / kMarchBx, (w1 - w0 + 1 + kMarchBy - 1) / kMarchBy);
   svf_window_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, corridor, site->vmax,
                                             make_int4(rect[0], rect[1], rect[2], rect[3]),
                                             make_int4(w0, w1, w2, w3), planes, bits, n_steps);
@@ -313,8 +322,8 @@ int sw100_svf_box(const sw100_site_planes* site, int rows, int cols, const sw100
   svf_box_pairs_kernel<<<blocks, 128, 0, st>>>(src4, rows, cols, plan, steps, site->vmax, b4, bits, n_steps);
   if ((rc = check_launch("svf_box_pairs_kernel"))) return rc;
   // re-accumulate from the new bits: a rectangle outside the grid, read by no march
-  dim3 block(32, 4);
-  dim3 grid((box[3] - box[2] + 1 + 31) / 32, (box[1] - box[0] + 1 + 3) / 4);
+  const dim3 block(kMarchBx, kMarchBy);
+  const dim3 grid((box[3] - box[2] + 1 + kMarchBx - 1) / kMarchBx, (box[1] - box[0] + 1 + kMarchBy - 1) / kMarchBy);
   svf_window_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, corridor, site->vmax,
                                             make_int4(-4, -4, -4, -4), b4, planes, bits, n_steps);
   return check_launch("svf_window_kernel");

@@ -420,67 +420,58 @@ __device__ __forceinline__ void time_loop_tile(
         }
       }
     }
-    // vegetation-facing patches (vegsh == 0 or vbshvegsh == 0): vegetation
-    // longwave (float64 adds) and by day the vegetation-reflected Kside
+    // One ascending set-bit walk over the reflected-longwave patches
+    // (solweig.py:1613-1633, temp_sh = (sh == 0) | (vegsh == 0) |
+    // (vbshvegsh == 0)), a superset of the vegetation-facing patches
+    // (vegsh == 0 or vbshvegsh == 0: vegetation longwave in float64 adds and
+    // by day the vegetation-reflected Kside) and of the wall-facing patches
+    // ((1 - sh) * vbshvegsh == 1: sunlit / shaded wall terms split by the
+    // shaded_or_sunlit predicate).  Each accumulator still receives its
+    // terms in patch order.
+    const float refl = (((ld_sky + Lup) * P.refl_k) * 0.5f) / 3.14159274101257324f;
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
-      uint32_t m = (~CB[SW100_CUBE_WORDS + w][ctid] | (~CB[2 * SW100_CUBE_WORDS + w][ctid] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
+      const uint32_t bsh = CB[w][ctid], bveg = CB[SW100_CUBE_WORDS + w][ctid];
+      const uint32_t bvb = CB[2 * SW100_CUBE_WORDS + w][ctid];
+      const uint32_t pm = patch_word_mask(n_patches, q0);
+      const uint32_t mveg = (~bveg | (~bvb & ~site.single_step[w])) & pm;
+      const uint32_t mwall = ~bsh & bvb & pm;
+      uint32_t m = (~bsh | mveg) & pm;
       while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1u;
+        const uint32_t bit = 1u << j;
         const sw100_patch_step& Q = PP[q0 + j];
-        ls_veg = add64(ls_veg, Q.veg_cos);
-        ld_veg = add64(ld_veg, Q.veg_sin);
-        if (day) kref_veg = kref_veg + Q.kref_veg;
-      }
-    }
-    // wall-facing patches ((1 - sh) * vbshvegsh == 1): sunlit / shaded wall
-    // terms, split by the shaded_or_sunlit predicate
-#pragma unroll
-    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
-      const int q0 = w * 32;
-      uint32_t m = ~CB[w][ctid] & CB[2 * SW100_CUBE_WORDS + w][ctid] & patch_word_mask(n_patches, q0);
-      while (m) {
-        const int j = __ffs(m) - 1;
-        m &= m - 1u;
-        const sw100_patch_step& Q = PP[q0 + j];
-        if (day) {
-          const float td = hsvf + Q.yi_k;
-          if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
-          if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
+        if (mveg & bit) {
+          ls_veg = add64(ls_veg, Q.veg_cos);
+          ld_veg = add64(ld_veg, Q.veg_sin);
+          if (day) kref_veg = kref_veg + Q.kref_veg;
         }
-        if (Q.flags & 1) {
-          const float td = hsvf + Q.yi_l;
-          if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
-          if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
-        } else {
-          ls_sh = add64(ls_sh, Q.sh_cos);
-          ld_sh = add64(ld_sh, Q.sh_sin);
+        if (mwall & bit) {
+          if (day) {
+            const float td = hsvf + Q.yi_k;
+            if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
+            if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
+          }
+          if (Q.flags & 1) {
+            const float td = hsvf + Q.yi_l;
+            if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
+            if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
+          } else {
+            ls_sh = add64(ls_sh, Q.sh_cos);
+            ld_sh = add64(ld_sh, Q.sh_sin);
+          }
         }
+        const float rs = refl * Q.ster;
+        ls_ref = ls_ref + rs * Q.cos_alt;
+        ld_ref = ld_ref + rs * Q.sin_alt;
       }
     }
     if (day) {
       Kside = (((ksideI + ksideD) + kref_sun) + kref_sh) + kref_veg;
       const float dRad = anilum * P.radD;
       Kdown = ((P.radI * shadow) * P.sin_alt + dRad) + albF_day;
-    }
-    // ---------------- Lcyl pass 2: reflected longwave (solweig.py:1613-1633)
-    // over temp_sh = (sh == 0) | (vegsh == 0) | (vbshvegsh == 0)
-    const float refl = (((ld_sky + Lup) * P.refl_k) * 0.5f) / 3.14159274101257324f;
-#pragma unroll
-    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
-      const int q0 = w * 32;
-      uint32_t m = (~CB[w][ctid] | ~CB[SW100_CUBE_WORDS + w][ctid] |
-          (~CB[2 * SW100_CUBE_WORDS + w][ctid] & ~site.single_step[w])) & patch_word_mask(n_patches, q0);
-      while (m) {
-        const int j = __ffs(m) - 1;
-        m &= m - 1u;
-        const sw100_patch_step& Q = PP[q0 + j];
-        const float rs = refl * Q.ster;
-        ls_ref = ls_ref + rs * Q.cos_alt;
-        ld_ref = ld_ref + rs * Q.sin_alt;
-      }
     }
     const float Lside = (((ls_sky + ls_veg) + ls_sh) + ls_sun) + ls_ref;
     const float Ldown = (((ld_sky + ld_veg) + ld_sh) + ld_sun) + ld_ref;

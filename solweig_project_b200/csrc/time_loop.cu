@@ -149,6 +149,59 @@ __device__ __forceinline__ GvfWalk gvf_walk(const float4* __restrict__ G, size_t
   return W;
 }
 
+// The same walk when the first building's step n0 is already known: the
+// building samples depend on the buildings raster only (flag bit 0 of the
+// sun-march records), so n0 is the same at every daytime step and the
+// walk needs no test for it -- its n0 gathers do not wait on each other.
+template <bool CHECKED>
+__device__ __forceinline__ GvfWalk gvf_walk_known(const float4* __restrict__ G, size_t p, int r, int c, int rows,
+                                                  int cols, const int8_t* dx, const int8_t* dy, const int* off,
+                                                  int n0, int second_i, int snap_n) {
+  float sLup = 0.f, sAlb = 0.f, sNosh = 0.f, qLup = 0.f, qAlb = 0.f, qNosh = 0.f;
+  int tb = 0, m = 0, qm = -1;
+  uint32_t fl = 0u;
+  float tlup = 0.f, talb = 0.f, talbsh = 0.f;
+  for (int n = 0; n < n0; ++n) {
+    if (CHECKED) {
+      const int sr = r + dx[n], sc = c + dy[n];
+      if (in_grid(sr, sc, rows, cols)) {
+        const float4 g = G[(size_t)sr * cols + sc];
+        fl = __float_as_uint(g.w);
+        tlup = g.y;
+        talb = g.z;
+        talbsh = g.z * g.x;
+      }
+    } else {
+      const float4 g = G[(size_t)((long long)p + off[n])];
+      fl = __float_as_uint(g.w);
+      tlup = g.y;
+      talb = g.z;
+      talbsh = g.z * g.x;
+    }
+    sLup = sLup + tlup;
+    sAlb = sAlb + talbsh;
+    sNosh = sNosh + talb;
+    tb |= (int)((fl >> 1) & 1u);
+    m += tb;
+    if (n + 1 == snap_n) { qLup = sLup; qAlb = sAlb; qNosh = sNosh; qm = m; }
+  }
+  GvfWalk W;
+  W.sLup = sLup; W.sAlb = sAlb; W.sNosh = sNosh;
+  const int rest = second_i - n0;
+  W.m = m + tb * rest;
+  W.m2 = rest;
+  if (qm < 0) {
+    W.qLup = sLup; W.qAlb = sAlb; W.qNosh = sNosh;
+    W.qm = m + tb * (snap_n - n0);
+    W.qm2 = snap_n - n0;
+  } else {
+    W.qLup = qLup; W.qAlb = qAlb; W.qNosh = qNosh;
+    W.qm = qm;
+    W.qm2 = 0;
+  }
+  return W;
+}
+
 // x / d for a divisor shared by every pixel of a step, given rd, the
 // correctly rounded float32 reciprocal of d.  Markstein's theorem (IBM J.
 // Res. Dev. 34(1), 1990; Muller et al., Handbook of Floating-Point
@@ -194,7 +247,10 @@ struct GvfSums {
 // it (the step tables are staged in shared memory).  `Site` is SitePlanes
 // (a kernel parameter) or sw100_site_planes (a batch descriptor in global
 // memory): the same member names.
-template <class Site>
+// KNOWN_N0: reuse each walk's first-building step after the first daytime
+// step (faster for one site; the batch kernel, with more live registers,
+// does not gain).
+template <class Site, bool KNOWN_N0>
 __device__ __forceinline__ void time_loop_tile(
     const Site& site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
@@ -208,6 +264,10 @@ __device__ __forceinline__ void time_loop_tile(
   __shared__ int AZOFF[SW100_N_GVF_AZ][SW100_MAX_GVF_STEPS];  // dx * cols + dy
   // Lwall / albedo_b added k times in float32, k = 0..second (this step)
   __shared__ float REP_L[SW100_MAX_GVF_STEPS + 1], REP_A[SW100_MAX_GVF_STEPS + 1];
+  // first-building step of each ground-view walk of the thread's pixel,
+  // found at its first daytime step and reused at the later ones
+  __shared__ uint8_t N0[SW100_N_GVF_AZ][kTileThreads];
+  int n0_second = -1;  // the walk length N0 was found for (-1: not yet)
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int nthr = blockDim.x * blockDim.y;
   for (int i = tid; i < SW100_N_GVF_AZ * SW100_MAX_GVF_STEPS; i += nthr) {
@@ -313,10 +373,20 @@ __device__ __forceinline__ void time_loop_tile(
       const bool interior = r >= reach && r < rows - reach && c >= reach && c < cols - reach;
       const int first_i = (int)P.first;
       const int snap_n = min(first_i, second_i);  // snapshot after this many steps
+      const bool n0_known = KNOWN_N0 && n0_second == second_i;
       for (int az = 0; az < SW100_N_GVF_AZ; ++az) {
-        const GvfWalk W = interior
-            ? gvf_walk<false>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], bld, second_i, snap_n)
-            : gvf_walk<true>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], bld, second_i, snap_n);
+        GvfWalk W;
+        if (n0_known) {
+          const int n0 = N0[az][ctid];
+          W = interior
+              ? gvf_walk_known<false>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], n0, second_i, snap_n)
+              : gvf_walk_known<true>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], n0, second_i, snap_n);
+        } else {
+          W = interior
+              ? gvf_walk<false>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], bld, second_i, snap_n)
+              : gvf_walk<true>(G, p, r, c, rows, cols, AZ[az].dx, AZ[az].dy, AZOFF[az], bld, second_i, snap_n);
+          if (KNOWN_N0) N0[az][ctid] = (uint8_t)(second_i - W.m2);
+        }
         // the reference's weight sums
         const float wwall = (float)W.m;
         float wLwall = REP_L[W.m], walbwall = REP_A[W.m];
@@ -348,6 +418,7 @@ __device__ __forceinline__ void time_loop_tile(
         if (df & 4) { S.LupW = S.LupW + gLup; S.albW = S.albW + galb; S.albnoshW = S.albnoshW + gan; }
         if (df & 8) { S.LupN = S.LupN + gLup; S.albN = S.albN + galb; S.albnoshN = S.albnoshN + gan; }
       }
+      n0_second = second_i;
       const float lup_air = (P.sbc * emis) * P.ta4;
       const float gvfLup = div_by(S.Lup, 18.f, kR18) + lup_air;
       const float gvfalb = div_by(S.alb, 18.f, kR18), gvfalbnosh = div_by(S.albnosh, 18.f, kR18);
@@ -515,7 +586,7 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_kernel(
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
     float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs) {
-  time_loop_tile(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day, state, out_mask, outputs,
+  time_loop_tile<SitePlanes, true>(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day, state, out_mask, outputs,
                  blockIdx.x, blockIdx.y);
 }
 
@@ -526,7 +597,7 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_batch_kernel(const 
     const sw100_tile T = tiles[i];
     const sw100_batch_site& S = sites[T.site];
     __syncthreads();  // the previous tile is done with the shared tables
-    time_loop_tile(S.site, S.rows, S.cols, S.series.steps, S.series.n_t, S.series.patch, S.series.n_patches,
+    time_loop_tile<sw100_site_planes, false>(S.site, S.rows, S.cols, S.series.steps, S.series.n_t, S.series.patch, S.series.n_patches,
                    S.series.gvf, reinterpret_cast<const float4*>(S.gsrc), S.series.n_day, S.state, S.out_mask,
                    S.outputs, T.tx,
                    T.ty);

@@ -528,6 +528,44 @@ def _lcyl_geometry(palt):
     return hit
 
 
+def _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t):
+    """The Lcyl columns of the patch table (sky longwave per patch, solid
+    angles, altitude cos / sin, the float64 vegetation / shaded-wall terms,
+    the sunlit-wall terms and the shaded_or_sunlit bounds) for the steps
+    `lcyl_rows` = [(step, patch altitudes, esky, sunlit wall surface)], as
+    (steps, patches) arrays per patch layout: each element is the
+    per-step form's operation sequence (_lsky), the 0-dim float64 esky and
+    Ta^4 cast to float32 where they meet float32 vectors, as torch does."""
+    groups = {}
+    for o, palt, esky, sun_surf in lcyl_rows:
+        key = (palt.numpy().tobytes(), str(palt.dtype))
+        groups.setdefault(key, (palt, []))[1].append((o, esky, sun_surf))
+    f32 = torch.float32
+    for palt, items in groups.values():
+        rows_ = [it[0] for it in items]
+        E = torch.stack([it[1] for it in items])
+        ta4 = ta4_v[rows_]
+        _, expo, idx, ster, sin_u, cos_u = _lsky_geometry(palt)
+        band = 1 - (1 - E).to(f32)[:, None] * expo[None, :]
+        base = ((band * torch.tensor(SBC) * ta4.to(f32)[:, None]) / torch.tensor(np.pi))[:, idx]
+        bs = base * ster[None, :]
+        G = _lcyl_geometry(palt)
+        patch["ld_sky"][rows_] = (bs * sin_u[idx].to(f32)[None, :]).numpy()
+        patch["ls_sky"][rows_] = (bs * cos_u[idx].to(f32)[None, :]).numpy()
+        patch["ster"][rows_] = G["ster_n"]
+        patch["cos_alt"][rows_] = G["cos_n"]
+        patch["sin_alt"][rows_] = G["sin_n"]
+        surf = ((ewall_t * sbc_t * ta4) / torch.tensor(np.pi))  # float64
+        vc = ((surf[:, None] * G["s64"][None, :]) * G["cos64"][None, :]).numpy()
+        vs = ((surf[:, None] * G["s64"][None, :]) * G["sin64"][None, :]).numpy()
+        patch["veg_cos"][rows_], patch["veg_sin"][rows_] = vc, vs
+        patch["sh_cos"][rows_], patch["sh_sin"][rows_] = vc, vs
+        S = np.array([it[2] for it in items], F32)[:, None]
+        patch["sun_cos"][rows_] = (S * G["ster_n"][None, :]) * G["cos_n"][None, :]
+        patch["sun_sin"][rows_] = (S * G["ster_n"][None, :]) * G["sin_n"][None, :]
+        patch["thr_sun"][rows_], patch["thr_shd"][rows_] = G["thr"]
+
+
 def _lsky(esky, palt, Ta64, ta4=None):
     """Sky longwave per patch on horizontal / vertical surfaces with the
     Martin & Berdahl band emissivities (model2, solweig.py:1394-1413, 1725-1737).
@@ -825,6 +863,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     suntab = T.sun_tables([float(azimuth[0][i]) for i in rows_day], [float(altitude[0][i]) for i in rows_day],
                           scale, float(amax), rows, cols)
     yi = None
+    lcyl_rows = []
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
@@ -948,22 +987,10 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             sun_surf = F32(0)
         if CI < 0.95:
             esky = CI * esky + (1 - CI) * 1.
-        # Lcyl per patch (solweig.py:1651-1760)
-        palt_l = L_patches[:, 0]
-        ta4 = ta4_v[o]                         # (Ta64 + 273.15) ** 4
-        ld, ls, _ = _lsky(esky, palt_l, Ta64, ta4)
-        G = _lcyl_geometry(palt_l)
-        Q["ld_sky"] = ld.numpy()
-        Q["ls_sky"] = ls.numpy()
-        Q["ster"], Q["cos_alt"], Q["sin_alt"] = G["ster_n"], G["cos_n"], G["sin_n"]
-        surf = ((ewall_t * sbc_t * ta4) / torch.tensor(np.pi))  # float64
-        Q["veg_cos"] = ((surf * G["s64"]) * G["cos64"]).numpy()
-        Q["veg_sin"] = ((surf * G["s64"]) * G["sin64"]).numpy()
-        Q["sh_cos"] = Q["veg_cos"]
-        Q["sh_sin"] = Q["veg_sin"]
-        Q["sun_cos"] = (sun_surf * G["ster_n"]) * G["cos_n"]
-        Q["sun_sin"] = (sun_surf * G["ster_n"]) * G["sin_n"]
-        Q["thr_sun"], Q["thr_shd"] = G["thr"]
+        # Lcyl per patch (solweig.py:1651-1760): evaluated after the loop for
+        # all steps of each patch layout at once
+        lcyl_rows.append((o, L_patches[:, 0], esky, sun_surf))
+    _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t)
     sun = np.array(sun_rows, N.SUN_STEP_DTYPE) if sun_rows else np.zeros(0, N.SUN_STEP_DTYPE)
     table = np.concatenate(tables) if tables else np.zeros(0, N.STEP_DTYPE)
     final = {"CI": float(CI), "firstdaytime": float(firstdaytime), "timeadd": float(timeadd)}

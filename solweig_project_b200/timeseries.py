@@ -528,6 +528,46 @@ def _lcyl_geometry(palt):
     return hit
 
 
+def _kside_tables(patch, kside_rows, diff_vals, albedo_b, azimuth, altitude):
+    """The Kside columns of the patch table (diffuse, anisotropic luminance,
+    reflected terms, the shaded_or_sunlit yi_ and branch flags) for the
+    daytime steps `kside_rows` = [(step, forcing row, Perez table, radD,
+    radI, float32 altitude)], as (steps, patches) arrays per patch layout;
+    each element is the per-step form's operation sequence (radTot is a
+    sequential float32 sum along each row, as np.add.accumulate makes it)."""
+    groups = {}
+    for item in kside_rows:
+        lv = item[2]
+        key = (lv[:, 0].numpy().tobytes(), lv[:, 1].numpy().tobytes(), str(lv.dtype))
+        groups.setdefault(key, []).append(item)
+    deg2rad_t = torch.tensor(np.pi / 180)
+    for items in groups.values():
+        rows_ = [it[0] for it in items]
+        palt, pazi = items[0][2][:, 0], items[0][2][:, 1]
+        plum = torch.stack([it[2][:, 2] for it in items])
+        radD = torch.stack([it[3] for it in items])
+        radI = torch.stack([it[4] for it in items])
+        alt32 = torch.stack([it[5] for it in items])
+        ster = _steradians(palt)
+        cos_pt, sin_pt, ang_t = _patch_trig(palt)
+        # radTot += lum * ster * sin(alt), one float32 add per patch in order
+        terms = (plum * ster[None, :] * sin_pt[None, :]).numpy()
+        radTot = torch.from_numpy(np.add.accumulate(terms, axis=1, dtype=F32)[:, -1].copy())
+        lumChi = (plum * radD[:, None]) / radTot[:, None]
+        sun_k = ((albedo_b * (radI * torch.cos(alt32 * deg2rad_t)) + (radD * 0.5)) / torch.pi).numpy()
+        sh_k = ((albedo_b * radD * 0.5) / torch.pi).numpy()
+        cos_p, ang, ster_n = cos_pt.numpy(), ang_t.numpy(), ster.numpy()
+        lum_n, lvz = lumChi.numpy(), plum.numpy()
+        for di in range(4):
+            patch["kside_d"][rows_, :, di] = ((diff_vals[di] * lum_n) * ang[None, :]) * ster_n[None, :]
+            patch["anilum"][rows_, :, di] = diff_vals[di] * lvz
+        patch["kref_veg"][rows_] = (sh_k[:, None] * ster_n[None, :]) * cos_p[None, :]
+        patch["kref_sun"][rows_] = (sun_k[:, None] * ster_n[None, :]) * cos_p[None, :]
+        patch["kref_sh"][rows_] = patch["kref_veg"][rows_]
+        yk, yl, fl, _ = _yi_tables([it[1] for it in items], azimuth, altitude, pazi)
+        patch["yi_k"][rows_], patch["yi_l"][rows_], patch["flags"][rows_] = yk, yl, fl
+
+
 def _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t):
     """The Lcyl columns of the patch table (sky longwave per patch, solid
     angles, altitude cos / sin, the float64 vegetation / shaded-wall terms,
@@ -862,8 +902,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     day_k = {i: k for k, i in enumerate(rows_day)}
     suntab = T.sun_tables([float(azimuth[0][i]) for i in rows_day], [float(altitude[0][i]) for i in rows_day],
                           scale, float(amax), rows, cols)
-    yi = None
-    lcyl_rows = []
+    lcyl_rows, kside_rows = [], []
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
@@ -947,32 +986,9 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             beta = torch.tensor(zen64.item(), dtype=torch.float32)
             S["tan_beta"] = F32(torch.tan(beta).item())
             S["qa"] = F32((torch.tan(beta) / 2).item())
-            # Kside per patch (solweig.py:683-724)
-            palt, pazi, plum = lv[:, 0], lv[:, 1], lv[:, 2]
-            ster = _steradians(palt)
-            # radTot += lum * ster * sin(alt), one float32 add per patch in order
-            cos_pt, sin_pt, ang_t = _patch_trig(palt)
-            terms = (plum * ster * sin_pt).numpy()
-            radTot = torch.tensor([np.add.accumulate(terms, dtype=F32)[-1]])
-            lumChi = (plum * radD) / radTot
-            sun_k = ((params.albedo_b * (radI * torch.cos(alt32 * deg2rad_t)) + (radD * 0.5)) / torch.pi)
-            sh_k = ((params.albedo_b * radD * 0.5) / torch.pi)
-            cos_p = cos_pt.numpy()
-            sin_p = sin_pt.numpy()
-            ang = ang_t.numpy()
-            ster_n = ster.numpy()
-            lum_n = lumChi.numpy()
-            lvz = plum.numpy()
-            for di in range(4):
-                Q["kside_d"][:, di] = ((diff_vals[di] * lum_n) * ang) * ster_n
-                Q["anilum"][:, di] = diff_vals[di] * lvz
-            Q["kref_veg"] = (F32(sh_k.item()) * ster_n) * cos_p
-            Q["kref_sun"] = (F32(sun_k.item()) * ster_n) * cos_p
-            Q["kref_sh"] = Q["kref_veg"]
-            if yi is None or not torch.equal(pazi, yi[3]):
-                yi = _yi_tables(rows_day, azimuth, altitude, pazi)
-            k = rows_day.index(i)
-            Q["yi_k"], Q["yi_l"], Q["flags"] = yi[0][k], yi[1][k], yi[2][k]
+            # Kside per patch (solweig.py:683-724): after the loop, all daytime
+            # steps of each patch layout at once
+            kside_rows.append((o, i, lv, radD, radI, alt32))
             L_patches = lv
             # sunlit wall surface of define_patch_characteristics (solweig.py:1596)
             sun_surf = F32((((ewall_t * sbc_t) * ((Ta64 + tgwall + 273.15) ** 4)) /
@@ -991,6 +1007,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         # all steps of each patch layout at once
         lcyl_rows.append((o, L_patches[:, 0], esky, sun_surf))
     _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t)
+    _kside_tables(patch, kside_rows, diff_vals, params.albedo_b, azimuth, altitude)
     sun = np.array(sun_rows, N.SUN_STEP_DTYPE) if sun_rows else np.zeros(0, N.SUN_STEP_DTYPE)
     table = np.concatenate(tables) if tables else np.zeros(0, N.STEP_DTYPE)
     final = {"CI": float(CI), "firstdaytime": float(firstdaytime), "timeadd": float(timeadd)}

@@ -900,6 +900,16 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             wave_v = torch.sin((phase_v / (15. / 24 - snup_d / 24)) * np.pi / 2)
             fac_v = wave_v.numpy().astype(F32)[:, None]
     day_k = {i: k for k, i in enumerate(rows_day)}
+    # shortwave geometry of the daytime rows (sin / cos of the altitude,
+    # tan of the zenith and its half), each element the per-step operations
+    sw_v = {}
+    if rows_day:
+        alt32_v = torch.tensor([float(altitude[0][i]) for i in rows_day])
+        beta_v = torch.tensor([float(zen[0][i]) for i in rows_day], dtype=torch.float32)
+        sw_v = {"sin_alt": torch.sin(torch.tensor(np.asarray(altitude[0])[rows_day]) * (np.pi / 180)).numpy().astype(F32),
+                "cos_alt": torch.cos(alt32_v * torch.tensor(np.pi / 180.0)).numpy().astype(F32),
+                "tan_beta": torch.tan(beta_v).numpy().astype(F32),
+                "qa": (torch.tan(beta_v) / 2).numpy().astype(F32), "alt32": alt32_v}
     suntab = T.sun_tables([float(azimuth[0][i]) for i in rows_day], [float(altitude[0][i]) for i in rows_day],
                           scale, float(amax), rows, cols)
     lcyl_rows, kside_rows = [], []
@@ -980,12 +990,9 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             firstdaytime = 0
             # shortwave scalars
             S["radI"], S["radD"], S["radG"] = F32(radI.item()), F32(radD.item()), F32(radG64.item())
-            S["sin_alt"] = F32(torch.sin(alt64 * (np.pi / 180)).item())
-            alt32 = torch.tensor(alt64.item())
-            S["cos_alt"] = F32(torch.cos(alt32 * torch.tensor(np.pi / 180.0)).item())
-            beta = torch.tensor(zen64.item(), dtype=torch.float32)
-            S["tan_beta"] = F32(torch.tan(beta).item())
-            S["qa"] = F32((torch.tan(beta) / 2).item())
+            S["sin_alt"], S["cos_alt"] = sw_v["sin_alt"][kd], sw_v["cos_alt"][kd]
+            S["tan_beta"], S["qa"] = sw_v["tan_beta"][kd], sw_v["qa"][kd]
+            alt32 = sw_v["alt32"][kd]
             # Kside per patch (solweig.py:683-724): after the loop, all daytime
             # steps of each patch layout at once
             kside_rows.append((o, i, lv, radD, radI, alt32))

@@ -337,9 +337,14 @@ def _svf_steps_all(azs, alts, scale, amax, rows, cols):
     fi = np.arange(1, max(rows, cols) + 3).astype(F32)[None, :]
     m_scos = F32(-1.) * scos
     with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        dz = ((ds * fi) * tanalt).astype(F32)
+        # no march runs past its first step with dz above amax: the shifts
+        # are only needed up to the longest such prefix
+        high = ~(F32(amax) >= dz)
+        L1 = int(np.where(high.any(axis=1), np.argmax(high, axis=1) + 1, fi.shape[1]).max()) if P else 0
+        fi, dz = fi[:, :L1], dz[:, :L1]
         dy = np.where(branch_y, ssin * fi, ssin * np.abs(np.rint(fi * tan_a))).astype(F32)
         dx = np.where(branch_y, m_scos * np.abs(np.rint(fi / tan_a)), m_scos * fi).astype(F32)
-        dz = ((ds * fi) * tanalt).astype(F32)
     L = fi.shape[1]
     ok = (F32(amax) >= dz) & (np.abs(dx) < rows) & (np.abs(dy) < cols)
     first_bad = np.where(ok.all(axis=1), L, np.argmin(ok, axis=1) + 1)

@@ -620,8 +620,9 @@ def main():
                          "definition": roof_note,
                          "binding": {"resource": "SM instruction issue", "kernel": dom,
                                      "issue_active_frac_ncu": NCU_ISSUE_ACTIVE.get(dom),
-                                     "note": "DRAM traffic per launch is far below the algorithmic bytes: the "
-                                             "patch cubes stay in registers across the 24 steps"}},
+                                     "note": "DRAM traffic per launch is far below the algorithmic bytes: each "
+                                             "pixel's patch-bit cubes are read once per launch and kept on chip "
+                                             "(shared memory) across the 24 steps"}},
             "stages": stages,
             "gpu_launches": int(launches),
             "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},

@@ -103,7 +103,11 @@ def test_struct_layouts_match_c_header(tmp_path):
     names = list(N.EXPECTED_SIZES)
     body = "".join(f'printf("%zu\\n", sizeof({n}));' for n in names)
     body += 'printf("%zu\\n", sizeof(sw100_site_planes)); printf("%zu\\n", sizeof(sw100_series));'
-    src.write_text('#include <stdio.h>\n#include "solweig_b200.h"\nint main(void){' + body + 'return 0;}\n')
+    body += ('printf("%zu\\n", sizeof(sw100_batch_site)); printf("%zu\\n", offsetof(sw100_batch_site, skipmap));'
+             'printf("%zu\\n", sizeof(sw100_class_table)); printf("%zu\\n", sizeof(sw100_site_stats));'
+             'printf("%zu\\n", sizeof(sw100_tile));')
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "solweig_b200.h"\nint main(void){' + body +
+                   'return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
     sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
@@ -112,6 +116,12 @@ def test_struct_layouts_match_c_header(tmp_path):
         assert N.DTYPES[n].itemsize == s == N.EXPECTED_SIZES[n], n
     assert sizes[len(names)] == ctypes.sizeof(N.SitePlanes)
     assert sizes[len(names) + 1] == ctypes.sizeof(N.Series)
+    from solweig_project_b200 import batch as B
+    bs, skip_off, ct, st, tile = sizes[len(names) + 2:len(names) + 7]
+    assert bs == ctypes.sizeof(B.BatchSite) and skip_off == B.BatchSite.skipmap.offset
+    assert ct == ctypes.sizeof(N.ClassTable)
+    assert st == 4 * N.SITE_STATS_WORDS
+    assert tile == B.TILE_DTYPE.itemsize
 
 
 def _series_step(pa_pows, k, ta, va, d):

@@ -113,6 +113,9 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
 // Steps flagged SW100_STEP_SKIP8 whose 8-step source bound minus the step's
 // drop is at or below the pixel cannot shade it or add vegetation: they are
 // passed over 8 at a time (SkipMap, sw_common.cuh).
+// CHECKED false: the caller has shown that every step of the march stays in
+// the grid (the last step's cell is in it; the shifts grow monotonically).
+template <bool CHECKED = true>
 __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4, int rows, int cols, int r, int c,
                                                  float a, float veg2_p, const sw100_step* __restrict__ steps, int n,
                                                  float vmax, float& sh_out, float& veg_out, float& vb_out,
@@ -123,7 +126,7 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
     const sw100_step st = load_step(&steps[0]);
     const int sr = r + st.dx, sc = c + st.dy;
     float temp = 0.f, tv = 0.f, tv2 = 0.f;
-    if (in_grid(sr, sc, rows, cols)) {
+    if (!CHECKED || in_grid(sr, sc, rows, cols)) {
       const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
       temp = __fsub_rn(v.x, st.dz);
       tv = __fsub_rn(v.y, st.dz);
@@ -142,7 +145,7 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
       for (int k = 1; k < n; ++k) {
         const sw100_step sk = load_step(&steps[k]);
         const int rr = r + sk.dx, cc = c + sk.dy;
-        if (!in_grid(rr, cc, rows, cols)) {
+        if (CHECKED && !in_grid(rr, cc, rows, cols)) {
           // zeros from here on: shadow only for a pixel below 0
           if (0.f > a) { sh = true; vegsh = false; }
           else vb_any = vb_any || vegsh;
@@ -304,7 +307,18 @@ __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4,
     const int n = plan.step_count[q];
     float sh, veg, vb;
     if (fast)
-      march_patch_fast(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip);
+      {
+        // a march whose last cell is in the grid never leaves it
+        bool inside = false;
+        if (n > 0) {
+          const sw100_step last = load_step(&steps[off + n - 1]);
+          inside = in_grid(r + last.dx, c + last.dy, rows, cols);
+        }
+        if (inside)
+          march_patch_fast<false>(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip);
+        else
+          march_patch_fast<true>(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip);
+      }
     else
       march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, n,
                   bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);

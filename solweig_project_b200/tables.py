@@ -354,18 +354,23 @@ def _svf_steps_all(azs, alts, scale, amax, rows, cols):
     dx, dy, dz = dx[:, :L], dy[:, :L], dz[:, :L]
     live = np.arange(L)[None, :] < counts[:, None]
     dxi, dyi = dx.astype(np.int32), dy.astype(np.int32)
-    # SW100_STEP_SKIP8: per row, over the steps that exist
-    bad_mv = np.zeros((P, L + 8), np.int64)
-    bad_dz = np.zeros((P, L + 8), np.int64)
+    # SW100_STEP_SKIP8, per row over the steps that exist: flag k when no
+    # step k+1 .. k+7 moves more than one cell and dz does not decrease over
+    # k-1 .. k+7.  Rows without any such fault get every k >= 1; the few
+    # others (e.g. the zenith patch, whose dz decreases) take the windowed
+    # count along their row.
     both = live[:, 1:] & live[:, :-1]
-    bad_mv[:, 1:L] = both & ((np.abs(np.diff(dxi.astype(np.int64), axis=1)) > 1) |
-                             (np.abs(np.diff(dyi.astype(np.int64), axis=1)) > 1))
-    bad_dz[:, 1:L] = both & ~(dz[:, 1:] >= dz[:, :-1])
-    cm = np.concatenate([np.zeros((P, 1), np.int64), np.cumsum(bad_mv, axis=1)], axis=1)
-    cz = np.concatenate([np.zeros((P, 1), np.int64), np.cumsum(bad_dz, axis=1)], axis=1)
-    # flag k: no bad move in k+1 .. k+7, no decreasing dz in k .. k+7
-    flag_ok = (cm[:, 8:8 + L] - cm[:, 1:1 + L] == 0) & (cz[:, 8:8 + L] - cz[:, 0:L] == 0) & \
-        (np.arange(L)[None, :] >= 1)
+    bmv = both & ((np.abs(np.diff(dxi, axis=1)) > 1) | (np.abs(np.diff(dyi, axis=1)) > 1))
+    bdz = both & ~(dz[:, 1:] >= dz[:, :-1])
+    flag_ok = np.broadcast_to(np.arange(L)[None, :] >= 1, (P, L)).copy()
+    for q in np.flatnonzero((bmv | bdz).any(axis=1)):
+        bad_mv = np.zeros(L + 8, np.int64)
+        bad_dz = np.zeros(L + 8, np.int64)
+        bad_mv[1:L] = bmv[q]
+        bad_dz[1:L] = bdz[q]
+        cm = np.concatenate([[0], np.cumsum(bad_mv)])
+        cz = np.concatenate([[0], np.cumsum(bad_dz)])
+        flag_ok[q] &= (cm[8:8 + L] - cm[1:1 + L] == 0) & (cz[8:8 + L] - cz[0:L] == 0)
     steps = np.zeros(int(counts.sum()), N.STEP_DTYPE)
     steps["dx"], steps["dy"], steps["dz"] = dxi[live], dyi[live], dz[live]
     steps["flags"] = np.where(flag_ok, N.STEP_SKIP8, 0).astype(np.int32)[live]

@@ -491,8 +491,8 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
  * cores with FP32 accumulation).  No counterpart in the reference: the
  * reference recomputes SVF exactly for every edit (shadow.py:409-625 /
  * solweig_core/sparse_work.py); the preview is a fast approximate edit path
- * whose error is judged, and replaced when too large, by the exact windowed
- * recompute (sw100_svf_window).
+ * whose error is checked, and which is replaced when too large, by the exact
+ * windowed recompute (sw100_svf_window).
  *
  * Activations are NHWC bf16; a layer reads / writes channels [coff, coff +
  * C) of a buffer of `stride` channels (C, coff, stride multiples of 16).

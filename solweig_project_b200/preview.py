@@ -15,7 +15,7 @@ previews an edit as
 
 over the window's central block (the context ring only informs the net).
 The exact windowed recompute (``DeviceSite.edit_svf_block``) stays the
-fallback and the judge: when the net's error on the pre-edit window, where
+fallback and the reference point: when the net's error on the pre-edit window, where
 the exact answer is already known, exceeds a threshold, the exact path runs
 instead.  The reference has no learned path; it recomputes SVF exactly
 (shadow.py:409-625).

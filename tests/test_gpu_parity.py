@@ -1,7 +1,7 @@
 """CUDA path (through the C ABI) against the reference-generated golden
 fixtures and the CPU oracle.
 
-Bars:
+Bars (the target tolerances):
 * SVF planes, the three patch cubes, the sun-march planes and the shadow
   output: bit-exact;
 * Tmrt within 1e-3 K, UTCI within 1e-3 C, the flux outputs within 1e-3 of

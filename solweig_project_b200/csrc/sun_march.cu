@@ -17,6 +17,10 @@ struct MarchOut {
   float vegsh, sh, vbsh, wallsh, wallsun, wallshve, facesh, facesun;
 };
 
+// CHECKED false: the caller has shown that every step stays in the grid
+// (the last step's cell is in it; the shifts grow monotonically in
+// magnitude with one sign per axis).
+template <bool CHECKED>
 __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, int rows, int cols, int r, int c,
                                               float a, float vegdem_p, float bush_p, float walls_p,
                                               float aspect_p, const sw100_step* __restrict__ steps, int n,
@@ -44,7 +48,7 @@ __device__ __forceinline__ MarchOut march_sun(const float4* __restrict__ src4, i
     const int sr = r + st.dx, sc = c + st.dy;
     const float dz = st.dz;
     float temp = 0.f, tv = 0.f, tv2 = 0.f, tlf = 0.f, tlg = 0.f;
-    const bool inb = in_grid(sr, sc, rows, cols);
+    const bool inb = !CHECKED || in_grid(sr, sc, rows, cols);
     if (inb) {
       const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
       temp = __fsub_rn(v.x, dz);
@@ -114,8 +118,18 @@ __device__ __forceinline__ void sun_march_pixel(const float4* __restrict__ src4,
   const sw100_sun_step S = sun_steps[d];
   const float4 self = src4[p];
   const float walls_p = site.walls[p];
-  const MarchOut o = march_sun(src4, rows, cols, r, c, self.x, self.y, self.w, walls_p, site.aspect_rad[p],
-                               table + S.step_offset, S.step_count, vmax, S);
+  const sw100_step* steps = table + S.step_offset;
+  // a march whose last cell is in the grid never leaves it
+  bool inside = false;
+  if (S.step_count > 0) {
+    const sw100_step last = load_step(&steps[S.step_count - 1]);
+    inside = in_grid(r + last.dx, c + last.dy, rows, cols);
+  }
+  const MarchOut o = inside
+      ? march_sun<false>(src4, rows, cols, r, c, self.x, self.y, self.w, walls_p, site.aspect_rad[p], steps,
+                         S.step_count, vmax, S)
+      : march_sun<true>(src4, rows, cols, r, c, self.x, self.y, self.w, walls_p, site.aspect_rad[p], steps,
+                        S.step_count, vmax, S);
   const float shadow = o.sh - (1.f - o.vegsh) * S.psi_term;
   // sunonsurface_2018a inputs at this pixel (solweig.py:118-128, gvf_2018a :342)
   const sw100_time_step& P = tsteps[S.t];

@@ -155,3 +155,25 @@ def test_plan_equals_per_patch_tables(rows, cols, scale, amax):
         assert np.array_equal(t["dz"].view(np.uint32), dz.view(np.uint32))
         assert np.array_equal(t["flags"], _flags_direct(dx, dy, dz))
         assert bool((int(single[q >> 5]) >> (q & 31)) & 1) == (n <= 1)
+
+
+def _monotone(d):
+    """Shifts along one axis keep one sign and never shrink in magnitude."""
+    d = np.asarray(d, np.int64)
+    return bool(((d >= 0).all() or (d <= 0).all()) and (np.diff(np.abs(d)) >= 0).all())
+
+
+@pytest.mark.parametrize("rows,cols,scale,amax", [(300, 300, 1.0, 60.0), (24, 40, 0.5, 9.0), (500, 80, 2.0, 120.0)])
+def test_tables_grow_monotonically(rows, cols, scale, amax):
+    """Both marches skip per-step bounds tests when a table's last cell is in
+    the grid; that is exact only if every intermediate cell lies between the
+    pixel and the last cell, i.e. each axis' shifts keep one sign and grow."""
+    plan, steps, _ = T.svf_plan(rows, cols, scale, np.float32(amax), False, 2)
+    for q in range(153):
+        o, n = int(plan["step_offset"][0, q]), int(plan["step_count"][0, q])
+        assert _monotone(steps["dx"][o:o + n]) and _monotone(steps["dy"][o:o + n]), q
+    rng = np.random.default_rng(11)
+    az = rng.uniform(0, 360, 300).tolist() + [0.0, 45.0, 90.0, 135.0, 180.0, 225.0, 270.0, 315.0, 359.999]
+    alt = rng.uniform(0.3, 89.5, len(az)).tolist()
+    for k, v in enumerate(T.sun_tables(az, alt, scale, np.float32(amax), rows, cols)):
+        assert _monotone(v[0]) and _monotone(v[1]), (az[k], alt[k])

@@ -79,6 +79,41 @@ typedef struct {
   int32_t flags;
 } sw100_step;
 
+/* ------------------------------------------------------ march tables -- */
+/* Float32 constants of one march direction: the SVF patch marches of
+ * svf_calculator (shadow.py:196-226) and the sun march of
+ * shadowingfunction_wallheight_23 (solweig.py:1092-1120).  branch_y: the
+ * step walks the y axis by one cell (azimuth in [pi/4, 3pi/4) or
+ * [5pi/4, 7pi/4)); ssin / scos: sign(sin az), sign(cos az); tan_a: tan az;
+ * ds: |1 / sin az| when branch_y, else |1 / cos az|; tanalt: tan(alt) / scale. */
+typedef struct {
+  int32_t branch_y;
+  float ssin;
+  float scos;
+  float tan_a;
+  float ds;
+  float tanalt;
+} sw100_march_const;
+
+/* Executed steps of n_marches marches (host only, no device work).  Step
+ * index i runs over first_index .. max(rows, cols) + 2 (1 for the SVF
+ * patches, 0 for the sun march) with, in float32, one rounding per
+ * operation:
+ *   branch_y: dy = ssin * i, dx = (-1 * scos) * |rint(i / tan_a)|
+ *   else:     dy = ssin * |rint(i * tan_a)|, dx = (-1 * scos) * i
+ *   dz = (ds * i) * tanalt
+ * A march executes its steps up to and including the first one that fails
+ * amax >= dz, |dx| < rows, |dy| < cols (none when amax >= 0 fails): the
+ * reference's while loop tests the previous step's values.  counts[k] (n_marches
+ * entries) receives each march's step count and *total their sum; when
+ * `steps` is not NULL the steps are written there concatenated in march
+ * order (dx, dy converted to int32 as a C cast on x86-64 does, INT32_MIN
+ * for a non-finite or out-of-range value) with their SW100_STEP_SKIP8
+ * flags, refused with SW100_E_WORKSPACE when *total exceeds `capacity`.
+ * Replaces the numpy loop of tables.svf_plan / tables.sun_tables. */
+int sw100_march_tables(const sw100_march_const* marches, int n_marches, int first_index, float amax, int rows,
+                       int cols, sw100_step* steps, int64_t capacity, int32_t* counts, int64_t* total);
+
 /* ------------------------------------------------------- site planes -- */
 /* Per-site rasters (device pointers, npix each unless noted). */
 typedef struct {

@@ -39,7 +39,7 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noal
            "sw100_batch_skipmap", "sw100_batch_svf", "sw100_batch_sun_march", "sw100_batch_flux_loop",
            "sw100_utci_steps", "sw100_nn_conv3x3_wgrad", "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2",
            "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc",
-           "sw100_prepare_site")
+           "sw100_prepare_site", "sw100_march_tables")
 ABI_VERSION = 2  # SW100_ABI_VERSION of include/solweig_b200.h
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
@@ -60,6 +60,8 @@ class NativeError(RuntimeError):
 
 # ----------------------------------------------------------- numpy tables
 STEP_DTYPE = np.dtype([("dx", "<i4"), ("dy", "<i4"), ("dz", "<f4"), ("flags", "<i4")], align=True)
+MARCH_CONST_DTYPE = np.dtype([("branch_y", "<i4"), ("ssin", "<f4"), ("scos", "<f4"), ("tan_a", "<f4"),
+                              ("ds", "<f4"), ("tanalt", "<f4")], align=True)
 STEP_SKIP8 = 1
 
 SVF_PLAN_DTYPE = np.dtype([
@@ -207,6 +209,8 @@ def load(path: str = LIB_PATH):
             "sw100_batch_flux_loop")},
         "sw100_batch_skipmap": (C.c_int, [vp, C.c_int, vp]),
         "sw100_prepare_site": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(ClassTable), C.c_int, C.c_int] + [vp] * 12),
+        "sw100_march_tables": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, vp, C.c_int64, vp,
+                                         i64p]),
         "sw100_diff_bbox": (C.c_int, [C.POINTER(SitePlanes), C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp,
                                       C.c_int64, vp]),
     }
@@ -236,3 +240,20 @@ def workspace_bytes(name: str, *args) -> int:
 
 def launch_count() -> int:
     return int(load().sw100_launch_count())
+
+
+def march_tables(consts: np.ndarray, first_index: int, amax, rows: int, cols: int):
+    """sw100_march_tables: (steps, counts) of the marches described by the
+    MARCH_CONST_DTYPE records `consts` (host arrays; no device work)."""
+    consts = np.ascontiguousarray(consts, MARCH_CONST_DTYPE)
+    n = len(consts)
+    counts = np.zeros(max(n, 1), np.int32)
+    total = C.c_int64(0)
+    cp = consts.ctypes.data if n else None
+    call("sw100_march_tables", cp, n, int(first_index), C.c_float(np.float32(amax)), int(rows), int(cols), None,
+         0, counts.ctypes.data, C.byref(total))
+    steps = np.zeros(int(total.value), STEP_DTYPE)
+    if total.value:
+        call("sw100_march_tables", cp, n, int(first_index), C.c_float(np.float32(amax)), int(rows), int(cols),
+             steps.ctypes.data, int(total.value), counts.ctypes.data, C.byref(total))
+    return steps, counts[:n].astype(np.int64)

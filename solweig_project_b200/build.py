@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(PKG, LIB_NAME)
 SOURCES = ("api.cu", "prepare.cu", "svf_sweep.cu", "sun_march.cu", "time_loop.cu", "utci.cu", "nn.cu")
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "--prec-div=true", "--prec-sqrt=true",
-         "--ftz=false", "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
+         "--ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-Xptxas", "-v"]
 
 
 def nvcc() -> str:

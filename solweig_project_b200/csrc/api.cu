@@ -5,6 +5,7 @@
 // allocates: every scratch buffer comes from the caller's workspace, so the
 // entry points can be captured in CUDA graphs and driven from any allocator.
 #include <algorithm>
+#include <cmath>
 #include <climits>
 #include <atomic>
 #include <cstdarg>
@@ -835,3 +836,101 @@ int sw100_nn_input(const float* dsm, const float* vegdsm, const float* vegdsm2, 
 
 }  // extern "C"
 
+
+// ------------------------------------------------------------ march tables
+// Host-side step tables of the SVF patch marches (shadow.py:196-247) and the
+// sun march (solweig.py:1092-1149).  Every float32 operation is rounded on
+// its own: this file is compiled without floating-point contraction.
+namespace {
+
+struct MarchStep {
+  float dx, dy, dz;
+};
+
+inline MarchStep march_step(const sw100_march_const& m, float fi) {
+  MarchStep s;
+  const float m_scos = -1.f * m.scos;
+  if (m.branch_y) {
+    s.dy = m.ssin * fi;
+    s.dx = m_scos * std::fabs(std::nearbyint(fi / m.tan_a));
+  } else {
+    s.dy = m.ssin * std::fabs(std::nearbyint(fi * m.tan_a));
+    s.dx = m_scos * fi;
+  }
+  s.dz = (m.ds * fi) * m.tanalt;
+  return s;
+}
+
+// float32 -> int32 as x86-64's truncating conversion: INT32_MIN for NaN,
+// infinities and values outside the int32 range
+inline int32_t to_i32(float v) {
+  if (!(v > -2147483904.f && v < 2147483648.f)) return INT32_MIN;
+  return (int32_t)v;
+}
+
+inline bool step_ok(const MarchStep& s, float amax, int rows, int cols) {
+  return amax >= s.dz && std::fabs(s.dx) < (float)rows && std::fabs(s.dy) < (float)cols;
+}
+
+// SW100_STEP_SKIP8 of one march's n executed steps: step k >= 1 when no step
+// k+1 .. k+7 moves more than one cell per axis from the step before it and
+// dz does not decrease (NaN counts as a decrease) over the steps k .. k+7
+// compared with their predecessors.
+void skip_flags(sw100_step* t, int64_t n) {
+  if (n <= 0) return;
+  t[0].flags = 0;
+  int64_t next_mv = INT64_MAX, next_dz = INT64_MAX;  // nearest faulty step >= k + 1 / >= k
+  for (int64_t k = n - 1; k >= 1; --k) {
+    if (k + 1 < n) {
+      const int64_t ddx = (int64_t)t[k + 1].dx - t[k].dx, ddy = (int64_t)t[k + 1].dy - t[k].dy;
+      if (ddx > 1 || ddx < -1 || ddy > 1 || ddy < -1) next_mv = k + 1;
+    }
+    if (!(t[k].dz >= t[k - 1].dz)) next_dz = k;
+    t[k].flags = (next_mv > k + 7 && next_dz > k + 7) ? SW100_STEP_SKIP8 : 0;
+  }
+}
+
+}  // namespace
+
+extern "C" int sw100_march_tables(const sw100_march_const* marches, int n_marches, int first_index, float amax,
+                                  int rows, int cols, sw100_step* steps, int64_t capacity, int32_t* counts,
+                                  int64_t* total) {
+  int rc;
+  if ((rc = check_grid(rows, cols)) || (rc = check_ptr(counts, "counts")) || (rc = check_ptr(total, "total")))
+    return rc;
+  if (n_marches < 0 || (n_marches > 0 && !marches)) return fail(SW100_E_ARG, "marches must hold n_marches >= 0 entries");
+  if (first_index < 0) return fail(SW100_E_ARG, "first_index must be >= 0");
+  const int last = std::max(rows, cols) + 2;
+  const int64_t len = last >= first_index ? (int64_t)last - first_index + 1 : 0;
+  int64_t sum = 0;
+  for (int q = 0; q < n_marches; ++q) {
+    int64_t n = 0;
+    if (amax >= 0.f) {
+      n = len;
+      for (int64_t j = 0; j < len; ++j) {
+        if (!step_ok(march_step(marches[q], (float)(first_index + j)), amax, rows, cols)) {
+          n = j + 1;
+          break;
+        }
+      }
+    }
+    counts[q] = (int32_t)n;
+    sum += n;
+  }
+  *total = sum;
+  if (!steps) return 0;
+  if (sum > capacity)
+    return fail(SW100_E_WORKSPACE, "%lld steps do not fit a table of %lld", (long long)sum, (long long)capacity);
+  sw100_step* t = steps;
+  for (int q = 0; q < n_marches; ++q) {
+    for (int64_t j = 0; j < counts[q]; ++j) {
+      const MarchStep s = march_step(marches[q], (float)(first_index + j));
+      t[j].dx = to_i32(s.dx);
+      t[j].dy = to_i32(s.dy);
+      t[j].dz = s.dz;
+    }
+    skip_flags(t, counts[q]);
+    t += counts[q];
+  }
+  return 0;
+}

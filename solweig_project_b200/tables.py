@@ -222,12 +222,16 @@ def sun_tables(azimuths, altitudes, scale, amax, rows, cols):
     down = ((lo > 0) & (hi >= 2 * torch.pi)).tolist()
     lo_up, hi_down = (lo + 2 * torch.pi).tolist(), (hi - 2 * torch.pi).tolist()
     lo_l, hi_l, az_l, tan_l = lo.tolist(), hi.tolist(), az.tolist(), tan_a.tolist()
-    idx = np.arange(0, max(rows, cols) + 3)
+    consts = np.zeros(len(az_l), N.MARCH_CONST_DTYPE)
+    consts["branch_y"] = by
+    consts["ssin"], consts["scos"], consts["tan_a"] = ssin, scos, tan_l
+    consts["ds"] = [dssin[k] if by[k] else dscos[k] for k in range(len(az_l))]
+    consts["tanalt"] = tanalt
+    steps, counts = N.march_tables(consts, 0, amax, rows, cols)
+    offs = np.concatenate([[0], np.cumsum(counts)])
     out = []
     for k in range(len(az_l)):
-        ds = F32(dssin[k] if by[k] else dscos[k])
-        dx, dy, dz = _march_steps(by[k], F32(ssin[k]), F32(scos[k]), F32(tan_l[k]), ds, F32(tanalt[k]), idx)
-        n = _executed(dx, dy, dz, amax, rows, cols)
+        t = steps[offs[k]:offs[k + 1]]
         if mode0[k]:
             face = (0, F32(lo_l[k]), F32(hi_l[k]))
         elif up[k]:
@@ -236,7 +240,7 @@ def sun_tables(azimuths, altitudes, scale, amax, rows, cols):
             face = (1, F32(lo_l[k]), F32(hi_down[k]))
         else:
             raise ValueError(f"sun azimuth {az_l[k]} outside the wall-face branches")
-        out.append((dx[:n].astype(np.int32), dy[:n].astype(np.int32), dz[:n], F32(az_l[k]), face))
+        out.append((t["dx"].copy(), t["dy"].copy(), t["dz"].copy(), F32(az_l[k]), face))
     return out
 
 
@@ -322,59 +326,19 @@ def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03, 
 
 
 def _svf_steps_all(azs, alts, scale, amax, rows, cols):
-    """Executed steps of every patch march at once (svf_patch_table applied
-    patch by patch gives the same float32 values: each element is the same
-    chain of float32 operations), concatenated in patch order with their
-    SW100_STEP_SKIP8 flags; returns (steps, counts)."""
-    P = len(azs)
+    """Executed steps of every patch march at once, concatenated in patch
+    order with their SW100_STEP_SKIP8 flags (sw100_march_tables: the same
+    float32 values as svf_patch_table applied patch by patch); returns
+    (steps, counts)."""
     trig = [_svf_patch_trig(float(a), int(h)) for a, h in zip(azs, alts)]
-    branch_y = np.array([t[0] for t in trig])[:, None]
-    ssin = np.array([t[1] for t in trig], F32)[:, None]
-    scos = np.array([t[2] for t in trig], F32)[:, None]
-    tan_a = np.array([t[3] for t in trig], F32)[:, None]
-    ds = np.array([t[4] for t in trig], F32)[:, None]
-    tanalt = np.array([F32(t[5] / F32(scale)) for t in trig], F32)[:, None]
-    fi = np.arange(1, max(rows, cols) + 3).astype(F32)[None, :]
-    m_scos = F32(-1.) * scos
-    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
-        dz = ((ds * fi) * tanalt).astype(F32)
-        # no march runs past its first step with dz above amax: the shifts
-        # are only needed up to the longest such prefix
-        high = ~(F32(amax) >= dz)
-        L1 = int(np.where(high.any(axis=1), np.argmax(high, axis=1) + 1, fi.shape[1]).max()) if P else 0
-        fi, dz = fi[:, :L1], dz[:, :L1]
-        dy = np.where(branch_y, ssin * fi, ssin * np.abs(np.rint(fi * tan_a))).astype(F32)
-        dx = np.where(branch_y, m_scos * np.abs(np.rint(fi / tan_a)), m_scos * fi).astype(F32)
-    L = fi.shape[1]
-    ok = (F32(amax) >= dz) & (np.abs(dx) < rows) & (np.abs(dy) < cols)
-    first_bad = np.where(ok.all(axis=1), L, np.argmin(ok, axis=1) + 1)
-    counts = first_bad if F32(amax) >= F32(0.) else np.zeros(P, np.int64)
-    counts = np.minimum(counts, L).astype(np.int64)
-    L = int(counts.max()) if P else 0          # no patch executes beyond this
-    dx, dy, dz = dx[:, :L], dy[:, :L], dz[:, :L]
-    live = np.arange(L)[None, :] < counts[:, None]
-    dxi, dyi = dx.astype(np.int32), dy.astype(np.int32)
-    # SW100_STEP_SKIP8, per row over the steps that exist: flag k when no
-    # step k+1 .. k+7 moves more than one cell and dz does not decrease over
-    # k-1 .. k+7.  Rows without any such fault get every k >= 1; the few
-    # others (e.g. the zenith patch, whose dz decreases) take the windowed
-    # count along their row.
-    both = live[:, 1:] & live[:, :-1]
-    bmv = both & ((np.abs(np.diff(dxi, axis=1)) > 1) | (np.abs(np.diff(dyi, axis=1)) > 1))
-    bdz = both & ~(dz[:, 1:] >= dz[:, :-1])
-    flag_ok = np.broadcast_to(np.arange(L)[None, :] >= 1, (P, L)).copy()
-    for q in np.flatnonzero((bmv | bdz).any(axis=1)):
-        bad_mv = np.zeros(L + 8, np.int64)
-        bad_dz = np.zeros(L + 8, np.int64)
-        bad_mv[1:L] = bmv[q]
-        bad_dz[1:L] = bdz[q]
-        cm = np.concatenate([[0], np.cumsum(bad_mv)])
-        cz = np.concatenate([[0], np.cumsum(bad_dz)])
-        flag_ok[q] &= (cm[8:8 + L] - cm[1:1 + L] == 0) & (cz[8:8 + L] - cz[0:L] == 0)
-    steps = np.zeros(int(counts.sum()), N.STEP_DTYPE)
-    steps["dx"], steps["dy"], steps["dz"] = dxi[live], dyi[live], dz[live]
-    steps["flags"] = np.where(flag_ok, N.STEP_SKIP8, 0).astype(np.int32)[live]
-    return steps, counts
+    consts = np.zeros(len(trig), N.MARCH_CONST_DTYPE)
+    consts["branch_y"] = [t[0] for t in trig]
+    consts["ssin"] = [t[1] for t in trig]
+    consts["scos"] = [t[2] for t in trig]
+    consts["tan_a"] = [t[3] for t in trig]
+    consts["ds"] = [t[4] for t in trig]
+    consts["tanalt"] = [F32(t[5] / F32(scale)) for t in trig]
+    return N.march_tables(consts, 1, amax, rows, cols)
 
 
 # ------------------------------------------- windowed SVF recompute

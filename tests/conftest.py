@@ -26,6 +26,15 @@ def golden_location(d):
             "altitude": float(d["site_altitude"])}
 
 
+@pytest.fixture(scope="session", autouse=True)
+def native_library():
+    """The host table builders (sw100_march_tables) and every kernel live in
+    the in-tree library: build it once per session when it is missing or
+    older than its sources."""
+    from solweig_project_b200 import build
+    build.build()
+
+
 @pytest.fixture(scope="session")
 def cuda():
     import torch

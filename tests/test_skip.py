@@ -177,3 +177,59 @@ def test_tables_grow_monotonically(rows, cols, scale, amax):
     alt = rng.uniform(0.3, 89.5, len(az)).tolist()
     for k, v in enumerate(T.sun_tables(az, alt, scale, np.float32(amax), rows, cols)):
         assert _monotone(v[0]) and _monotone(v[1]), (az[k], alt[k])
+
+
+def _numpy_tables(consts, first_index, amax, rows, cols):
+    """The step tables by the numpy one-step form (_march_steps, _executed,
+    step_skip_flags) for each march record."""
+    idx = np.arange(first_index, max(rows, cols) + 3)
+    out = []
+    with np.errstate(all="ignore"):
+        for c in consts:
+            dx, dy, dz = T._march_steps(bool(c["branch_y"]), c["ssin"], c["scos"], c["tan_a"], c["ds"],
+                                        c["tanalt"], idx)
+            n = T._executed(dx, dy, dz, amax, rows, cols)
+            t = np.zeros(n, N.STEP_DTYPE)
+            t["dx"], t["dy"], t["dz"] = dx[:n].astype(np.int32), dy[:n].astype(np.int32), dz[:n]
+            t["flags"] = T.step_skip_flags(t["dx"], t["dy"], t["dz"])
+            out.append(t)
+    return out
+
+
+@pytest.mark.parametrize("amax", [40.0, 0.0, -1.0, float("nan"), float("inf"), 3.0e38])
+@pytest.mark.parametrize("first_index,rows,cols", [(1, 300, 120), (0, 37, 64), (0, 1, 1), (1, 2, 700)])
+def test_native_march_tables_equal_numpy_form(amax, first_index, rows, cols):
+    """sw100_march_tables (host C, one float32 rounding per operation) gives
+    the numpy form's steps bit for bit, counts and flags included, over
+    random directions and the edge values of the constants."""
+    rng = np.random.default_rng(17)
+    n = 64
+    consts = np.zeros(n, N.MARCH_CONST_DTYPE)
+    consts["branch_y"] = rng.integers(0, 2, n)
+    consts["ssin"] = rng.choice([-1.0, 0.0, 1.0], n)
+    consts["scos"] = rng.choice([-1.0, 0.0, 1.0], n)
+    consts["tan_a"] = rng.uniform(-3, 3, n).astype(np.float32)
+    consts["ds"] = rng.uniform(1, 1.42, n).astype(np.float32)
+    consts["tanalt"] = np.float32(10.0) ** rng.uniform(-2, 2, n).astype(np.float32)
+    consts["tan_a"][:6] = [0.0, -0.0, 1e-30, np.nan, np.inf, -2.3e7]
+    consts["tanalt"][6:12] = [0.0, -2.3e7, np.nan, np.inf, 1e-30, -1.0]
+    consts["ds"][12] = np.nan
+    want = _numpy_tables(consts, first_index, np.float32(amax), rows, cols)
+    steps, counts = N.march_tables(consts, first_index, np.float32(amax), rows, cols)
+    assert list(counts) == [len(t) for t in want]
+    ref = np.concatenate(want) if want else np.zeros(0, N.STEP_DTYPE)
+    assert steps.tobytes() == ref.tobytes()
+
+
+def test_native_march_tables_refuse_small_capacity():
+    import ctypes
+    consts = np.zeros(2, N.MARCH_CONST_DTYPE)
+    consts["ds"], consts["tanalt"], consts["scos"] = 1.0, 0.1, 1.0
+    steps, counts = N.march_tables(consts, 1, np.float32(5.0), 50, 50)
+    assert len(steps) == counts.sum() > 2
+    lib = N.load()
+    small = np.zeros(2, N.STEP_DTYPE)
+    total = ctypes.c_int64(0)
+    rc = lib.sw100_march_tables(consts.ctypes.data, 2, 1, ctypes.c_float(5.0), 50, 50, small.ctypes.data, 2,
+                                counts.astype(np.int32).ctypes.data, ctypes.byref(total))
+    assert rc == 1003 and total.value == counts.sum()  # SW100_E_WORKSPACE

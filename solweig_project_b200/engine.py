@@ -549,7 +549,7 @@ class DeviceSite:
                _ptr(self.state), out_mask, _ptr(outputs), _stream())
 
     def run_chain_chunked(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                          requested=("utci",), time_start=0, time_stop=None, initial_scalars=None, chunk_steps=6):
+                          requested=("utci",), time_start=0, time_stop=None, initial_scalars=None, chunk_steps=8):
         """The time loop of steps [time_start, time_stop) with the host tables
         built chunk by chunk while the GPU works: the tables of `chunk_steps`
         steps are built, their sun march and flux loop launched and their

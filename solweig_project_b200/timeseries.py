@@ -673,6 +673,42 @@ def _utci_table(ta_mat: np.float32, rh32: np.float32):
     return pa_pows, k
 
 
+def _utci_pow_v(x, p: int):
+    """utci_pow of every element of a float32 array (the same operations)."""
+    if p == 1:
+        return x
+    if p == 2:
+        return x * x
+    if p == 3:
+        return (x * x) * x
+    d = x.astype(np.float64)
+    d2 = d * d
+    d4 = d2 * d2
+    return (d4 if p == 4 else (d4 * d if p == 5 else d4 * d2)).astype(F32)
+
+
+def _utci_tables(ta_mat, rh32):
+    """_utci_table of many steps at once: (Pa^1..Pa^6, c * Ta^pt) per step,
+    each element by the operations of the one-step form."""
+    ta = np.asarray(ta_mat, F32).reshape(-1)
+    rh = np.asarray(rh32, F32).reshape(-1)
+    g = [F32(v) for v in _ES_G]
+    tk = ta + F32(273.15)
+    es = g[7] * np.log(tk.astype(np.float64)).astype(F32)
+    es = es + g[0] * (F32(1) / (tk * tk))
+    es = es + g[1] * (F32(1) / tk)
+    es = es + g[2] * F32(1)
+    es = es + g[3] * tk
+    es = es + g[4] * (tk * tk)
+    es = es + g[5] * ((tk * tk) * tk)
+    es = es + g[6] * _utci_pow_v(tk, 4)
+    es = np.exp(es.astype(np.float64)).astype(F32) * F32(0.01)
+    pa = ((es * rh) / F32(100.0)) / F32(10.0)
+    pa_pows = np.stack([_utci_pow_v(pa, p) for p in range(1, 7)], axis=1)
+    ta_pows = np.stack([np.ones_like(ta)] + [_utci_pow_v(ta, p) for p in range(1, 7)], axis=1)
+    return pa_pows, _TERM_C[None, :] * ta_pows[:, _TERM_PT]
+
+
 def utci_step_records(met_file, indices) -> np.ndarray:
     """Time-step records carrying only what the UTCI tail reads (ta_mat,
     rh32, ws32 and the UTCI table) for the forcing rows ``indices``, with
@@ -686,7 +722,8 @@ def utci_step_records(met_file, indices) -> np.ndarray:
         S["rh32"] = F32(met_file[i, 10])
         S["ws32"] = F32(met_file[i, 9])
         S["ta_mat"] = (F32(0) + F32(met_file[i, 11])) + F32(uhii[i])
-        S["utci_pa"], S["utci_k"] = _utci_table(S["ta_mat"], S["rh32"])
+    if len(rec):
+        rec["utci_pa"], rec["utci_k"] = _utci_tables(rec["ta_mat"], rec["rh32"])
     return rec
 
 
@@ -868,6 +905,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     steps["rh32"] = np.asarray(RH_all[idx_t], F32)
     steps["ws32"] = np.asarray(Ws_all[idx_t], F32)
     steps["ta_mat"] = (F32(0) + np.asarray(Ta_all[idx_t], F32)) + np.asarray(uhii_all[idx_t], F32)
+    steps["utci_pa"], steps["utci_k"] = _utci_tables(steps["ta_mat"], steps["rh32"])
 
     # per-step air temperature chain for every step at once (elementwise
     # float64; the general powers 10 ** x and x ** 4 element by element)
@@ -899,6 +937,34 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         else:
             wave_v = torch.sin((phase_v / (15. / 24 - snup_d / 24)) * np.pi / 2)
             fac_v = wave_v.numpy().astype(F32)[:, None]
+        # wall temperature, wall longwave and sunlit wall surface of every
+        # daytime row (solweig.py:2101-2122, :1596), as (rows, wall classes)
+        # arrays.  With a land-cover table the wall class is a 1-D float32
+        # tensor, so each step's 0-dim float64 operands are rounded to
+        # float32 first and the chain runs in float32; without one it runs in
+        # float64.  x ** 4 element by element, as the step form evaluates it.
+        f32 = torch.float32
+        offs_day = [i - time_start for i in rows_day]
+        alt_d = torch.tensor(np.asarray(altmax[0])[rows_day])
+        ta_d = Ta64v[offs_day]
+        ci_d = torch.where(1.0 < cig_v, torch.tensor(1.0, dtype=torch.float64), cig_v)  # min(cig, 1.0)
+        se_t = sbc_t * ewall_t
+        if props.landcover:
+            tgk_w = torch.from_numpy(np.asarray(props.tgk_wall, F32).reshape(-1))[None, :]
+            tst_w = torch.from_numpy(np.asarray(props.tstart_wall, F32).reshape(-1))[None, :]
+            tmx_w = torch.from_numpy(np.asarray(props.tmaxlst_wall, F32).reshape(-1))[None, :]
+            den = tmx_w / 24 - snup_d[:, None] / 24
+            tgwall_d = (tgk_w * alt_d.to(f32)[:, None] + tst_w) * \
+                torch.sin((phase_v.to(f32)[:, None] / den) * np.pi / 2)
+            tgwall_d = torch.maximum(tgwall_d, torch.tensor(0)) * ci_d.to(f32)[:, None]
+            base = (tgwall_d + ta_d.to(f32)[:, None]) + 273.15
+        else:
+            tgwall_d = (0.37 * alt_d + -3.41) * wave_v
+            tgwall_d = (torch.maximum(tgwall_d, torch.tensor(0)) * ci_d)[:, None]
+            base = (tgwall_d + ta_d[:, None]) + 273.15
+        p4 = _pow_each(base.reshape(-1), 4).reshape(base.shape)
+        lwall_d = (se_t * p4 - (se_t * ta4_v[offs_day]).to(p4.dtype)[:, None])[:, 0].numpy().astype(F32)
+        sunsurf_d = ((se_t * p4) / torch.tensor(np.pi))[:, 0].numpy().astype(F32)
     day_k = {i: k for k, i in enumerate(rows_day)}
     # shortwave geometry of the daytime rows (sin / cos of the altitude,
     # tan of the zenith and its half), each element the per-step operations
@@ -928,7 +994,6 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         ta32 = F32(Ta64.item())
         S["ta32"] = ta32
         S["ta4"] = F32(ta4_v[o].item())
-        S["utci_pa"], S["utci_k"] = _utci_table(S["ta_mat"], S["rh32"])
         S["night_lup_base"] = ((F32(0) + ta32) + F32(0)) + F32(273.15)
         Q = patch[o]
         if alt64 > 0:
@@ -954,28 +1019,16 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             sun_off += len(dz)
             # ground temperature wave (solweig.py:2101-2122)
             kd = day_k[i]
-            altmax64 = torch.tensor(altmax[0][i])
-            phase = phase_v[kd]
             CI_TgG = min(cig_v[kd], 1.0)
             S["cig"] = F32(float(CI_TgG))
-            S["altmax32"] = F32(altmax64.item())
-            if props.landcover:
-                tgk_w = torch.from_numpy(np.asarray(props.tgk_wall, F32))
-                tst_w = torch.from_numpy(np.asarray(props.tstart_wall, F32))
-                tmx_w = torch.from_numpy(np.asarray(props.tmaxlst_wall, F32))
-                tgwall = (tgk_w * altmax64 + tst_w) * torch.sin((phase / (tmx_w / 24 - SNUP / 24)) * np.pi / 2)
-            else:
-                tgwall = (0.37 * altmax64 + -3.41) * wave_v[kd]
+            S["altmax32"] = F32(float(altmax[0][i]))
             fac_n = fac_v[kd]
             if code_slot is None:
                 S["tg_factor"][:len(tvals)] = fac_n
             else:
                 for code, k in code_slot.items():
                     S["tg_factor"][code] = fac_n[k]
-            tgwall = torch.maximum(tgwall, torch.tensor(0))
-            tgwall = tgwall * CI_TgG
-            lwall = sbc_t * ewall_t * (tgwall + Ta64 + 273.15) ** 4 - sbc_t * ewall_t * (Ta64 + 273.15) ** 4
-            S["lwall"] = F32(lwall.reshape(-1)[0].item())
+            S["lwall"] = lwall_d[kd]
             # thermal lag weights (solweig.py:451-488), one timeadd for all six planes
             S["tw_first"] = int(firstdaytime == 1)
             if timeadd >= (59 / 1440):
@@ -998,8 +1051,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             kside_rows.append((o, i, lv, radD, radI, alt32))
             L_patches = lv
             # sunlit wall surface of define_patch_characteristics (solweig.py:1596)
-            sun_surf = F32((((ewall_t * sbc_t) * ((Ta64 + tgwall + 273.15) ** 4)) /
-                            torch.tensor(np.pi)).reshape(-1)[0].item())
+            sun_surf = sunsurf_d[kd]
         else:
             S["is_day"] = 0
             S["day_row"] = -1

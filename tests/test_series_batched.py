@@ -108,3 +108,16 @@ def test_sun_tables_equal_one_step_form(scale, amax, rows, cols):
         assert np.float32(azf).tobytes() == np.float32(v[3]).tobytes()
         assert (mode, np.float32(lo).tobytes(), np.float32(hi).tobytes()) == \
             (v[4][0], np.float32(v[4][1]).tobytes(), np.float32(v[4][2]).tobytes())
+
+
+def test_utci_tables_equal_one_step_form():
+    """The UTCI step tables built for all steps at once equal the one-step
+    form bit for bit (float32 chain, float64 log / exp / high powers rounded
+    once), over the forcing range and its edges."""
+    rng = np.random.default_rng(23)
+    ta = np.concatenate([rng.uniform(-60, 70, 20000), [-50.0, 0.0, -0.0, 46.0, 70.0, np.nan]]).astype(np.float32)
+    rh = np.concatenate([rng.uniform(0, 100, 20000), [0.0, 100.0, 5.0, 50.0, np.nan, 30.0]]).astype(np.float32)
+    pa_v, k_v = TS._utci_tables(ta, rh)
+    for j in range(len(ta)):
+        pa, k = TS._utci_table(ta[j], rh[j])
+        assert pa.tobytes() == pa_v[j].tobytes() and k.tobytes() == k_v[j].tobytes(), (j, ta[j], rh[j])

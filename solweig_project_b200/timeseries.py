@@ -983,20 +983,13 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
             CI = 1.
-        alt64 = torch.tensor(altitude[0][i])
-        azi64 = torch.tensor(azimuth[0][i])
-        zen64 = torch.tensor(zen[0][i])
-        Ta64 = Ta64v[o]
-        RH64 = RH64v[o]
-        radG64 = torch.tensor(radG_all[i])
-        jd = jday[0][i]
         esky = esky_v[o]
-        ta32 = F32(Ta64.item())
+        ta32 = F32(float(Ta_all[i]))
         S["ta32"] = ta32
         S["ta4"] = F32(ta4_v[o].item())
         S["night_lup_base"] = ((F32(0) + ta32) + F32(0)) + F32(273.15)
         Q = patch[o]
-        if alt64 > 0:
+        if torch.tensor(altitude[0][i]) > 0:
             S["is_day"] = 1
             S["day_row"] = len(sun_rows)
             d = dc["pos"][i]
@@ -1005,7 +998,8 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             radI, radD = dc["radI"][d], dc["radD"][d]
             lv = dc["lv"][d]
             if lv is None:   # sun below the horizon in the Perez geometry: the 0-dim form
-                lv = _perez((zen64 * (180 / np.pi)).item(), azi64.item(), radD, radI, jd.item())
+                lv = _perez((torch.tensor(zen[0][i]) * (180 / np.pi)).item(), torch.tensor(azimuth[0][i]).item(),
+                            radD, radI, jday[0][i].item())
             # sun march table and wall-face bounds
             dx, dy, dz, az_f, face = suntab[day_k[i]]
             t = np.zeros(len(dz), N.STEP_DTYPE)
@@ -1042,7 +1036,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             S["tw_a"], S["tw_b"] = F32((1 - w).item()), F32(w.item())
             firstdaytime = 0
             # shortwave scalars
-            S["radI"], S["radD"], S["radG"] = F32(radI.item()), F32(radD.item()), F32(radG64.item())
+            S["radI"], S["radD"], S["radG"] = F32(radI.item()), F32(radD.item()), F32(float(radG_all[i]))
             S["sin_alt"], S["cos_alt"] = sw_v["sin_alt"][kd], sw_v["cos_alt"][kd]
             S["tan_beta"], S["qa"] = sw_v["tan_beta"][kd], sw_v["qa"][kd]
             alt32 = sw_v["alt32"][kd]

@@ -280,11 +280,13 @@ def run_exact_chain(*, dsm, trees, dem, walls, aspect, scale, met_file, altitude
     requested = _check_variables(requested)
     site = E.DeviceSite(dsm, trees, dem, walls, aspect, scale, landcover=landcover, lc_class=lc_class,
                         windcoeff=windcoeff, params=_model_params(model_parameters))
+    rasters_ready = torch.cuda.Event()   # the sun marches need the rasters only, not the SVF
+    rasters_ready.record()
     site.run_svf()
     if return_device:
         ser = site.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location)
         return site.run_time_loop(ser, requested=[k for k in N.OUT_BITS if k in requested])
     # host tables of later steps are built while the GPU runs earlier ones
     out, _ = site.run_chain_chunked(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                                    requested=requested)
+                                    requested=requested, rasters_ready=rasters_ready)
     return out

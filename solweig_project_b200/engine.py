@@ -548,8 +548,16 @@ class DeviceSite:
         N.call("sw100_flux_loop", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc),
                _ptr(self.state), out_mask, _ptr(outputs), _stream())
 
+    def side_stream(self) -> torch.cuda.Stream:
+        """Second stream of this site: sun marches, which read only the
+        rasters, run there beside the SVF sweep and the flux loops."""
+        if getattr(self, "_side", None) is None:
+            self._side = torch.cuda.Stream(device=self.device)
+        return self._side
+
     def run_chain_chunked(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                          requested=("utci",), time_start=0, time_stop=None, initial_scalars=None, chunk_steps=8):
+                          requested=("utci",), time_start=0, time_stop=None, initial_scalars=None, chunk_steps=8,
+                          rasters_ready=None):
         """The time loop of steps [time_start, time_stop) with the host tables
         built chunk by chunk while the GPU works: the tables of `chunk_steps`
         steps are built, their sun march and flux loop launched and their
@@ -558,8 +566,13 @@ class DeviceSite:
         (device planes) and the carried scalars (CI, timeadd, firstdaytime)
         pass from chunk to chunk exactly as between the reference's
         consecutive windows, so the result equals one launch over all steps
-        bit for bit.  Returns ({name: (T, rows, cols) float32 ndarray},
-        final carried scalars)."""
+        bit for bit.  Each chunk's tables go up and its sun march runs on the
+        side stream, after `rasters_ready` (an event recorded on the current
+        stream once the rasters were last written; None: everything queued
+        before this call), so it overlaps the SVF sweep and the previous
+        chunk's flux loop; the flux loop waits for it on the current stream.
+        Returns ({name: (T, rows, cols) float32 ndarray}, final carried
+        scalars)."""
         if self.svf_result is None:
             raise RuntimeError("run_svf() (or set_svf()) must come before the time loop")
         if time_stop is None:
@@ -567,21 +580,41 @@ class DeviceSite:
         if chunk_steps < 1:
             raise ValueError("chunk_steps must be >= 1")
         names = [k for k in N.OUT_BITS if k in requested]
+        mask = 0
+        for k in names:
+            mask |= N.OUT_BITS[k]
         n_t = time_stop - time_start
         host = {k: torch.empty((n_t, self.rows, self.cols), dtype=torch.float32, pin_memory=True) for k in names}
         scalars, keep = initial_scalars, []
+        main, side = torch.cuda.current_stream(), self.side_stream()
+        if rasters_ready is None:
+            rasters_ready = torch.cuda.Event()
+            rasters_ready.record(main)
+        side.wait_event(rasters_ready)
         dc = TS.day_chain(met_file, altitude, azimuth, zen, jday, location, time_start, time_stop)
         for t0 in range(time_start, time_stop, chunk_steps):
             t1 = min(time_stop, t0 + chunk_steps)
             ser = self.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
                                     time_start=t0, time_stop=t1, initial_scalars=scalars, day_chain=dc)
             scalars = ser.final
-            out = self.run_time_loop(ser, requested=names)
-            for k in names:
-                host[k][t0 - time_start:t1 - time_start].copy_(out[k], non_blocking=True)
-                TRANSFER["d2h"] += out[k].numel() * out[k].element_size()
-            keep.append((out, self._keep))
-        torch.cuda.current_stream().synchronize()
+            with torch.cuda.stream(side):
+                s, dev = self.upload_series(ser)
+                gsrc = torch.empty((max(1, s.n_day), self.rows, self.cols, 4), dtype=torch.float32,
+                                   device=self.device)
+                if s.n_day:
+                    self.launch_sun_march(s, gsrc)
+                marched = torch.cuda.Event()
+                marched.record(side)
+            main.wait_event(marched)
+            out = torch.empty((len(names), t1 - t0, self.rows, self.cols), dtype=torch.float32, device=self.device)
+            self.launch_flux_loop(s, gsrc, mask, out)
+            for i, k in enumerate(names):
+                host[k][t0 - time_start:t1 - time_start].copy_(out[i], non_blocking=True)
+                TRANSFER["d2h"] += out[i].numel() * out[i].element_size()
+            # every buffer stays referenced until the final synchronize: the
+            # side-stream allocations are read on the current stream
+            keep.append((out, dev, gsrc))
+        main.synchronize()
         return {k: v.numpy() for k, v in host.items()}, scalars
 
     def load_state(self, state: dict):

@@ -51,8 +51,10 @@ __device__ __forceinline__ float atan_r(float x) { return (float)atan((double)x)
 __device__ __forceinline__ float sin_r(float x) { return (float)sin((double)x); }
 __device__ __forceinline__ float cos_r(float x) { return (float)cos((double)x); }
 
-// cylindric_wedge (solweig.py:404-449) + NaN -> 0.5 (solweig.py:2168)
-__device__ __forceinline__ float cylindric_wedge(float ta, float tb, float qa) {
+// cylindric_wedge (solweig.py:404-449) + NaN -> 0.5 (solweig.py:2168).
+// Out of line: its double-precision atan / sin / cos are a large block of
+// code run once per pixel and step, kept out of the step's loop code.
+__device__ __noinline__ float cylindric_wedge(float ta, float tb, float qa) {
   const float tt = ta * tb;
   const float xa = 1.f - 2.f / tt;
   const float ha = 2.f / tt;

@@ -558,14 +558,18 @@ def _kside_tables(patch, kside_rows, diff_vals, albedo_b, azimuth, altitude):
         sh_k = ((albedo_b * radD * 0.5) / torch.pi).numpy()
         cos_p, ang, ster_n = cos_pt.numpy(), ang_t.numpy(), ster.numpy()
         lum_n, lvz = lumChi.numpy(), plum.numpy()
-        for di in range(4):
-            patch["kside_d"][rows_, :, di] = ((diff_vals[di] * lum_n) * ang[None, :]) * ster_n[None, :]
-            patch["anilum"][rows_, :, di] = diff_vals[di] * lvz
-        patch["kref_veg"][rows_] = (sh_k[:, None] * ster_n[None, :]) * cos_p[None, :]
-        patch["kref_sun"][rows_] = (sun_k[:, None] * ster_n[None, :]) * cos_p[None, :]
-        patch["kref_sh"][rows_] = patch["kref_veg"][rows_]
+        # the four (sh, vegsh) codes as a last axis, one whole-field write each
+        # (a slice when the rows are consecutive, as daytime rows are)
+        sel = slice(rows_[0], rows_[-1] + 1) if rows_ == list(range(rows_[0], rows_[-1] + 1)) else rows_
+        dv = np.asarray(diff_vals, F32)[None, None, :]
+        patch["kside_d"][sel] = ((dv * lum_n[:, :, None]) * ang[None, :, None]) * ster_n[None, :, None]
+        patch["anilum"][sel] = dv * lvz[:, :, None]
+        kref_sh = (sh_k[:, None] * ster_n[None, :]) * cos_p[None, :]
+        patch["kref_veg"][sel] = kref_sh
+        patch["kref_sh"][sel] = kref_sh
+        patch["kref_sun"][sel] = (sun_k[:, None] * ster_n[None, :]) * cos_p[None, :]
         yk, yl, fl, _ = _yi_tables([it[1] for it in items], azimuth, altitude, pazi)
-        patch["yi_k"][rows_], patch["yi_l"][rows_], patch["flags"][rows_] = yk, yl, fl
+        patch["yi_k"][sel], patch["yi_l"][sel], patch["flags"][sel] = yk, yl, fl
 
 
 def _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t):

@@ -587,6 +587,7 @@ def _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t):
     f32 = torch.float32
     for palt, items in groups.values():
         rows_ = [it[0] for it in items]
+        sel = slice(rows_[0], rows_[-1] + 1) if rows_ == list(range(rows_[0], rows_[-1] + 1)) else rows_
         E = torch.stack([it[1] for it in items])
         ta4 = ta4_v[rows_]
         _, expo, idx, ster, sin_u, cos_u = _lsky_geometry(palt)
@@ -594,20 +595,20 @@ def _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t):
         base = ((band * torch.tensor(SBC) * ta4.to(f32)[:, None]) / torch.tensor(np.pi))[:, idx]
         bs = base * ster[None, :]
         G = _lcyl_geometry(palt)
-        patch["ld_sky"][rows_] = (bs * sin_u[idx].to(f32)[None, :]).numpy()
-        patch["ls_sky"][rows_] = (bs * cos_u[idx].to(f32)[None, :]).numpy()
-        patch["ster"][rows_] = G["ster_n"]
-        patch["cos_alt"][rows_] = G["cos_n"]
-        patch["sin_alt"][rows_] = G["sin_n"]
+        patch["ld_sky"][sel] = (bs * sin_u[idx].to(f32)[None, :]).numpy()
+        patch["ls_sky"][sel] = (bs * cos_u[idx].to(f32)[None, :]).numpy()
+        patch["ster"][sel] = G["ster_n"]
+        patch["cos_alt"][sel] = G["cos_n"]
+        patch["sin_alt"][sel] = G["sin_n"]
         surf = ((ewall_t * sbc_t * ta4) / torch.tensor(np.pi))  # float64
         vc = ((surf[:, None] * G["s64"][None, :]) * G["cos64"][None, :]).numpy()
         vs = ((surf[:, None] * G["s64"][None, :]) * G["sin64"][None, :]).numpy()
-        patch["veg_cos"][rows_], patch["veg_sin"][rows_] = vc, vs
-        patch["sh_cos"][rows_], patch["sh_sin"][rows_] = vc, vs
+        patch["veg_cos"][sel], patch["veg_sin"][sel] = vc, vs
+        patch["sh_cos"][sel], patch["sh_sin"][sel] = vc, vs
         S = np.array([it[2] for it in items], F32)[:, None]
-        patch["sun_cos"][rows_] = (S * G["ster_n"][None, :]) * G["cos_n"][None, :]
-        patch["sun_sin"][rows_] = (S * G["ster_n"][None, :]) * G["sin_n"][None, :]
-        patch["thr_sun"][rows_], patch["thr_shd"][rows_] = G["thr"]
+        patch["sun_cos"][sel] = (S * G["ster_n"][None, :]) * G["cos_n"][None, :]
+        patch["sun_sin"][sel] = (S * G["ster_n"][None, :]) * G["sin_n"][None, :]
+        patch["thr_sun"][sel], patch["thr_shd"][sel] = G["thr"]
 
 
 def _lsky(esky, palt, Ta64, ta4=None):

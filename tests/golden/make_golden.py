@@ -1,8 +1,10 @@
 """Generate the golden fixtures by running the reference implementation.
 
-Run in a container where the reference checkout is available (read-only):
+Run where a read-only checkout of the reference is available:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>
+
+(``--ref`` may be replaced by the environment variable ``SOLWEIG_REFERENCE``.)
 
 It imports ``solweig_gpu`` from the reference with I/O-only stubs for GDAL,
 timezonefinder and pytz (they are used only for raster I/O and time zones),
@@ -38,6 +40,16 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 
 from solweig_project_b200 import synthetic  # noqa: E402
+
+
+def reference_path(arg):
+    """The reference checkout named by ``--ref`` or ``$SOLWEIG_REFERENCE``."""
+    ref = arg or os.environ.get("SOLWEIG_REFERENCE")
+    if not ref:
+        raise SystemExit("name the reference checkout with --ref or SOLWEIG_REFERENCE")
+    if not os.path.isdir(os.path.join(ref, "solweig_gpu")):
+        raise SystemExit(f"{ref!r} holds no solweig_gpu package")
+    return ref
 
 
 def install_stubs(ref):
@@ -262,9 +274,10 @@ def run_case(name, spec, ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (or $SOLWEIG_REFERENCE)")
     ap.add_argument("--cases", nargs="*", default=list(CASES))
     args = ap.parse_args()
+    args.ref = reference_path(args.ref)
     install_stubs(args.ref)
     import torch
     torch.set_num_threads(max(1, os.cpu_count() or 1))

@@ -1,7 +1,9 @@
 """Sun geometry of the benchmark workloads, computed with the reference's own
 ``Solweig_2015a_metdata_noload`` (solweig_gpu/sun_position.py:905-1010).
 
-    python tests/golden/make_sun_geometry.py [--ref /root/reference]
+    python tests/golden/make_sun_geometry.py --ref <reference checkout>
+
+(``--ref`` may be replaced by the environment variable ``SOLWEIG_REFERENCE``.)
 
 Writes tests/golden/sun_geometry.npz with, per site, the float64 (1, 24)
 arrays altitude / azimuth / zen / jday / dectime / altmax that
@@ -25,15 +27,15 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 sys.path.insert(0, HERE)
 
-from make_golden import install_stubs  # noqa: E402
+from make_golden import install_stubs, reference_path  # noqa: E402
 from solweig_project_b200 import synthetic  # noqa: E402
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (or $SOLWEIG_REFERENCE)")
     args = ap.parse_args()
-    install_stubs(args.ref)
+    install_stubs(reference_path(args.ref))
     import solweig_gpu.sun_position as rsun
     out = {}
 

@@ -65,6 +65,11 @@ NCU_TRAFFIC = {"flux_loop": (500 * 500, 119_174_400), "svf_sweep": (1024 * 1024,
 # should not move the figure)
 E2E_TIMED = 7
 NCU_ISSUE_ACTIVE = {"flux_loop": 0.541, "svf_sweep": 0.758, "sun_march": 0.791}
+# active lanes per issued warp instruction (of 32) in the same captures
+NCU_ACTIVE_LANES = {"flux_loop": 21.16, "svf_sweep": 24.42, "sun_march": 26.50}
+# reference pins of the 500 x 500 city (seed 1234): Tmrt / UTCI of the
+# unmodified reference and of an FP64 re-evaluation at seeded sample pixels
+PINS = {"exact500": os.path.join(REPO, "tests", "golden", "large_c2_500.npz")}
 
 
 def parse():
@@ -199,6 +204,30 @@ class ClockSampler:
         reasons = sorted({self.REASONS[i] for r in rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(sm), "source": "nvidia-smi"}
+
+
+def _err(got, want):
+    d = np.asarray(got, np.float64) - np.asarray(want, np.float64)
+    d = d[~np.isnan(d)]
+    return {"max": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d)))}
+
+
+def error_vs_fp64(pin_path, tmrt, utci):
+    """Tmrt / UTCI of the timed step against the reference pins of the same
+    city (tests/golden/make_golden_large.py): the unmodified reference's
+    float32 values and an FP64 re-evaluation of the same chain (same shadow
+    geometry), at 4096 ground + 256 building sample pixels of every step."""
+    with np.load(pin_path) as z:
+        d = {k: z[k] for k in z.files}
+    T, s = d["sample_tmrt"].shape[0], d["samples"]
+    tm, ut = tmrt.reshape(T, -1)[:, s], utci.reshape(T, -1)[:, s]
+    tm64 = d["sample_tmrt"].astype(np.float64) + d["sample_tmrt64_delta"]
+    ut64 = d["sample_utci"].astype(np.float64) + d["sample_utci64_delta"]
+    return {"samples": f"{s.size} px x {T} steps", "tmrt_K": _err(tm, tm64), "utci_C": _err(ut, ut64),
+            "reference_tmrt_K": _err(d["sample_tmrt"], tm64), "reference_utci_C": _err(d["sample_utci"], ut64),
+            "vs_reference_tmrt_K": _err(tm, d["sample_tmrt"]), "vs_reference_utci_C": _err(ut, d["sample_utci"]),
+            "reference_all_px_tmrt_K": {"max": float(d["ref_fp64_tmrt_max"]), "rms": float(d["ref_fp64_tmrt_rms"])},
+            "reference_all_px_utci_C": {"max": float(d["ref_fp64_utci_max"]), "rms": float(d["ref_fp64_utci_rms"])}}
 
 
 def cpu_baseline(city, met, geo, lc_class, crop=64):
@@ -367,11 +396,18 @@ def run_batched(args, world, rank, local):
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         npix_rank = batch.pixels
-        svf_steps = sum(m.n_steps * m.site.rows * m.site.cols for m in batch.members)
         dom = max(("svf", "flux"), key=lambda k: stage_ms[k])
         if dom == "svf":
-            achieved = SVF_GATHER_BYTES_PER_STEP * svf_steps / (stage_ms["svf"] * 1e6)
-            note = "march gather bytes (12 B x executed steps per pixel) / launch time"
+            # source gathers the sweeps execute, counted site by site with the
+            # counting sweep (untimed; the batch kernel runs the same marches)
+            gathers = 0
+            for m in batch.members:
+                tmp_p = torch.empty((N.SVF_PLANES, m.site.rows, m.site.cols), dtype=torch.float32, device=dev)
+                tmp_b = torch.empty((3, N.CUBE_WORDS, m.site.rows, m.site.cols), dtype=torch.int32, device=dev)
+                gathers += m.site.count_svf_gathers(tmp_p, tmp_b)
+            achieved = SVF_GATHER_BYTES_PER_STEP * gathers / (stage_ms["svf"] * 1e6)
+            note = "march gather bytes (12 B x source gathers executed, counted by sw100_svf_sweep_count) / " \
+                   "launch time"
         else:
             achieved = FLUX_BYTES_PER_PX_STEP * npix_rank * N_STEPS_DAY / (stage_ms["flux"] * 1e6)
             note = "compulsory 190 B per pixel-step / launch time"
@@ -524,6 +560,8 @@ def main():
 
     for _ in range(args.warmup):
         step()
+    # source gathers the sweep's marches execute (counting kernel, untimed)
+    svf_gathers = site.count_svf_gathers(planes, bits)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -592,15 +630,23 @@ def main():
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         stages = {
-            "svf_sweep": {"ms": svf_t, "gbs_gather": SVF_GATHER_BYTES_PER_STEP * svf_steps * npix / (svf_t * 1e6)},
-            "sun_march": {"ms": march_t},
+            "svf_sweep": {"ms": svf_t, "table_steps_per_px": svf_steps,
+                          "executed_gathers_per_px": svf_gathers / npix,
+                          "gbs_gather": SVF_GATHER_BYTES_PER_STEP * svf_gathers / (svf_t * 1e6),
+                          "issue_active_frac_ncu": NCU_ISSUE_ACTIVE["svf_sweep"],
+                          "active_lanes_ncu": NCU_ACTIVE_LANES["svf_sweep"]},
+            "sun_march": {"ms": march_t, "issue_active_frac_ncu": NCU_ISSUE_ACTIVE["sun_march"],
+                          "active_lanes_ncu": NCU_ACTIVE_LANES["sun_march"]},
             "flux_loop": {"ms": loop_t,
-                          "gbs_compulsory": FLUX_BYTES_PER_PX_STEP * npix * N_STEPS_DAY / (loop_t * 1e6)},
+                          "gbs_compulsory": FLUX_BYTES_PER_PX_STEP * npix * N_STEPS_DAY / (loop_t * 1e6),
+                          "issue_active_frac_ncu": NCU_ISSUE_ACTIVE["flux_loop"],
+                          "active_lanes_ncu": NCU_ACTIVE_LANES["flux_loop"]},
         }
         dom = max(stages, key=lambda k: stages[k]["ms"])
         if dom == "svf_sweep":
             achieved = stages[dom]["gbs_gather"]
-            roof_note = "march gather bytes (12 B x executed steps per pixel) / launch time"
+            roof_note = "march gather bytes (12 B x source gathers executed, counted by sw100_svf_sweep_count) / " \
+                        "launch time"
         elif dom == "flux_loop":
             achieved = stages[dom]["gbs_compulsory"]
             roof_note = "compulsory 190 B per pixel-step / launch time"
@@ -624,6 +670,7 @@ def main():
                          "definition": roof_note,
                          "binding": {"resource": "SM instruction issue", "kernel": dom,
                                      "issue_active_frac_ncu": NCU_ISSUE_ACTIVE.get(dom),
+                                     "active_lanes_ncu": NCU_ACTIVE_LANES.get(dom),
                                      "note": "DRAM traffic per launch is far below the algorithmic bytes: each "
                                              "pixel's patch-bit cubes are read once per launch and kept on chip "
                                              "(shared memory) across the 24 steps"}},
@@ -633,6 +680,9 @@ def main():
         }
         if e2e is not None:
             line["e2e"] = e2e
+        pin = PINS.get(args.workload) if args.side is None else None
+        if pin is not None and os.path.exists(pin):
+            line["error_vs_fp64"] = error_vs_fp64(pin, outputs[1].cpu().numpy(), outputs[0].cpu().numpy())
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(city, met, geo, lc_class)
         print(json.dumps(line), flush=True)

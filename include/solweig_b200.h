@@ -225,6 +225,18 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
                     const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
                     void* workspace, int64_t workspace_bytes, void* stream);
 
+/* The same sweep (identical outputs), also counting into *executed (device
+ * memory, overwritten) the source gathers its marches execute -- the steps
+ * the early exits and the 8-step shortcut leave out are not counted.  Each
+ * gather reads the 12 bytes dsm / vegdsm / vegdsm2 that the march step
+ * counts of the reference's step tables are defined on
+ * (solweig_core/numba_cpu/step_table_gen.py:240-321), so 12 x *executed are
+ * the algorithmic bytes of the launch.  For measurement, not for the hot
+ * path: the counter costs time. */
+int sw100_svf_sweep_count(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                          const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
+                          void* workspace, int64_t workspace_bytes, uint64_t* executed, void* stream);
+
 /* ------------------------------------------- windowed SVF recompute -- */
 /* Corridor descriptor of one patch for sw100_svf_window (one int32 per
  * patch, built by the host from the step table): bits 0-1 the axis of the
@@ -302,23 +314,30 @@ int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbs
  * allocations, or latency-bound loops that cannot afford cudaMalloc /
  * cudaFree (both may synchronise the device).  Such callers still pass
  * their inputs and outputs; the scratch space of the sweep (the packed
- * march source and the bush step flags) lives in a file-scope static
- * device array of SW100_SVF_NOALLOC_SCRATCH_BYTES bytes, which every GPU
- * that loads this library holds until the process exits.
+ * march source, the bush step flags and the 8 x 8 skip map) lives in a
+ * file-scope static device array of SW100_SVF_NOALLOC_SCRATCH_BYTES bytes,
+ * which every GPU that loads this library holds until the process exits.
+ * The launches are those of sw100_svf_sweep, with that array as the
+ * workspace.
  *
  * Limits: the grid must satisfy
- *   align256(rows * cols * 16) + align256(n_steps * 4) <= SW100_SVF_NOALLOC_SCRATCH_BYTES
+ *   sw100_svf_workspace_bytes(rows, cols, n_steps) <= SW100_SVF_NOALLOC_SCRATCH_BYTES
+ * i.e. align256(rows * cols * 16) + align256(n_steps * 4)
+ *      + align256(ceil(rows / 8) * ceil(cols / 8) * 4)
  * (up to 1024 x 1024 pixels with 65536 table steps); larger requests are
  * refused with SW100_E_SIZE before anything is launched.
  *
  * The first call on each device looks up the array's device address with
  * that device current (cudaGetSymbolAddress) and caches it; make that first
- * call before any stream capture on the device.  All calls share the one
+ * call before any stream capture on the device.  The cached address is not
+ * refreshed after cudaDeviceReset(): a process that resets a device must not
+ * call this entry point on that device again.  All calls share the one
  * array, which keeps the last call's contents (the bush flags are cleared
- * on every call): calls that overlap on the GPU, on different streams or
- * from different threads, race on it and must be serialised by the
- * caller.  Results are identical to sw100_svf_sweep. */
-#define SW100_SVF_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024 + 256 * 1024)
+ * on every call, and the packed source and skip map are rewritten): calls
+ * that overlap on the GPU, on different streams or from different threads,
+ * race on it and must be serialised by the caller.  Results are identical
+ * to sw100_svf_sweep. */
+#define SW100_SVF_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024 + 256 * 1024 + 64 * 1024)
 int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
                             const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
                             void* stream);
@@ -541,10 +560,18 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
  * float32 output instead of bf16, bias may be NULL.  A data gradient is
  * this call on the output gradient with the data-gradient weight layout.
  * err (device int32, may be NULL) is set to 1 when a bounded wait of the
- * kernel expired. */
+ * kernel expired: the block then issues no further copy or MMA, waits for
+ * the MMAs it issued (with the default limit), frees its tensor memory and
+ * writes no output; err is set to 2 when that drain ran out as well. */
 int sw100_nn_conv3x3_tc(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* wt,
                         const float* bias, int cout, void* y, int ystride, int ycoff, int relu, int out_f32,
                         int32_t* err, void* stream);
+/* Polls of an mbarrier before a wait of the tensor-core kernels gives up
+ * (default 2^22; a negative value restores it).  Returns the previous
+ * limit.  Process-wide; meant for tests of the timeout path (a limit of 0
+ * makes every pipeline wait run out at once).  No counterpart in the
+ * reference. */
+int sw100_set_wait_limit(int polls);
 /* dw (float32, forward layout) and dbias (may be NULL) += the gradients of
  * a 3 x 3 convolution given its input x and output gradient dy. */
 int sw100_nn_conv3x3_wgrad(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* dy,

@@ -24,14 +24,14 @@ N_GVF_AZ = 18
 UTCI_TERMS = 210
 MAX_GVF_STEPS = 64
 SVF_PLANES = 19
-SVF_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024 + 256 * 1024
+SVF_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024 + 256 * 1024 + 64 * 1024
 
 OUT_UTCI, OUT_TMRT, OUT_KUP, OUT_KDOWN, OUT_LUP, OUT_LDOWN, OUT_SHADOW = (1 << i for i in range(7))
 OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDOWN, "lup": OUT_LUP,
             "ldown": OUT_LDOWN, "shadow": OUT_SHADOW}
 
 # Exported symbols (checked by the CPU tests against include/solweig_b200.h)
-SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noalloc", "sw100_pack_cubes",
+SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_count", "sw100_svf_sweep_noalloc", "sw100_pack_cubes",
            "sw100_sun_march_workspace_bytes", "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop",
            "sw100_flux_loop", "sw100_utci", "sw100_abi_version", "sw100_last_error", "sw100_launch_count",
            "sw100_svf_window_workspace_bytes", "sw100_svf_window", "sw100_diff_bbox_workspace_bytes",
@@ -39,7 +39,7 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_noal
            "sw100_batch_skipmap", "sw100_batch_svf", "sw100_batch_sun_march", "sw100_batch_flux_loop",
            "sw100_utci_steps", "sw100_nn_conv3x3_wgrad", "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2",
            "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc",
-           "sw100_prepare_site", "sw100_march_tables")
+           "sw100_prepare_site", "sw100_march_tables", "sw100_set_wait_limit")
 ABI_VERSION = 2  # SW100_ABI_VERSION of include/solweig_b200.h
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
@@ -174,6 +174,8 @@ def load(path: str = LIB_PATH):
         "sw100_svf_workspace_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, i64p]),
         "sw100_svf_sweep": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp,
                                       C.c_int64, vp]),
+        "sw100_svf_sweep_count": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp,
+                                            C.c_int64, vp, vp]),
         "sw100_svf_sweep_noalloc": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp,
                                               vp]),
         "sw100_pack_cubes": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32), vp, vp]),
@@ -208,6 +210,7 @@ def load(path: str = LIB_PATH):
             "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
             "sw100_batch_flux_loop")},
         "sw100_batch_skipmap": (C.c_int, [vp, C.c_int, vp]),
+        "sw100_set_wait_limit": (C.c_int, [C.c_int]),
         "sw100_prepare_site": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(ClassTable), C.c_int, C.c_int] + [vp] * 12),
         "sw100_march_tables": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, vp, C.c_int64, vp,
                                          i64p]),

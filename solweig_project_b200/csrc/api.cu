@@ -24,6 +24,10 @@ __global__ void pack4_kernel(const float* a, const float* b, const float* c, con
 __global__ void svf_sweep_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                  const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
                                  uint32_t* bits, int n_steps, const float* skipmap);
+__global__ void svf_sweep_count_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
+                                       const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
+                                       uint32_t* bits, int n_steps, const float* skipmap,
+                                       unsigned long long* executed);
 __global__ void svf_skipmap_kernel(const float4* src4, int rows, int cols, float* m, int crow, int ccol);
 __global__ void svf_window_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                   const sw100_step* steps, const int32_t* corridor, float vmax, int4 rect, int4 win,
@@ -55,7 +59,7 @@ __global__ void utci_kernel(const float* ta, const float* rh, const float* tmrt,
                             float* out);
 __global__ void nn_conv3x3_tc_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
                                      const __nv_bfloat16* Wt, const float* bias, int Cout, void* Yv, int ystride,
-                                     int ycoff, int relu, int out_f32, int* err);
+                                     int ycoff, int relu, int out_f32, int* err, int wait_limit);
 __global__ void nn_wgrad_kernel(const __nv_bfloat16* X, int N, int H, int W, int Cin, int xstride, int xcoff,
                                 const __nv_bfloat16* dY, int Cout, int dstride, int dcoff, float* dW, float* dbias,
                                 int rows_per_block);
@@ -89,6 +93,9 @@ namespace {
 
 thread_local std::string g_last_error;
 std::atomic<int64_t> g_launches{0};
+// polls of an mbarrier before a tensor-core kernel's wait gives up
+constexpr int kDefaultTcWaitLimit = 1 << 22;
+std::atomic<int> g_tc_wait_limit{kDefaultTcWaitLimit};
 
 constexpr int64_t kMaxPixels = int64_t(1) << 31;  // int32 pixel offsets inside kernels
 constexpr int64_t kAlign = 256;
@@ -222,9 +229,14 @@ int sw100_svf_workspace_bytes(int rows, int cols, int n_steps, int64_t* bytes) {
   return 0;
 }
 
-int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
-                    const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits, void* workspace,
-                    int64_t workspace_bytes, void* stream) {
+}  // extern "C"
+
+namespace {
+// Packing, bush flags and skip map of a sweep, then the sweep itself (the
+// counting kernel when `executed` is set).
+int run_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                  const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits, void* workspace,
+                  int64_t workspace_bytes, unsigned long long* executed, void* stream) {
   int rc;
   if ((rc = check_grid(rows, cols))) return rc;
   if ((rc = validate_site_march(site))) return rc;
@@ -253,9 +265,35 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
   // similar obstacles (less divergence than a 32 x 1 row: -20 % time)
   const dim3 sblock(kMarchBx, kMarchBy);
   const dim3 sgrid((cols + kMarchBx - 1) / kMarchBx, (rows + kMarchBy - 1) / kMarchBy);
-  svf_sweep_kernel<<<sgrid, sblock, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                             site->vmax, out_planes, out_bits, n_steps, skipmap);
-  return check_launch("svf_sweep_kernel");
+  if (executed == nullptr) {
+    svf_sweep_kernel<<<sgrid, sblock, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
+                                               site->vmax, out_planes, out_bits, n_steps, skipmap);
+    return check_launch("svf_sweep_kernel");
+  }
+  cudaError_t e = cudaMemsetAsync(executed, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+  svf_sweep_count_kernel<<<sgrid, sblock, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
+                                                   site->vmax, out_planes, out_bits, n_steps, skipmap, executed);
+  return check_launch("svf_sweep_count_kernel");
+}
+}  // namespace
+
+extern "C" {
+
+int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                    const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits, void* workspace,
+                    int64_t workspace_bytes, void* stream) {
+  return run_svf_sweep(site, rows, cols, plan, steps, n_steps, out_planes, out_bits, workspace, workspace_bytes,
+                       nullptr, stream);
+}
+
+int sw100_svf_sweep_count(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
+                          const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
+                          void* workspace, int64_t workspace_bytes, uint64_t* executed, void* stream) {
+  int rc;
+  if ((rc = check_ptr(executed, "executed"))) return rc;
+  return run_svf_sweep(site, rows, cols, plan, steps, n_steps, out_planes, out_bits, workspace, workspace_bytes,
+                       reinterpret_cast<unsigned long long*>(executed), stream);
 }
 
 int sw100_svf_window_workspace_bytes(int rows, int cols, int64_t* bytes) {
@@ -604,8 +642,9 @@ constexpr int kMaxDevices = 128;
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
+// Device address of the scratch array on the current device, looked up with
+// that device current on the first call for it and cached (the cache is not
+// refreshed after cudaDeviceReset; see the header).
 int noalloc_scratch(void** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -627,36 +666,23 @@ extern "C" int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, 
                                        const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
                                        void* stream) {
   int rc;
-  if ((rc = check_grid(rows, cols))) return rc;
-  if ((rc = validate_site_march(site))) return rc;
-  if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(out_planes, "out_planes")) ||
-      (rc = check_ptr(out_bits, "out_bits")))
-    return rc;
-  if ((rc = check_grid(rows, cols))) return rc;
-  if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
-  const int64_t need = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4);
+  int64_t need = 0;
+  if ((rc = sw100_svf_workspace_bytes(rows, cols, n_steps, &need))) return rc;
   if (need > (int64_t)SW100_SVF_NOALLOC_SCRATCH_BYTES)
     return fail(SW100_E_SIZE,
                 "grid %d x %d with %d steps needs %lld scratch bytes; the allocation-free sweep has %lld "
                 "(at most 1024 x 1024 pixels)",
                 rows, cols, n_steps, (long long)need, (long long)SW100_SVF_NOALLOC_SCRATCH_BYTES);
+  if ((rc = validate_site_march(site))) return rc;
+  if ((rc = check_ptr(plan, "plan")) || (rc = check_ptr(steps, "steps")) || (rc = check_ptr(out_planes, "out_planes")) ||
+      (rc = check_ptr(out_bits, "out_bits")))
+    return rc;
   void* scratch = nullptr;
   if ((rc = noalloc_scratch(&scratch))) return rc;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  float4* src4 = static_cast<float4*>(scratch);
-  uint32_t* flags = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + align_up((int64_t)rows * cols * 16));
-  if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
-  dim3 block(32, 4);
-  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
-  if (site->bush_any) {
-    cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)n_steps * 4, st);
-    if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
-    svf_bush_flags_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, flags, n_steps);
-    if ((rc = check_launch("svf_bush_flags_kernel"))) return rc;
-  }
-  svf_sweep_kernel<<<grid, block, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                           site->vmax, out_planes, out_bits, n_steps, nullptr);
-  return check_launch("svf_sweep_kernel");
+  // the workspace sweep's own launches (packing, bush flags, skip map,
+  // sweep), with the static array as its workspace
+  return run_svf_sweep(site, rows, cols, plan, steps, n_steps, out_planes, out_bits, scratch,
+                       (int64_t)SW100_SVF_NOALLOC_SCRATCH_BYTES, nullptr, stream);
 }
 
 extern "C" int sw100_utci_steps(const sw100_time_step* steps, int n_steps, const float* tmrt,
@@ -713,8 +739,14 @@ int sw100_nn_conv3x3_tc(const void* x, int n, int h, int w, int cin, int xstride
   }
   nn_conv3x3_tc_kernel<<<(unsigned)blocks, 128, smem, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const __nv_bfloat16*>(x), n, h, w, cin, xstride, xcoff, static_cast<const __nv_bfloat16*>(wt), bias,
-      cout, y, ystride, ycoff, relu, out_f32, err);
+      cout, y, ystride, ycoff, relu, out_f32, err, g_tc_wait_limit.load());
   return check_launch("nn_conv3x3_tc_kernel");
+}
+
+int sw100_set_wait_limit(int polls) {
+  const int prev = g_tc_wait_limit.load();
+  g_tc_wait_limit.store(polls < 0 ? kDefaultTcWaitLimit : polls);
+  return prev;
 }
 
 int sw100_nn_conv3x3_wgrad(const void* x, int n, int h, int w, int cin, int xstride, int xcoff, const void* dy,

@@ -77,9 +77,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait; false when it gave up
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
-  for (int i = 0; i < (1 << 22); ++i)
+// bounded wait: at most `limit` polls; false when it gave up
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; ++i)
     if (mbar_try_wait(addr, parity)) return true;
   return false;
 }
@@ -123,6 +123,8 @@ __device__ __forceinline__ int core_off(int r, int h) { return (r >> 3) * 256 + 
 constexpr int kTcStepsPerStage = 4;
 constexpr int kTcStageBytes = kTcStepsPerStage * 4096;
 constexpr int kTcStages = 3;
+// polls of an mbarrier before a wait gives up (the default wait limit)
+constexpr int kTcWaitLimit = 1 << 22;
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(128) nn_conv3x3_tc_kernel(const __nv_bfloat16*
                                                             const __nv_bfloat16* __restrict__ Wt,
                                                             const float* __restrict__ bias, int Cout, void* Yv,
                                                             int ystride, int ycoff, int relu, int out_f32,
-                                                            int* __restrict__ err) {
+                                                            int* __restrict__ err, int wait_limit) {
   // dynamic shared memory: kTcStages A stage buffers, then kTcStages B
   // stage buffers, 1024-byte aligned; 96 KB per CTA also caps the CTAs per
   // SM at 2, so TMEM (<= 128 columns each) is never oversubscribed
@@ -199,17 +201,22 @@ __global__ void __launch_bounds__(128) nn_conv3x3_tc_kernel(const __nv_bfloat16*
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
 
+  // Pipeline status, the same for every thread of the block (each wait's
+  // outcome is combined with __syncthreads_and).  Once a wait has run out,
+  // no further copy or MMA is issued: the block drains what it issued and
+  // frees its tensor memory.
   bool ok = true;
+  int last_commit = -1;  // the last stage whose MMAs were committed (thread 0)
   load_stage(0);
   if (nstages > 1) load_stage(1);
-  for (int g = 0; g < nstages; ++g) {
+  for (int g = 0; g < nstages && ok; ++g) {
     const int buf = g % kTcStages;
     // this stage's copies are done (the next stage's may still be in flight)
     if (g + 1 < nstages) asm volatile("cp.async.wait_group 1;" ::: "memory");
     else asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (tid == 0 && ok) {
+    if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int s0 = g * kTcStepsPerStage;
       const int ns = min(kTcStepsPerStage, nsteps - s0);
@@ -219,17 +226,34 @@ __global__ void __launch_bounds__(128) nn_conv3x3_tc_kernel(const __nv_bfloat16*
         tc::mma_f16(tmem, ad, bd, idesc, (s0 + j) > 0 ? 1u : 0u);
       }
       tc::commit(tc::smem_u32(&mbar[buf]));
+      last_commit = g;
     }
     // stage g + 2 reuses the buffer of stage g - 1: wait for its MMAs first
     if (g + 2 < nstages) {
-      if (g >= 1 && ok) ok = tc::mbar_wait(tc::smem_u32(&mbar[(g - 1) % kTcStages]), ((g - 1) / kTcStages) & 1);
-      load_stage(g + 2);
+      bool w = true;
+      if (g >= 1) w = tc::mbar_wait(tc::smem_u32(&mbar[(g - 1) % kTcStages]), ((g - 1) / kTcStages) & 1, wait_limit);
+      ok = __syncthreads_and(w) != 0;
+      if (ok) load_stage(g + 2);
     }
   }
   // the last stage's MMAs (its commit covers every earlier one)
-  if (ok && nstages > 0)
-    ok = tc::mbar_wait(tc::smem_u32(&mbar[(nstages - 1) % kTcStages]), ((nstages - 1) / kTcStages) & 1);
-  if (!ok && err) atomicExch(err, 1);
+  if (ok && nstages > 0) {
+    const bool w =
+        tc::mbar_wait(tc::smem_u32(&mbar[(nstages - 1) % kTcStages]), ((nstages - 1) / kTcStages) & 1, wait_limit);
+    ok = __syncthreads_and(w) != 0;
+  }
+  if (!ok) {
+    // drain: no copy is left in flight, and the MMAs issued so far (the last
+    // commit covers them all) are waited for with the default limit before
+    // the tensor memory they write is freed
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    bool drained = true;
+    if (tid == 0 && last_commit >= 0)
+      drained = tc::mbar_wait(tc::smem_u32(&mbar[last_commit % kTcStages]), (last_commit / kTcStages) & 1,
+                              max(wait_limit, kTcWaitLimit));
+    drained = __syncthreads_and(drained) != 0;
+    if (tid == 0 && err) atomicExch(err, drained ? 1 : 2);
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   // epilogue: 16 columns at a time from this warp's 32 TMEM lanes
   if (ok) {

@@ -27,12 +27,16 @@ struct SvfAcc {
 };
 
 // One patch march for one pixel (shadow.py:228-316).  Returns final sh
-// (1 = sky visible), vegsh and vbshvegsh as floats.
+// (1 = sky visible), vegsh and vbshvegsh as floats.  COUNT: add the number
+// of source gathers the march executes to *ns (the counting instantiation
+// of the sweep; the plain one compiles the counter away).
+template <bool COUNT = false>
 __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int rows, int cols, int r,
                                             int c, float a, float veg2_p, float bush_p,
                                             const sw100_step* __restrict__ steps, int n,
                                             const uint32_t* __restrict__ bflags, bool bush_any,
-                                            float vmax, float& sh_out, float& veg_out, float& vb_out) {
+                                            float vmax, float& sh_out, float& veg_out, float& vb_out,
+                                            int* ns = nullptr) {
   const bool bushplant = bush_p > 1.f;
   float f = a;
   float sh = 0.f;
@@ -47,6 +51,7 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
     float temp = 0.f, tv = 0.f, tv2 = 0.f, tb = 0.f;
     const bool inb = in_grid(sr, sc, rows, cols);
     if (inb) {
+      if (COUNT) ++*ns;
       const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
       temp = __fsub_rn(v.x, dz);
       tv = __fsub_rn(v.y, dz);
@@ -115,11 +120,11 @@ __device__ __forceinline__ void march_patch(const float4* __restrict__ src4, int
 // passed over 8 at a time (SkipMap, sw_common.cuh).
 // CHECKED false: the caller has shown that every step of the march stays in
 // the grid (the last step's cell is in it; the shifts grow monotonically).
-template <bool CHECKED = true>
+template <bool CHECKED = true, bool COUNT = false>
 __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4, int rows, int cols, int r, int c,
                                                  float a, float veg2_p, const sw100_step* __restrict__ steps, int n,
                                                  float vmax, float& sh_out, float& veg_out, float& vb_out,
-                                                 SkipMap skip = SkipMap{nullptr, 0}) {
+                                                 SkipMap skip = SkipMap{nullptr, 0}, int* ns = nullptr) {
   bool sh = false, vegsh = false, vb_any = false;
   if (n > 0) {
     // first step (index 1 of shadow.py): the trunk-zone rule of :288-293
@@ -127,6 +132,7 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
     const int sr = r + st.dx, sc = c + st.dy;
     float temp = 0.f, tv = 0.f, tv2 = 0.f;
     if (!CHECKED || in_grid(sr, sc, rows, cols)) {
+      if (COUNT) ++*ns;
       const float4 v = __ldg(&src4[(size_t)sr * cols + sc]);
       temp = __fsub_rn(v.x, st.dz);
       tv = __fsub_rn(v.y, st.dz);
@@ -157,6 +163,7 @@ __device__ __forceinline__ void march_patch_fast(const float4* __restrict__ src4
           k += 7;
           continue;
         }
+        if (COUNT) ++*ns;
         const float4 v = __ldg(&src4[(size_t)rr * cols + cc]);
         if (__fsub_rn(v.x, sk.dz) > a) { sh = true; vegsh = false; break; }
         vegsh = vegsh || ((__fsub_rn(v.y, sk.dz) > a) && !(__fsub_rn(v.z, sk.dz) > a));
@@ -285,11 +292,13 @@ __device__ __forceinline__ void load_plan(const sw100_svf_plan* __restrict__ pla
 }
 
 // The 153 patch marches, the sums and the outputs of pixel (r, c).
+// COUNT: also add the source gathers executed to *ns.
+template <bool COUNT = false>
 __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4, int rows, int cols,
                                                 const sw100_svf_plan& plan, const sw100_step* __restrict__ steps,
                                                 const uint32_t* __restrict__ bflags, float vmax,
                                                 float* __restrict__ out, uint32_t* __restrict__ bits, int r, int c,
-                                                SkipMap skip = SkipMap{nullptr, 0}) {
+                                                SkipMap skip = SkipMap{nullptr, 0}, int* ns = nullptr) {
   const size_t npix = (size_t)rows * cols;
   const size_t p = (size_t)r * cols + c;
   const float4 self = src4[p];
@@ -315,13 +324,15 @@ __device__ __forceinline__ void svf_sweep_pixel(const float4* __restrict__ src4,
           inside = in_grid(r + last.dx, c + last.dy, rows, cols);
         }
         if (inside)
-          march_patch_fast<false>(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip);
+          march_patch_fast<false, COUNT>(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip,
+                                         ns);
         else
-          march_patch_fast<true>(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip);
+          march_patch_fast<true, COUNT>(src4, rows, cols, r, c, a, veg2_p, steps + off, n, vmax, sh, veg, vb, skip,
+                                        ns);
       }
     else
-      march_patch(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, n,
-                  bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb);
+      march_patch<COUNT>(src4, rows, cols, r, c, a, veg2_p, bush_p, steps + off, n,
+                         bush_any ? bflags + off : nullptr, bush_any, vmax, sh, veg, vb, ns);
     svf_set_bits(wsh, wveg, wvb, q, n, sh, veg, vb);
     svf_add_patch(A, plan, q, sh, veg, vb);
   }
@@ -366,6 +377,30 @@ __global__ void __launch_bounds__(128, 12) svf_sweep_kernel(
   const int r = blockIdx.y * blockDim.y + threadIdx.y;
   if (r >= rows || c >= cols) return;
   svf_sweep_pixel(src4, rows, cols, plan, steps, bflags, vmax, out, bits, r, c, SkipMap{skipmap, (cols + 7) / 8});
+}
+
+// The same sweep, also counting the source gathers its marches execute
+// (each gathers the 12 bytes dsm / vegdsm / vegdsm2 the survey's step
+// counts are defined on): the algorithmic bytes of a launch are 12 x this
+// count.  Results are identical to svf_sweep_kernel's; the count is
+// reduced per warp and added to *executed with one atomic per warp.
+__global__ void __launch_bounds__(128, 12) svf_sweep_count_kernel(
+    const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
+    const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
+    float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps, const float* __restrict__ skipmap,
+    unsigned long long* __restrict__ executed) {
+  __shared__ sw100_svf_plan plan;
+  load_plan(plan_g, plan, n_steps);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  int ns = 0;
+  if (r < rows && c < cols)
+    svf_sweep_pixel<true>(src4, rows, cols, plan, steps, bflags, vmax, out, bits, r, c,
+                          SkipMap{skipmap, (cols + 7) / 8}, &ns);
+  unsigned long long v = (unsigned long long)ns;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0) atomicAdd(executed, v);
 }
 
 // ------------------------------------------------------------- batches

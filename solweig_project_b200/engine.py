@@ -14,6 +14,7 @@ Layout in HBM (npix = rows * cols):
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
 from dataclasses import dataclass
 
@@ -35,6 +36,9 @@ def require_cuda():
         raise N.NativeUnavailable("no CUDA device: the B200 backend runs on the GPU only")
     N.load()
 
+
+# chunks of the chunked time loop whose device buffers are alive at once
+CHUNKS_IN_FLIGHT = 3
 
 # host <-> device bytes moved by this module (inputs, tables, results)
 TRANSFER = {"h2d": 0, "d2h": 0}
@@ -439,6 +443,17 @@ class DeviceSite:
         N.call("sw100_svf_sweep", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), n_steps,
                _ptr(planes), _ptr(bits), _ptr(ws), ws.numel(), _stream())
 
+    def count_svf_gathers(self, planes, bits, patch_option=2) -> int:
+        """The sweep into caller buffers through the counting kernel: the
+        number of source gathers its marches execute (12 bytes each), for
+        measurement (sw100_svf_sweep_count)."""
+        plan_d, steps_d, n_steps, _, ws = self.svf_tables(patch_option)
+        site = self.site_struct()
+        cnt = torch.zeros(1, dtype=torch.int64, device=self.device)
+        N.call("sw100_svf_sweep_count", C.byref(site), self.rows, self.cols, _ptr(plan_d), _ptr(steps_d), n_steps,
+               _ptr(planes), _ptr(bits), _ptr(ws), ws.numel(), _ptr(cnt), _stream())
+        return int(cnt.item())
+
     def run_svf(self, patch_option=2, exact_statics=False) -> SvfResult:
         d = self.device
         planes = torch.empty((N.SVF_PLANES, self.rows, self.cols), dtype=torch.float32, device=d)
@@ -571,6 +586,10 @@ class DeviceSite:
         stream once the rasters were last written; None: everything queued
         before this call), so it overlaps the SVF sweep and the previous
         chunk's flux loop; the flux loop waits for it on the current stream.
+        Device memory stays bounded whatever the number of steps: at most
+        `CHUNKS_IN_FLIGHT` chunks keep their device buffers (outputs, sun-march
+        records, tables); before an older chunk's buffers are released, the
+        host waits for the event recorded after that chunk's copies.
         Returns ({name: (T, rows, cols) float32 ndarray}, final carried
         scalars)."""
         if self.svf_result is None:
@@ -585,7 +604,7 @@ class DeviceSite:
             mask |= N.OUT_BITS[k]
         n_t = time_stop - time_start
         host = {k: torch.empty((n_t, self.rows, self.cols), dtype=torch.float32, pin_memory=True) for k in names}
-        scalars, keep = initial_scalars, []
+        scalars, ring = initial_scalars, collections.deque()
         main, side = torch.cuda.current_stream(), self.side_stream()
         if rasters_ready is None:
             rasters_ready = torch.cuda.Event()
@@ -594,8 +613,17 @@ class DeviceSite:
         dc = TS.day_chain(met_file, altitude, azimuth, zen, jday, location, time_start, time_stop)
         for t0 in range(time_start, time_stop, chunk_steps):
             t1 = min(time_stop, t0 + chunk_steps)
-            ser = self.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                                    time_start=t0, time_stop=t1, initial_scalars=scalars, day_chain=dc)
+            ser = TS.build_series(met_file=met_file, altitude=altitude, azimuth=azimuth, zen=zen, jday=jday,
+                                  dectime=dectime, altmax=altmax, location=location, scale=self.scale,
+                                  amax=self.amax, rows=self.rows, cols=self.cols, props=self.props,
+                                  params=self.params, time_start=t0, time_stop=t1, initial_scalars=scalars,
+                                  day_chain=dc)
+            if ser.class_idx is not None:
+                # the device planes of this site index the tables by the
+                # cleaned land-cover code (device_props); a per-pixel class
+                # plane from the host would have to be uploaded on the side
+                # stream, which this loop does not do
+                raise RuntimeError("the chunked time loop expects device-side land-cover classes")
             scalars = ser.final
             with torch.cuda.stream(side):
                 s, dev = self.upload_series(ser)
@@ -611,10 +639,18 @@ class DeviceSite:
             for i, k in enumerate(names):
                 host[k][t0 - time_start:t1 - time_start].copy_(out[i], non_blocking=True)
                 TRANSFER["d2h"] += out[i].numel() * out[i].element_size()
-            # every buffer stays referenced until the final synchronize: the
-            # side-stream allocations are read on the current stream
-            keep.append((out, dev, gsrc))
+            # the side-stream allocations are read on the current stream: a
+            # chunk's buffers are released only once the event recorded after
+            # its copies has completed
+            done = torch.cuda.Event()
+            done.record(main)
+            ring.append((done, out, dev, gsrc))
+            if len(ring) > CHUNKS_IN_FLIGHT:
+                old = ring.popleft()
+                old[0].synchronize()
+                del old
         main.synchronize()
+        ring.clear()
         return {k: v.numpy() for k, v in host.items()}, scalars
 
     def load_state(self, state: dict):

@@ -39,3 +39,34 @@ def test_chunked_time_loop_equals_single_launch(cuda, chunk):
         assert np.array_equal(got[k].view(np.uint32), ref[k].view(np.uint32)), (chunk, k)
     assert np.array_equal(b.state.cpu().numpy().view(np.uint32), ref_state.view(np.uint32))
     assert final == ser.final
+
+
+@pytest.mark.gpu
+def test_chunked_time_loop_device_memory_does_not_grow_with_steps(cuda):
+    """Three days of forcing hold no more device memory than one: only a
+    bounded ring of chunks keeps its device buffers."""
+    import torch
+    from solweig_project_b200 import synthetic
+    geo = synthetic.load_sun_geometry("single")
+    met1 = synthetic.make_met(11)
+    loc = dict(synthetic.DEFAULT_LOCATION)
+
+    def days(n):
+        met = np.concatenate([met1] * n)
+        met[:, 1] = np.repeat(met1[0, 1] + np.arange(n), 24)
+        g = {k: np.concatenate([geo[k] + (d if k in ("dectime", "jday") else 0) for d in range(n)], axis=-1)
+             for k in geo}
+        return (met, g["altitude"], g["azimuth"], g["zen"], g["jday"], g["dectime"], g["altmax"], loc)
+
+    peaks = []
+    for n in (1, 3):
+        _, s = _site()
+        s.run_svf()
+        torch.cuda.synchronize()
+        base = torch.cuda.memory_allocated()
+        torch.cuda.reset_peak_memory_stats()
+        out, _ = s.run_chain_chunked(*days(n), requested=("utci", "tmrt"), chunk_steps=4)
+        assert out["tmrt"].shape[0] == 24 * n and np.isfinite(out["tmrt"]).all()
+        peaks.append(torch.cuda.max_memory_allocated() - base)
+        del s
+    assert peaks[1] <= peaks[0] * 1.05 + (1 << 20), peaks

@@ -85,6 +85,45 @@ def test_conv_kernels_match_the_checker(cuda):
 
 
 @pytest.mark.gpu
+def test_conv_wait_timeout_reports_and_leaves_the_context_usable(cuda):
+    """With a wait limit of 0 every pipeline wait of the tensor-core
+    convolution runs out at once: the kernel issues nothing more, drains
+    the MMAs it issued, frees its tensor memory, writes no output and sets
+    err = 1; the context stays usable and the next call (default limit) is
+    correct."""
+    import torch
+    from solweig_project_b200 import _native as N
+    from solweig_project_b200 import engine as E
+    lib = N.load()
+    p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)  # noqa: E731
+    rng = np.random.default_rng(5)
+    n, h, w, cin, cout = 1, 16, 40, 64, 32       # 36 K steps: 9 pipeline stages
+    x = _bf(rng.standard_normal((n, h, w, cin))).cuda()
+    wm = torch.tensor(rng.standard_normal((9, cout, cin)).astype(np.float32) * 0.2, device="cuda")
+    wf = torch.empty(9 * cout * cin, dtype=torch.bfloat16, device="cuda")
+    N.call("sw100_nn_weights", p(wm), cin, cout, p(wf), None, E._stream())
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    y = torch.full((n, h, w, cout), 7.0, dtype=torch.float32, device="cuda")
+    prev = lib.sw100_set_wait_limit(0)
+    try:
+        N.call("sw100_nn_conv3x3_tc", p(x), n, h, w, cin, cin, 0, p(wf), None, cout, p(y), cout, 0, 0, 1, p(err),
+               E._stream())
+        torch.cuda.synchronize()
+    finally:
+        lib.sw100_set_wait_limit(-1)
+    assert prev == 1 << 22
+    assert int(err.item()) == 1
+    assert bool((y == 7.0).all())                    # no output written
+    err.zero_()
+    N.call("sw100_nn_conv3x3_tc", p(x), n, h, w, cin, cin, 0, p(wf), None, cout, p(y), cout, 0, 0, 1, p(err),
+           E._stream())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    wq = _np(wf).reshape(9, cout, cin)
+    assert _rel(_np(y), onn.conv3x3(_np(x), wq, np.zeros(cout))) < 1e-4
+
+
+@pytest.mark.gpu
 def test_pool_up_and_loss_kernels_match_the_checker(cuda):
     import torch
     from solweig_project_b200 import _native as N

@@ -62,6 +62,24 @@ def test_noalloc_sweep_matches_workspace_sweep(cuda, seed, side, dem_level):
         assert np.array_equal(bits, want_b)
 
 
+def test_noalloc_sweep_with_bush_after_other_grids(cuda):
+    """A grid with bush (its step flags live in the shared array and are
+    cleared on every call) swept between calls on a larger grid without bush:
+    every call equals the workspace sweep of its own grid."""
+    from conftest import load_golden
+    from solweig_project_b200.engine import DeviceSite
+    d = load_golden("bush24")
+    bush = DeviceSite(d["dsm"], d["trees"], d["dem"], d["walls_ref"], d["aspect_ref"], float(d["scale"]),
+                      landcover=d["landcover"], lc_class=d["lc_class"], amaxvalue=d["amaxvalue"])
+    assert bush.bush_any
+    other = _site(24, 80)
+    for site in (bush, other, bush):
+        (want_p, want_b), got = _sweep_pair(site)
+        for planes, bits in got:
+            assert np.array_equal(planes.view(np.uint32), want_p.view(np.uint32))
+            assert np.array_equal(bits, want_b)
+
+
 def test_noalloc_sweep_refuses_grids_beyond_its_scratch(cuda):
     from solweig_project_b200 import _native as N
     lib = N.load()

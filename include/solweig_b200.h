@@ -225,6 +225,12 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
                     const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
                     void* workspace, int64_t workspace_bytes, void* stream);
 
+/* Planes 16-18 of an SVF result (svfbuveg, tan(asvf), tan(svfalfa), as the
+ * sweep writes them) from its planes 0 (svf) and 11 (svfveg): for SVF
+ * planes that come from elsewhere (the reference's 19-tuple or a cache,
+ * utci_process.py:864-897).  planes: SW100_SVF_PLANES * npix floats. */
+int sw100_svf_statics(float* planes, int rows, int cols, float trans_veg, void* stream);
+
 /* The same sweep (identical outputs), also counting into *executed (device
  * memory, overwritten) the source gathers its marches execute -- the steps
  * the early exits and the 8-step shortcut leave out are not counted.  Each

@@ -31,7 +31,7 @@ OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDO
             "ldown": OUT_LDOWN, "shadow": OUT_SHADOW}
 
 # Exported symbols (checked by the CPU tests against include/solweig_b200.h)
-SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_count", "sw100_svf_sweep_noalloc", "sw100_pack_cubes",
+SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_count", "sw100_svf_statics", "sw100_svf_sweep_noalloc", "sw100_pack_cubes",
            "sw100_sun_march_workspace_bytes", "sw100_sun_march", "sw100_time_loop_workspace_bytes", "sw100_time_loop",
            "sw100_flux_loop", "sw100_utci", "sw100_abi_version", "sw100_last_error", "sw100_launch_count",
            "sw100_svf_window_workspace_bytes", "sw100_svf_window", "sw100_diff_bbox_workspace_bytes",
@@ -176,6 +176,7 @@ def load(path: str = LIB_PATH):
                                       C.c_int64, vp]),
         "sw100_svf_sweep_count": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp,
                                             C.c_int64, vp, vp]),
+        "sw100_svf_statics": (C.c_int, [vp, C.c_int, C.c_int, C.c_float, vp]),
         "sw100_svf_sweep_noalloc": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp, vp,
                                               vp]),
         "sw100_pack_cubes": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32), vp, vp]),

@@ -75,9 +75,15 @@ def svf_calculator(patch_option, amaxvalue=None, a=None, vegdem=None, vegdem2=No
     return PackedSvf(res) if packed else PackedSvf(res).bundle()
 
 
-def _pack_bundle(site: E.DeviceSite, svf_bundle):
-    """Accept a PackedSvf or the reference's 19-tuple (torch / numpy)."""
+def _pack_bundle(site: E.DeviceSite, svf_bundle, cubes_window=None):
+    """Accept a PackedSvf or the reference's 19-tuple (torch / numpy).
+    ``cubes_window`` = (r0, r1, c0, c1): the tuple's three patch cubes cover
+    only that window of the site (the reference's pre-cropped bundles,
+    utci_process.py:651-663); the site's bit cubes are zero outside it,
+    where no output is kept (a pixel's patch sums read its own cubes only)."""
     if isinstance(svf_bundle, PackedSvf):
+        if cubes_window is not None:
+            raise ValueError("svf_bundle_cubes_cropped=True needs the reference's 19-tuple, not a PackedSvf")
         r = svf_bundle.result
         site.set_svf(r.planes, r.bits, r.single_step)
         return
@@ -90,22 +96,27 @@ def _pack_bundle(site: E.DeviceSite, svf_bundle):
     for k, v in enumerate((svf, svfaveg, svfE, svfEaveg, svfEveg, svfN, svfNaveg, svfNveg, svfS, svfSaveg, svfSveg,
                            svfveg, svfW, svfWaveg, svfWveg, svftotal)):
         planes[k] = torch.as_tensor(_np32(v) if not isinstance(v, torch.Tensor) else v, dtype=torch.float32).to(d)
-    # time-loop statics (utci_process.py:864-897), evaluated like the sweep's epilogue
-    tv = site.params.transVeg
-    planes[16] = planes[0] - (1.0 - planes[11]) * (1.0 - tv)
-    cpu_svf, cpu_veg = planes[0].cpu(), planes[11].cpu()
-    tmp = cpu_svf + cpu_veg - 1.0
-    tmp[tmp < 0.0] = 0.0
-    planes[17] = torch.tan(torch.acos(torch.sqrt(cpu_svf))).to(d)
-    planes[18] = torch.tan(torch.asin(torch.exp(torch.log(1.0 - tmp) / 2.0))).to(d)
+    # time-loop statics (utci_process.py:864-897), on the device as the sweep's epilogue writes them
+    N.call("sw100_svf_statics", E._ptr(planes), site.rows, site.cols, float(site.params.transVeg), E._stream())
     _, _, _, single, _ = site.svf_tables(2)
     cubes = [torch.as_tensor(_np32(c) if not isinstance(c, torch.Tensor) else c, dtype=torch.float32).to(d).contiguous()
              for c in (shmat, vegshmat, vbshvegshmat)]
-    P = cubes[0].shape[2]
-    bits = torch.empty((3, N.CUBE_WORDS, site.rows, site.cols), dtype=torch.int32, device=d)
+    r0, r1, c0, c1 = cubes_window if cubes_window is not None else (0, site.rows, 0, site.cols)
+    crows, ccols, P = cubes[0].shape
+    if (crows, ccols) != (r1 - r0, c1 - c0) or any(tuple(c.shape) != (crows, ccols, P) for c in cubes):
+        raise ValueError(f"patch cubes of shape {tuple(cubes[0].shape)} do not cover the "
+                         f"{'write window' if cubes_window is not None else 'grid'} {(r1 - r0, c1 - c0)}")
     single_c = (C.c_uint32 * N.CUBE_WORDS)(*[int(x) for x in single])
-    N.call("sw100_pack_cubes", E._ptr(cubes[0]), E._ptr(cubes[1]), E._ptr(cubes[2]), site.rows, site.cols, P,
-           single_c, E._ptr(bits), E._stream())
+    if cubes_window is None:
+        bits = torch.empty((3, N.CUBE_WORDS, site.rows, site.cols), dtype=torch.int32, device=d)
+        N.call("sw100_pack_cubes", E._ptr(cubes[0]), E._ptr(cubes[1]), E._ptr(cubes[2]), site.rows, site.cols, P,
+               single_c, E._ptr(bits), E._stream())
+    else:
+        crop = torch.empty((3, N.CUBE_WORDS, crows, ccols), dtype=torch.int32, device=d)
+        N.call("sw100_pack_cubes", E._ptr(cubes[0]), E._ptr(cubes[1]), E._ptr(cubes[2]), crows, ccols, P,
+               single_c, E._ptr(crop), E._stream())
+        bits = torch.zeros((3, N.CUBE_WORDS, site.rows, site.cols), dtype=torch.int32, device=d)
+        bits[:, :, r0:r1, c0:c1] = crop
     site.svf_result = E.SvfResult(planes, bits, np.asarray(single, np.uint32))
     site.t["svfbuveg"], site.t["hsvf"], site.t["tan_alfa"] = planes[16], planes[17], planes[18]
     site.t["bits"] = bits
@@ -152,8 +163,6 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
     elif svf_bundle_cubes_cropped:
         raise ValueError("svf_bundle_cubes_cropped=True requires out_window: the pre-cropped cube extent must "
                          "match a declared write window")
-    if svf_bundle_cubes_cropped:
-        raise NotImplementedError("pre-cropped cube bundles are not supported; pass the full-window bundle")
     if save_wbgt:
         raise NotImplementedError("WBGT is not part of this library")
     if windcoeff_by_dir is not None:
@@ -167,7 +176,7 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
                         landcover=None if landcover_grid is None else _np32(landcover_grid), lc_class=lc_class,
                         windcoeff=None if windcoeff is None else _np32(windcoeff),
                         amaxvalue=None if amaxvalue is None else float(_np32(amaxvalue)), params=params)
-    _pack_bundle(site, svf_bundle)
+    _pack_bundle(site, svf_bundle, cubes_window=out_window if svf_bundle_cubes_cropped else None)
     init_scalars = None
     if initial_state is not None:
         init_scalars = _validate_state(initial_state, rows, cols, time_start, out_window)
@@ -192,9 +201,31 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
         return outputs
     st = site.state_dict()
     final = {k: (v[r0:r1, c0:c1].clone() if out_window is not None else v) for k, v in st.items()}
+    twater = water_temperature(met_file, jday, dectime, time_start, time_stop, landcover_grid is not None,
+                               None if initial_state is None else initial_state.get("Twater"))
     final.update(CI=final_scalars["CI"], firstdaytime=final_scalars["firstdaytime"],
-                 timeadd=final_scalars["timeadd"], Twater=None, next_step=int(time_stop))
+                 timeadd=final_scalars["timeadd"], Twater=twater, next_step=int(time_stop))
     return outputs, final
+
+
+def water_temperature(met_file, jday, dectime, time_start, time_stop, landcover_on, carried=None):
+    """The water temperature the reference carries across steps
+    (utci_process.py:841-846, 917-922): with land cover on, at every
+    midnight row (and the first row) it becomes the mean air temperature of
+    that day's forcing rows; a warm start resumes the carried value (None:
+    not yet established).  Returns a float, or None while not established.
+    Land-cover cleaning maps code 3 (the class whose ground takes it) to 5
+    before the chain runs, so the value never reaches a pixel; it is carried
+    for the state contract."""
+    twater = None if carried is None else float(carried)
+    if not landcover_on:
+        return twater
+    ta = np.asarray(met_file[:, 11], np.float64)
+    day_of = np.asarray(jday)[0]
+    for i in range(time_start, time_stop):
+        if (dectime[i] - np.floor(dectime[i])) == 0 or i == 0:
+            twater = float(np.mean(ta[day_of == np.floor(dectime[i])]))
+    return twater
 
 
 def _validate_state(state, rows, cols, time_start, out_window):

@@ -29,6 +29,7 @@ __global__ void svf_sweep_count_kernel(const float4* src4, int rows, int cols, c
                                        uint32_t* bits, int n_steps, const float* skipmap,
                                        unsigned long long* executed);
 __global__ void svf_skipmap_kernel(const float4* src4, int rows, int cols, float* m, int crow, int ccol);
+__global__ void svf_statics_kernel(float* planes, int64_t npix, float trans_veg);
 __global__ void svf_window_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                   const sw100_step* steps, const int32_t* corridor, float vmax, int4 rect, int4 win,
                                   float* out, uint32_t* bits, int n_steps);
@@ -285,6 +286,16 @@ int sw100_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw1
                     int64_t workspace_bytes, void* stream) {
   return run_svf_sweep(site, rows, cols, plan, steps, n_steps, out_planes, out_bits, workspace, workspace_bytes,
                        nullptr, stream);
+}
+
+int sw100_svf_statics(float* planes, int rows, int cols, float trans_veg, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(planes, "planes"))) return rc;
+  const int64_t npix = (int64_t)rows * cols;
+  const int blocks = (int)std::min<int64_t>((npix + 255) / 256, 148 * 8);
+  svf_statics_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(planes, npix, trans_veg);
+  return check_launch("svf_statics_kernel");
 }
 
 int sw100_svf_sweep_count(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,

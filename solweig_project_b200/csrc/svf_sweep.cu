@@ -216,6 +216,37 @@ __device__ __forceinline__ void svf_set_bits(uint32_t* wsh, uint32_t* wveg, uint
   if (n <= 1 ? (vb == 1.f) : (vb != 0.f)) wvb[q >> 5] |= bit;
 }
 
+// Time-loop statics of a pixel from its svf and svfveg
+// (utci_process.py:864-897): svfbuveg, tan(asvf) with asvf =
+// acos(sqrt(svf)) and tan(svfalfa) with svfalfa = asin(exp(log(1 - tmp) /
+// 2)), tmp = max(svf + svfveg - 1, 0); every float32 operation of the
+// reference rounded once, transcendentals evaluated in double.
+__device__ __forceinline__ void svf_statics(float svf, float veg, float trans_veg, float& buveg, float& hsvf,
+                                            float& tan_alfa) {
+  buveg = svf - (1.f - veg) * (1.f - trans_veg);
+  const float s = (float)sqrt((double)svf);
+  const float asvf = (float)acos((double)s);
+  hsvf = (float)tan((double)asvf);
+  float tmp = svf + veg - 1.f;
+  if (tmp < 0.f) tmp = 0.f;
+  const float lg = (float)log((double)(1.f - tmp));
+  const float ex = (float)exp((double)(lg / 2.f));
+  const float alfa = (float)asin((double)ex);
+  tan_alfa = (float)tan((double)alfa);
+}
+
+// The three statics planes of an SVF result given as planes (a bundle that
+// did not come from this library's sweep): planes 16-18 from planes 0 and 11.
+__global__ void svf_statics_kernel(float* __restrict__ planes, int64_t npix, float trans_veg) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (int64_t)gridDim.x * blockDim.x) {
+    float b, h, t;
+    svf_statics(planes[p], planes[11 * npix + p], trans_veg, b, h, t);
+    planes[16 * npix + p] = b;
+    planes[17 * npix + p] = h;
+    planes[18 * npix + p] = t;
+  }
+}
+
 // Tails, clamps (shadow.py:587-613), the 16 SVF planes, the three
 // time-loop statics and the bit cubes of pixel p.
 __device__ __forceinline__ void svf_finish(SvfAcc& A, const sw100_svf_plan& plan, float veg2_p, size_t p,
@@ -240,18 +271,7 @@ __device__ __forceinline__ void svf_finish(SvfAcc& A, const sw100_svf_plan& plan
                           A.svfS, A.avegS, A.vegS, A.veg,   A.svfW, A.avegW, A.vegW, total};
 #pragma unroll
   for (int k = 0; k < 16; ++k) out[k * npix + p] = vals[k];
-  // time-loop statics (utci_process.py:864-897): every float32 operation of
-  // the reference rounded once; transcendentals evaluated in double
-  out[16 * npix + p] = A.svf - (1.f - A.veg) * (1.f - plan.trans_veg);
-  const float s = (float)sqrt((double)A.svf);
-  const float asvf = (float)acos((double)s);
-  out[17 * npix + p] = (float)tan((double)asvf);
-  float tmp = A.svf + A.veg - 1.f;
-  if (tmp < 0.f) tmp = 0.f;
-  const float lg = (float)log((double)(1.f - tmp));
-  const float ex = (float)exp((double)(lg / 2.f));
-  const float alfa = (float)asin((double)ex);
-  out[18 * npix + p] = (float)tan((double)alfa);
+  svf_statics(A.svf, A.veg, plan.trans_veg, out[16 * npix + p], out[17 * npix + p], out[18 * npix + p]);
 #pragma unroll
   for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
     bits[(0 * SW100_CUBE_WORDS + w) * npix + p] = wsh[w];

@@ -454,43 +454,32 @@ class DeviceSite:
                _ptr(planes), _ptr(bits), _ptr(ws), ws.numel(), _ptr(cnt), _stream())
         return int(cnt.item())
 
-    def run_svf(self, patch_option=2, exact_statics=False) -> SvfResult:
+    def run_svf(self, patch_option=2) -> SvfResult:
         d = self.device
         planes = torch.empty((N.SVF_PLANES, self.rows, self.cols), dtype=torch.float32, device=d)
         bits = torch.empty((3, N.CUBE_WORDS, self.rows, self.cols), dtype=torch.int32, device=d)
         self.launch_svf(planes, bits, patch_option)
         self.svf_result = SvfResult(planes, bits, self.svf_tables(patch_option)[3])
-        self._prepare_loop_statics(exact_statics)
+        self._prepare_loop_statics()
         return self.svf_result
 
-    def set_svf(self, planes, bits, single_step, exact_statics=False):
+    def set_svf(self, planes, bits, single_step):
         """Install an SVF result computed earlier (a cached bundle)."""
         self.svf_result = SvfResult(planes, bits, np.asarray(single_step, np.uint32))
-        self._prepare_loop_statics(exact_statics)
+        self._prepare_loop_statics()
 
-    def _prepare_loop_statics(self, exact=False):
+    def _prepare_loop_statics(self):
         """Per-pixel statics of the time loop derived from the SVF planes:
         svfbuveg (utci_process.py:864), tan(asvf) with asvf = acos(sqrt(svf))
         (utci_process.py:865, solweig.py:550) and tan(svfalfa)
-        (utci_process.py:892-897).  The sweep kernel writes all three (each
-        transcendental rounded once from double); with ``exact`` the two
-        transcendental planes are re-evaluated by torch's CPU kernels, whose
-        rounding is the reference's own."""
+        (utci_process.py:892-897), planes 16-18 of the result (written by
+        the sweep's epilogue, or by sw100_svf_statics for planes that came
+        from elsewhere)."""
         r = self.svf_result
         self.t["svfbuveg"] = r.plane("svfbuveg")
         self.t["bits"] = r.bits
-        if not exact:
-            self.t["hsvf"] = r.plane("hsvf")
-            self.t["tan_alfa"] = r.plane("tan_alfa")
-            return
-        svf = r.plane("svf").detach().to("cpu")
-        svfveg = r.plane("svfveg").detach().to("cpu")
-        hsvf = torch.tan(torch.acos(torch.sqrt(svf)))
-        tmp = svf + svfveg - 1.0
-        tmp[tmp < 0.0] = 0.0
-        tan_alfa = torch.tan(torch.asin(torch.exp(torch.log(1.0 - tmp) / 2.0)))
-        self.t["hsvf"] = hsvf.to(self.device)
-        self.t["tan_alfa"] = tan_alfa.to(self.device)
+        self.t["hsvf"] = r.plane("hsvf")
+        self.t["tan_alfa"] = r.plane("tan_alfa")
 
     # ---------------------------------------------------------- time loop
     def build_series(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, time_start=0,

@@ -271,8 +271,16 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
                        Tgmap1=state["Tgmap1"].copy(), TgOut1=state["TgOut1"].copy())
             capture.append(cap)
     if return_final_state:
+        # water temperature (utci_process.py:841-846, 917-922): with land
+        # cover on, the mean air temperature of the day at every midnight row
+        twater = None if initial_state is None or initial_state.get("Twater") is None \
+            else float(initial_state["Twater"])
+        if landcover == 1:
+            for i in range(time_start, time_stop):
+                if (dectime[i] - np.floor(dectime[i])) == 0 or i == 0:
+                    twater = float(np.mean(Ta_all[jday[0] == np.floor(dectime[i])]))
         final = {k: state[k] for k in STATE_PLANES}
         final.update(CI=float(CI), firstdaytime=float(firstdaytime), timeadd=float(timeadd),
-                     Twater=None, next_step=int(time_stop))
+                     Twater=twater, next_step=int(time_stop))
         return outputs, final
     return outputs

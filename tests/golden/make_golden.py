@@ -245,6 +245,7 @@ def run_case(name, spec, ref):
         out["final_" + k] = _np(final_state[k]).astype(np.float32)
     for k in ("CI", "firstdaytime", "timeadd"):
         out["final_" + k] = np.float64(final_state[k])
+    out["final_Twater"] = np.float64(np.nan if final_state["Twater"] is None else final_state["Twater"])
     T = met.shape[0]
     for k in STEP_PLANES:
         planes = []

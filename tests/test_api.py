@@ -132,6 +132,66 @@ def test_dropins_against_reference(cuda):
     assert_bits_equal(win["shadow"], out["shadow"][:, 5:30, 2:20], "window shadow")
 
 
+@pytest.mark.gpu
+def test_water_temperature_and_warm_start_against_reference(cuda):
+    """final_state["Twater"] is the reference's (utci_process.py:917-922,
+    1085) and a warm start carries it."""
+    d = load_golden("city36")
+    bundle = tuple(d["svf_" + k].astype(np.float32) for k in
+                   ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg", "svfNveg", "svfS",
+                    "svfSaveg", "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg", "vegshmat", "vbshvegshmat",
+                    "shmat", "svftotal"))
+    kw = dict(a=d["dsm"], temp2=d["dem"], walls=d["walls_ref"], dirwalls=d["aspect_ref"], svf_bundle=bundle,
+              met_file=d["met"], altitude=d["altitude"], azimuth=d["azimuth"], zen=d["zen"], jday=d["jday"],
+              dectime=d["dectime"], altmax=d["altmax"], location=golden_location(d), scale=1.0,
+              amaxvalue=d["amaxvalue"], landcover_grid=d["landcover"], lc_class=d["lc_class"],
+              requested_variables=("utci", "tmrt"))
+    out, final = api.run_utci_window(temp1=d["trees"].copy(), return_final_state=True, **kw)
+    assert final["Twater"] == float(d["final_Twater"])
+    assert max_abs(out["tmrt"], d["out_tmrt"]) <= 1e-3
+    first, state = api.run_utci_window(temp1=d["trees"].copy(), time_stop=7, return_final_state=True, **kw)
+    assert state["Twater"] == float(d["final_Twater"])      # established at the first (midnight) row
+    state["Twater"] = None
+    rest, final2 = api.run_utci_window(temp1=d["trees"].copy(), time_start=7, initial_state=state,
+                                       return_final_state=True, **kw)
+    assert final2["Twater"] is None                         # no midnight row in 7..23: stays unestablished
+    assert max_abs(rest["tmrt"], out["tmrt"][7:]) <= 1e-4
+    # without land cover the reference never establishes it
+    nolc = dict(kw, landcover_grid=None, lc_class=None)
+    _, f3 = api.run_utci_window(temp1=d["trees"].copy(), return_final_state=True, **nolc)
+    assert f3["Twater"] is None
+
+
+@pytest.mark.gpu
+def test_pre_cropped_cube_bundle(cuda):
+    """svf_bundle_cubes_cropped=True (the solver's mode,
+    incremental/solver.py:2080; utci_process.py:651-663): cubes cut to the
+    write window give the window of the full-bundle run bit for bit, and the
+    reference's outputs there within the tolerances."""
+    d = load_golden("city36")
+    names = ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg", "svfNveg", "svfS", "svfSaveg",
+             "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg", "vegshmat", "vbshvegshmat", "shmat", "svftotal")
+    full = tuple(d["svf_" + k].astype(np.float32) for k in names)
+    w = (5, 30, 2, 20)
+    cropped = full[:15] + tuple(c[w[0]:w[1], w[2]:w[3], :] for c in full[15:18]) + full[18:]
+    kw = dict(a=d["dsm"], temp2=d["dem"], walls=d["walls_ref"], dirwalls=d["aspect_ref"], met_file=d["met"],
+              altitude=d["altitude"], azimuth=d["azimuth"], zen=d["zen"], jday=d["jday"], dectime=d["dectime"],
+              altmax=d["altmax"], location=golden_location(d), scale=1.0, amaxvalue=d["amaxvalue"],
+              landcover_grid=d["landcover"], lc_class=d["lc_class"], out_window=w,
+              requested_variables=("utci", "tmrt", "shadow", "kdown", "lup"))
+    a = api.run_utci_window(temp1=d["trees"].copy(), svf_bundle=full, **kw)
+    b = api.run_utci_window(temp1=d["trees"].copy(), svf_bundle=cropped, svf_bundle_cubes_cropped=True, **kw)
+    sl = (slice(None), slice(w[0], w[1]), slice(w[2], w[3]))
+    for k in a:
+        assert b[k].shape == (24, w[1] - w[0], w[3] - w[2])
+        assert_bits_equal(b[k], a[k], f"cropped {k}")
+    assert_bits_equal(b["shadow"], d["out_shadow"][sl], "shadow vs reference")
+    assert max_abs(b["tmrt"], d["out_tmrt"][sl]) <= 1e-3
+    assert max_abs(b["utci"], d["out_utci"][sl]) <= 1e-3
+    with pytest.raises(ValueError, match="do not cover"):
+        api.run_utci_window(temp1=d["trees"].copy(), svf_bundle=full, svf_bundle_cubes_cropped=True, **kw)
+
+
 def _utci_f64(ta, rh, tmrt, va):
     """UTCI of calculate_utci.py:259-330 re-evaluated in float64 (the float32
     regression coefficients, every other operation in double), with the
@@ -224,3 +284,15 @@ def test_recompute_utci_steps_equals_a_full_run(cuda):
     idx = [3, 11, 12, 20]
     fast = api.recompute_utci_steps(met2, idx, {i: base["tmrt"][i] for i in idx}, d["dsm"], d["dem"])
     assert_bits_equal(fast, edited["utci"][idx], "utci fast path")
+    # against the CPU oracle (the reference's chain restated) run with the edited forcing
+    from oracle import window as ow
+    names = ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg", "svfNveg", "svfS", "svfSaveg",
+             "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg", "vegshmat", "vbshvegshmat", "shmat", "svftotal")
+    want = ow.run_utci_window(a=d["dsm"], temp1=d["trees"], temp2=d["dem"], walls=d["walls_ref"],
+                              dirwalls=d["aspect_ref"], svf_bundle=tuple(d["svf_" + k].astype(np.float32)
+                                                                          for k in names),
+                              met_file=met2, altitude=d["altitude"], azimuth=d["azimuth"], zen=d["zen"],
+                              jday=d["jday"], dectime=d["dectime"], altmax=d["altmax"],
+                              location=golden_location(d), scale=1.0, amaxvalue=d["amaxvalue"],
+                              landcover_grid=d["landcover"], lc_class=d["lc_class"], requested_variables=("utci",))
+    assert max_abs(fast, want["utci"][idx]) <= 1e-3

@@ -135,6 +135,28 @@ def test_batch_equals_single_site_runs(cuda, tmp_path):
 
     batch.run()
     check("plain")
+    # the first site against the CPU oracle (the reference's chain restated)
+    from golden_util import max_abs
+    from oracle import svf as osvf
+    from oracle import window as ow
+    from solweig_project_b200 import synthetic
+    c = synthetic.make_city(48, 64, seed=3, n_buildings=6, n_trees=6, side_range=(4, 12))
+    geo = synthetic.load_sun_geometry("single")
+    vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(c.dsm, c.trees, c.dem)
+    bundle = osvf.svf_calculator(2, amax, c.dsm, vegdsm, vegdsm2, bush, c.scale)
+    p0, _ = batch.svf(0)
+    p0 = p0.cpu().numpy()
+    for k in range(15):
+        assert np.array_equal(p0[k].view(np.uint32), np.asarray(bundle[k], np.float32).view(np.uint32)), k
+    want = ow.run_utci_window(a=c.dsm, temp1=c.trees, temp2=c.dem, walls=c.walls, dirwalls=c.aspect,
+                              svf_bundle=bundle, met_file=synthetic.make_met(7),
+                              location=dict(synthetic.DEFAULT_LOCATION), scale=c.scale, landcover_grid=c.landcover,
+                              lc_class=synthetic.default_lc_class(), requested_variables=("utci", "tmrt", "shadow"),
+                              **geo)
+    got = {k: v.cpu().numpy() for k, v in batch.outputs(0).items()}
+    assert np.array_equal(got["shadow"].view(np.uint32), want["shadow"].view(np.uint32))
+    assert max_abs(got["tmrt"], want["tmrt"]) <= 1e-3
+    assert max_abs(got["utci"], want["utci"]) <= 1e-3
     for p, b in (batch.svf(i) for i in range(len(sites))):
         p.zero_()
     batch.replay()

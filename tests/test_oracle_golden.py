@@ -54,6 +54,7 @@ def test_oracle_time_loop_bit_exact(case):
         assert_bits_equal(final[k], d["final_" + k], f"{case} final {k}")
     assert final["CI"] == pytest.approx(float(d["final_CI"]), abs=0)
     assert final["timeadd"] == float(d["final_timeadd"])
+    assert final["Twater"] == float(d["final_Twater"])
 
 
 def test_oracle_rejects_unknown_variable():

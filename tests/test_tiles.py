@@ -66,3 +66,18 @@ def test_tiled_batch_equals_single_tile_runs(cuda, tmp_path):
         assert np.array_equal(arr.view(np.uint32), res[key]["utci"].view(np.uint32))
         assert tgt == (gt[0] + c0, 1.0, 0.0, gt[3] - r0, 0.0, -1.0)
         assert md[13]["Time"].startswith("2025-07-01T13:")
+    # one tile against the CPU oracle (the reference's chain restated) run on
+    # that tile's own window, as the reference runs each tile
+    from golden_util import max_abs
+    from oracle import svf as osvf
+    from oracle import window as ow
+    key, r0, r1, c0, c1 = TL.tile_windows(150, 130, 64, 10)[4]
+    sl = (slice(r0, r1), slice(c0, c1))
+    vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(city.dsm[sl], city.trees[sl], city.dem[sl])
+    bundle = osvf.svf_calculator(2, amax, city.dsm[sl], vegdsm, vegdsm2, bush, city.scale)
+    want = ow.run_utci_window(a=city.dsm[sl], temp1=city.trees[sl], temp2=city.dem[sl], walls=city.walls[sl],
+                              dirwalls=city.aspect[sl], svf_bundle=bundle, met_file=met, location=loc,
+                              scale=city.scale, landcover_grid=city.landcover[sl], lc_class=lc,
+                              requested_variables=("utci", "tmrt"), **geo)
+    assert max_abs(res[key]["tmrt"], want["tmrt"]) <= 1e-3
+    assert max_abs(res[key]["utci"], want["utci"]) <= 1e-3

@@ -124,6 +124,34 @@ def test_windowed_recompute_equals_full_sweep(cuda):
 
 
 @pytest.mark.gpu
+def test_windowed_recompute_against_the_oracle(cuda):
+    """One edit checked against the CPU oracle (the reference's
+    svf_calculator restated) run on the edited rasters: the window update's
+    planes and patch cubes are bit-exact."""
+    from golden_util import assert_bits_equal
+    from oracle import svf as osvf
+    from solweig_project_b200.engine import DeviceSite
+    city = _scene(23, 72, 80)
+    amax = F32(48.0)
+    site = DeviceSite(city.dsm, city.trees, city.dem, city.walls, city.aspect, city.scale, amaxvalue=amax)
+    site.run_svf()
+    dsm = city.dsm.copy()
+    dsm[30:41, 35:44] = city.dem[30:41, 35:44] + F32(25.0)
+    assert site.edit_svf(dsm, city.trees, city.dem)["mode"] == "window"
+    vegdsm, vegdsm2, bush, _ = osvf.scene_from_rasters(dsm, city.trees, city.dem)
+    want = osvf.svf_calculator(2, amax, dsm, vegdsm, vegdsm2, bush, city.scale)
+    got = site.svf_result
+    planes = got.planes.cpu().numpy()
+    for k, name in enumerate(osvf.SVF_ORDER[:15]):
+        assert_bits_equal(planes[k], want[k], name)
+    assert_bits_equal(planes[15], want[18], "svftotal")
+    sh, veg, vb = (x.cpu().numpy() for x in got.cubes())
+    assert_bits_equal(veg, np.asarray(want[15], F32), "vegshmat")
+    assert_bits_equal(vb, np.asarray(want[16], F32), "vbshvegshmat")
+    assert_bits_equal(sh, np.asarray(want[17], F32), "shmat")
+
+
+@pytest.mark.gpu
 def test_windowed_recompute_falls_back_to_a_full_sweep(cuda):
     from solweig_project_b200.engine import DeviceSite
     city = _scene(4, 64, 64)

@@ -6,6 +6,8 @@
 * :func:`recompute_utci_steps` <- ``solweig_gpu/utci_process.py:1093-1196``
 * :func:`run_exact_chain`  -- the whole chain for one site from host rasters
   (what ``compute_utci`` does between its raster I/O, utci_process.py:1376-1470)
+* :func:`thermal_comfort`  <- ``solweig_gpu/solweig_gpu.py:500-670`` (rasters
+  on disk -> tiled GeoTIFF outputs; :mod:`solweig_project_b200.comfort`)
 
 All of them run on the CUDA library; there is no CPU path.  A missing GPU or
 library raises :class:`~solweig_project_b200._native.NativeUnavailable`.
@@ -19,8 +21,11 @@ import torch
 
 from . import _native as N
 from . import engine as E
+from . import formats as FM
 from . import tables as T
 from . import timeseries as TS
+
+from .comfort import thermal_comfort  # noqa: E402,F401  (re-exported drop-in)
 
 F32 = np.float32
 VALID_VARIABLES = frozenset({"utci", "tmrt", "kup", "kdown", "lup", "ldown", "shadow", "ta", "wind"})
@@ -50,6 +55,20 @@ class PackedSvf:
         return (*p, veg, vb, sh, r.plane("svftotal"))
 
 
+def _geotransform_of(gdal_dsm, building_dsm_path):
+    """Georeferencing to copy into the cache rasters: a dataset-like object
+    with GetGeoTransform(), a 6-tuple, or the building DSM raster on disk."""
+    if gdal_dsm is not None:
+        if hasattr(gdal_dsm, "GetGeoTransform"):
+            return tuple(gdal_dsm.GetGeoTransform()), None
+        gt = tuple(float(v) for v in gdal_dsm)
+        if len(gt) != 6:
+            raise ValueError("gdal_dsm must be a dataset with GetGeoTransform() or a 6-value geotransform")
+        return gt, None
+    r = FM.read_raster(building_dsm_path)
+    return r.geotransform, r.epsg
+
+
 def svf_calculator(patch_option, amaxvalue=None, a=None, vegdem=None, vegdem2=None, bush=None, scale=None,
                    save_rasters=False, building_dsm_path=None, tree_path=None, dem_path=None, output_dir=None,
                    number=None, gdal_dsm=None, packed=False):
@@ -59,10 +78,38 @@ def svf_calculator(patch_option, amaxvalue=None, a=None, vegdem=None, vegdem2=No
     ``scale`` pixels per metre.  Returns the 19-tuple (svf, svfaveg, svfE,
     svfEaveg, svfEveg, svfN, svfNaveg, svfNveg, svfS, svfSaveg, svfSveg,
     svfveg, svfW, svfWaveg, svfWveg, vegshmat, vbshvegshmat, shmat, SVFtotal)
-    of CUDA tensors, or a :class:`PackedSvf` with ``packed=True``."""
+    of CUDA tensors, or a :class:`PackedSvf` with ``packed=True``.
+
+    ``save_rasters=True`` also writes the reference's cache
+    (shadow.py:100-164, 444-487): ``svfs[_<number>].zip`` (15 GeoTIFFs),
+    ``shadowmats[_<number>].npz`` and ``SkyViewFactor[_<number>].tif`` in
+    ``output_dir``, georeferenced from ``gdal_dsm`` (a dataset with
+    GetGeoTransform() or a geotransform) or the raster at
+    ``building_dsm_path``.  Without the march rasters it reads the building
+    DSM, trees and DEM rasters from the three paths and derives them as
+    compute_utci does (scale = 1 / pixel size)."""
+    geo, epsg = None, None
     if save_rasters:
-        raise NotImplementedError("GeoTIFF/zip cache output is outside this library; "
-                                  "call with save_rasters=False and write the returned planes")
+        if output_dir is None:
+            raise ValueError("When save_rasters=True, output_dir must be provided.")
+        if any(x is None for x in (amaxvalue, a, vegdem, vegdem2, bush, scale)):
+            if building_dsm_path is None or tree_path is None or dem_path is None:
+                raise ValueError("When save_rasters=True and SVF tensors are not provided, "
+                                 "building_dsm_path, tree_path, and dem_path must be provided.")
+            dsm_r = FM.read_raster(building_dsm_path)
+            if dsm_r.geotransform is None:
+                raise ValueError(f"{building_dsm_path} carries no geotransform (the scale comes from it)")
+            a = dsm_r.data
+            trees = FM.read_raster(tree_path).data.copy()
+            dem = FM.read_raster(dem_path).data
+            scale = 1.0 / dsm_r.geotransform[1]
+            vegdem, vegdem2, bush, amaxvalue, _ = E.march_inputs(a, trees, dem)
+            geo, epsg = dsm_r.geotransform, dsm_r.epsg
+        elif gdal_dsm is None and building_dsm_path is None:
+            raise ValueError("When save_rasters=True with precomputed tensors, provide either gdal_dsm or "
+                             "building_dsm_path so GeoTIFF metadata can be copied.")
+        else:
+            geo, epsg = _geotransform_of(gdal_dsm, building_dsm_path)
     required = {"amaxvalue": amaxvalue, "a": a, "vegdem": vegdem, "vegdem2": vegdem2, "bush": bush, "scale": scale}
     missing = [k for k, v in required.items() if v is None]
     if missing:
@@ -72,6 +119,8 @@ def svf_calculator(patch_option, amaxvalue=None, a=None, vegdem=None, vegdem2=No
     site = E.DeviceSite.from_march_rasters(_np32(a), _np32(vegdem), _np32(vegdem2), _np32(bush),
                                            float(_np32(amaxvalue)), float(scale))
     res = site.run_svf(patch_option)
+    if save_rasters:
+        FM.write_svf_cache(output_dir, res.planes, res.cubes(), geo, number=number, epsg=epsg)
     return PackedSvf(res) if packed else PackedSvf(res).bundle()
 
 

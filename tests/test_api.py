@@ -296,3 +296,41 @@ def test_recompute_utci_steps_equals_a_full_run(cuda):
                               location=golden_location(d), scale=1.0, amaxvalue=d["amaxvalue"],
                               landcover_grid=d["landcover"], lc_class=d["lc_class"], requested_variables=("utci",))
     assert max_abs(fast, want["utci"][idx]) <= 1e-3
+
+
+def test_svf_calculator_save_rasters_argument_checks(tmp_path):
+    z = np.zeros((4, 4), np.float32)
+    with pytest.raises(ValueError, match="output_dir must be provided"):
+        api.svf_calculator(2, 1.0, z, z, z, z, 1.0, save_rasters=True)
+    with pytest.raises(ValueError, match="gdal_dsm or building_dsm_path"):
+        api.svf_calculator(2, 1.0, z, z, z, z, 1.0, save_rasters=True, output_dir=str(tmp_path))
+    with pytest.raises(ValueError, match="building_dsm_path, tree_path, and dem_path"):
+        api.svf_calculator(2, save_rasters=True, output_dir=str(tmp_path), building_dsm_path="x.tif")
+
+
+@pytest.mark.gpu
+def test_svf_calculator_writes_the_reference_cache(cuda, tmp_path):
+    """save_rasters=True (shadow.py:100-164, 444-487): the cache it writes
+    holds the reference's planes and cubes bit for bit, georeferenced; the
+    standalone form reads the three rasters and gives the same cache."""
+    from solweig_project_b200 import formats as FM
+    d = load_golden("city36")
+    from oracle.svf import scene_from_rasters
+    vegdsm, vegdsm2, bush, amax = scene_from_rasters(d["dsm"], d["trees"], d["dem"])
+    gt = (600000.0, 1.0, 0.0, 3300000.0, 0.0, -1.0)
+    api.svf_calculator(2, amax, d["dsm"], vegdsm, vegdsm2, bush, 1.0, save_rasters=True,
+                       output_dir=str(tmp_path / "a"), number="0_0", gdal_dsm=gt)
+    for name, tif in (("Building_DSM.tif", d["dsm"]), ("Trees.tif", d["trees"]), ("DEM.tif", d["dem"])):
+        with open(tmp_path / name, "wb") as fh:
+            fh.write(FM.tiff_bytes(tif, gt, epsg=32614))
+    api.svf_calculator(2, save_rasters=True, output_dir=str(tmp_path / "b"), number="0_0",
+                       building_dsm_path=str(tmp_path / "Building_DSM.tif"), tree_path=str(tmp_path / "Trees.tif"),
+                       dem_path=str(tmp_path / "DEM.tif"))
+    for sub in ("a", "b"):
+        planes, (sh, veg, vb) = FM.read_svf_cache(str(tmp_path / sub), number="0_0")
+        for k, v in planes.items():
+            assert_bits_equal(v, d["svf_" + k], f"{sub} {k}")
+        assert_bits_equal(sh, d["svf_shmat"].astype(np.float32), "shmat")
+        assert_bits_equal(veg, d["svf_vegshmat"].astype(np.float32), "vegshmat")
+        assert_bits_equal(vb, d["svf_vbshvegshmat"].astype(np.float32), "vbshvegshmat")
+        assert FM.svf_cache_extent_matches((36, 36), gt, str(tmp_path / sub), number="0_0")

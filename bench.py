@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--side", type=int, default=None, help="override the workload's square side (px)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--timeline", action="store_true",
+                    help="print the host timeline of one end-to-end call (after the bench line)")
     return ap.parse_args()
 
 
@@ -613,6 +615,14 @@ def main():
         e2e_ms = torch.tensor([float(np.median(e2e_times))], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+        if args.timeline and rank == 0:
+            tl = E.Timeline()
+            torch.cuda.synchronize()
+            api.run_exact_chain(dsm=pinned["dsm"].numpy(), trees=pinned["trees"].numpy(), dem=pinned["dem"].numpy(),
+                                walls=pinned["walls"].numpy(), aspect=pinned["aspect"].numpy(), scale=city.scale,
+                                met_file=met, location=loc, landcover=pinned["landcover"].numpy(),
+                                lc_class=lc_class, requested=("utci", "tmrt"), timeline=tl, **geo)
+            timeline_rows = tl.report()
         e2e = {"value": world * npix * N_STEPS_DAY / (float(e2e_ms.item()) / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": float(e2e_ms.item()), "timed_calls": len(e2e_times), "statistic": "median"}
@@ -686,6 +696,11 @@ def main():
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(city, met, geo, lc_class)
         print(json.dumps(line), flush=True)
+        if args.timeline and e2e is not None:
+            print("host timeline of one end-to-end call (ms): phase | host phase | host since start | "
+                  "GPU since start at the phase's end", flush=True)
+            for name, dt, t, gpu in timeline_rows:
+                print(f"  {name:28s} {dt:8.3f} {t:8.3f} {'' if gpu is None else f'{gpu:8.3f}'}", flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

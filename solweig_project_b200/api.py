@@ -353,20 +353,27 @@ def recompute_utci_steps(met_file, time_indices, tmrt_planes, buildings_dsm, dem
 
 def run_exact_chain(*, dsm, trees, dem, walls, aspect, scale, met_file, altitude, azimuth, zen, jday, dectime,
                     altmax, location, landcover=None, lc_class=None, windcoeff=None, requested=("utci", "tmrt"),
-                    model_parameters=None, return_device=False):
+                    model_parameters=None, return_device=False, timeline=None, chunk_steps=8):
     """SVF sweep + time loop for one site from host rasters: the work
     compute_utci does between reading and writing rasters
-    (utci_process.py:1376-1470)."""
+    (utci_process.py:1376-1470).  The time loop runs in chunks of
+    ``chunk_steps`` steps whose host tables are built while the GPU runs the
+    previous chunk; ``timeline`` (an engine.Timeline) records the host
+    phases of the call."""
     requested = _check_variables(requested)
+    tl = timeline if timeline is not None else E.Timeline(enabled=False)
     site = E.DeviceSite(dsm, trees, dem, walls, aspect, scale, landcover=landcover, lc_class=lc_class,
                         windcoeff=windcoeff, params=_model_params(model_parameters))
+    tl.mark("upload + prepare site", torch.cuda.current_stream())
     rasters_ready = torch.cuda.Event()   # the sun marches need the rasters only, not the SVF
     rasters_ready.record()
     site.run_svf()
+    tl.mark("svf tables + sweep launch", torch.cuda.current_stream())
     if return_device:
         ser = site.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location)
         return site.run_time_loop(ser, requested=[k for k in N.OUT_BITS if k in requested])
     # host tables of later steps are built while the GPU runs earlier ones
     out, _ = site.run_chain_chunked(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                                    requested=requested, rasters_ready=rasters_ready)
+                                    requested=requested, rasters_ready=rasters_ready, timeline=timeline,
+                                    chunk_steps=chunk_steps)
     return out

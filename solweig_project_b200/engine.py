@@ -37,6 +37,42 @@ def require_cuda():
     N.load()
 
 
+class Timeline:
+    """Host phases of a call: mark(name) stamps the end of a phase
+    (time.perf_counter); with a stream, a CUDA event is recorded there too,
+    so the GPU's progress at that point can be read afterwards."""
+
+    def __init__(self, enabled=True):
+        import time
+        self.enabled = enabled
+        self._clock = time.perf_counter
+        self.t0 = self._clock() if enabled else 0.0
+        self.marks = []
+        self.start_event = None
+        if enabled and torch.cuda.is_available():
+            self.start_event = torch.cuda.Event(enable_timing=True)
+            self.start_event.record()
+
+    def mark(self, name, stream=None):
+        if not self.enabled:
+            return
+        ev = None
+        if stream is not None:
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(stream)
+        self.marks.append((name, self._clock(), ev))
+
+    def report(self):
+        """[(phase, host ms since the previous mark, host ms since the
+        start, GPU ms since the start at the recorded event or None)]."""
+        out, prev = [], self.t0
+        for name, t, ev in self.marks:
+            gpu = self.start_event.elapsed_time(ev) if ev is not None and self.start_event is not None else None
+            out.append((name, (t - prev) * 1e3, (t - self.t0) * 1e3, gpu))
+            prev = t
+        return out
+
+
 # chunks of the chunked time loop whose device buffers are alive at once
 CHUNKS_IN_FLIGHT = 3
 
@@ -494,14 +530,26 @@ class DeviceSite:
         return ser
 
     def upload_series(self, ser: TS.Series):
-        d = self.device
-        dev = {"steps": _table(ser.steps, d), "sun": _table(ser.sun, d), "sun_table": _table(ser.sun_table, d),
-               "patch": _table(ser.patch, d), "gvf": _table(ser.gvf, d)}
+        """The five tables of a series in one page-locked buffer and one
+        host-to-device copy (each table 256-byte aligned); returns the
+        Series record of device pointers and the device buffer."""
+        parts = [np.ascontiguousarray(a).view(np.uint8).reshape(-1)
+                 for a in (ser.steps, ser.sun, ser.sun_table, ser.patch, ser.gvf)]
+        offs, total = [], 0
+        for a in parts:
+            offs.append(total)
+            total += (max(a.size, 16) + 255) // 256 * 256
+        host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        hv = host.numpy()
+        for a, o in zip(parts, offs):
+            hv[o:o + a.size] = a
+        TRANSFER["h2d"] += total
+        dev = host.to(self.device, non_blocking=True)
+        base = dev.data_ptr()
         s = N.Series()
-        s.steps, s.sun, s.sun_table = dev["steps"].data_ptr(), dev["sun"].data_ptr(), dev["sun_table"].data_ptr()
-        s.patch, s.gvf = dev["patch"].data_ptr(), dev["gvf"].data_ptr()
+        s.steps, s.sun, s.sun_table, s.patch, s.gvf = (base + o for o in offs)
         s.n_t, s.n_day, s.n_patches = len(ser.steps), len(ser.sun), ser.patch.shape[1]
-        return s, dev
+        return s, {"tables": dev, "staging": host}
 
     def run_time_loop(self, ser: TS.Series, requested=("utci",), series_dev=None, workspace=None):
         """All steps of the series in one library call; returns
@@ -552,6 +600,12 @@ class DeviceSite:
         N.call("sw100_flux_loop", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc),
                _ptr(self.state), out_mask, _ptr(outputs), _stream())
 
+    def copy_stream(self) -> torch.cuda.Stream:
+        """Stream of the chunked loop's device-to-host output copies."""
+        if getattr(self, "_copy", None) is None:
+            self._copy = torch.cuda.Stream(device=self.device)
+        return self._copy
+
     def side_stream(self) -> torch.cuda.Stream:
         """Second stream of this site: sun marches, which read only the
         rasters, run there beside the SVF sweep and the flux loops."""
@@ -561,7 +615,7 @@ class DeviceSite:
 
     def run_chain_chunked(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
                           requested=("utci",), time_start=0, time_stop=None, initial_scalars=None, chunk_steps=8,
-                          rasters_ready=None):
+                          rasters_ready=None, timeline=None):
         """The time loop of steps [time_start, time_stop) with the host tables
         built chunk by chunk while the GPU works: the tables of `chunk_steps`
         steps are built, their sun march and flux loop launched and their
@@ -575,6 +629,7 @@ class DeviceSite:
         stream once the rasters were last written; None: everything queued
         before this call), so it overlaps the SVF sweep and the previous
         chunk's flux loop; the flux loop waits for it on the current stream.
+        `timeline` (a Timeline, optional) records the host phases.
         Device memory stays bounded whatever the number of steps: at most
         `CHUNKS_IN_FLIGHT` chunks keep their device buffers (outputs, sun-march
         records, tables); before an older chunk's buffers are released, the
@@ -594,12 +649,14 @@ class DeviceSite:
         n_t = time_stop - time_start
         host = {k: torch.empty((n_t, self.rows, self.cols), dtype=torch.float32, pin_memory=True) for k in names}
         scalars, ring = initial_scalars, collections.deque()
-        main, side = torch.cuda.current_stream(), self.side_stream()
+        main, side, copy = torch.cuda.current_stream(), self.side_stream(), self.copy_stream()
         if rasters_ready is None:
             rasters_ready = torch.cuda.Event()
             rasters_ready.record(main)
         side.wait_event(rasters_ready)
+        tl = timeline if timeline is not None else Timeline(enabled=False)
         dc = TS.day_chain(met_file, altitude, azimuth, zen, jday, location, time_start, time_stop)
+        tl.mark("day chain")
         for t0 in range(time_start, time_stop, chunk_steps):
             t1 = min(time_stop, t0 + chunk_steps)
             ser = TS.build_series(met_file=met_file, altitude=altitude, azimuth=azimuth, zen=zen, jday=jday,
@@ -614,6 +671,7 @@ class DeviceSite:
                 # stream, which this loop does not do
                 raise RuntimeError("the chunked time loop expects device-side land-cover classes")
             scalars = ser.final
+            tl.mark(f"tables {t0}-{t1}")
             with torch.cuda.stream(side):
                 s, dev = self.upload_series(ser)
                 gsrc = torch.empty((max(1, s.n_day), self.rows, self.cols, 4), dtype=torch.float32,
@@ -625,20 +683,28 @@ class DeviceSite:
             main.wait_event(marched)
             out = torch.empty((len(names), t1 - t0, self.rows, self.cols), dtype=torch.float32, device=self.device)
             self.launch_flux_loop(s, gsrc, mask, out)
-            for i, k in enumerate(names):
-                host[k][t0 - time_start:t1 - time_start].copy_(out[i], non_blocking=True)
-                TRANSFER["d2h"] += out[i].numel() * out[i].element_size()
-            # the side-stream allocations are read on the current stream: a
-            # chunk's buffers are released only once the event recorded after
-            # its copies has completed
+            # outputs go back on a copy stream, overlapping the next chunk
+            fluxed = torch.cuda.Event()
+            fluxed.record(main)
+            copy.wait_event(fluxed)
+            with torch.cuda.stream(copy):
+                for i, k in enumerate(names):
+                    host[k][t0 - time_start:t1 - time_start].copy_(out[i], non_blocking=True)
+                    TRANSFER["d2h"] += out[i].numel() * out[i].element_size()
+            # the side-stream allocations are read on the current stream and
+            # `out` on the copy stream: a chunk's buffers are released only
+            # once the event recorded after its copies has completed
             done = torch.cuda.Event()
-            done.record(main)
+            done.record(copy)
             ring.append((done, out, dev, gsrc))
+            tl.mark(f"launch {t0}-{t1}", main)
             if len(ring) > CHUNKS_IN_FLIGHT:
                 old = ring.popleft()
                 old[0].synchronize()
                 del old
         main.synchronize()
+        copy.synchronize()
+        tl.mark("wait for the GPU")
         ring.clear()
         return {k: v.numpy() for k, v in host.items()}, scalars
 

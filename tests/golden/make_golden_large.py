@@ -1,7 +1,9 @@
 """Reference pins at the benchmark sizes: the 200 x 200 and 500 x 500 seeded
-cities (the 500 x 500 one is the city ``bench.py`` times), 24 hourly steps.
+cities (the 500 x 500 one is the city ``bench.py`` times), three sites of
+the 64-site batched workload and a 512 x 512 city of the 4096 x 4096 tile's
+generator (buildings up to 120 m), 24 hourly steps.
 
-    python tests/golden/make_golden_large.py --ref <reference checkout> [--cases c1_200 c2_500]
+    python tests/golden/make_golden_large.py --ref <reference checkout> [--cases c1_200 c2_500 ...]
 
 (``--ref`` may be replaced by the environment variable ``SOLWEIG_REFERENCE``.)
 
@@ -55,10 +57,17 @@ sys.path.insert(0, HERE)
 from make_golden import SVF_NAMES, install_stubs, reference_path  # noqa: E402
 from solweig_project_b200 import synthetic  # noqa: E402
 
-# name: (side, seed, h_max)
+# name: (side, seed, h_max) of a single-site city at lat 30.3 / lon -97.7, or
+# ("multi", i): site i of the 64-site batched workload (its own seed,
+# density, canopy cover, latitude and forcing)
 CASES = {
     "c1_200": (200, 1234, 40.0),
     "c2_500": (500, 1234, 40.0),
+    "c3_site37": ("multi", 37),
+    "c3_site47": ("multi", 47),
+    "c3_site17": ("multi", 17),
+    # the 4096 x 4096 tile's generator (buildings up to 120 m) at 512 x 512
+    "c4_proxy512": (512, 1234, 120.0),
 }
 N_GROUND = 4096
 N_BUILDING = 256
@@ -102,7 +111,20 @@ class _Float64Torch:
         return getattr(self._torch, name)
 
 
-def run_case(name, side, seed, h_max, ref):
+def make_case_inputs(spec):
+    """(city, met, location) of a case spec (see CASES)."""
+    if spec[0] == "multi":
+        sp = synthetic.multi_site_specs()[spec[1]]
+        city = synthetic.make_city(sp["side"], sp["side"], seed=sp["seed"], density=sp["density"],
+                                   canopy_cover=sp["canopy"], with_walls=False)
+        loc = {"latitude": sp["latitude"], "longitude": sp["longitude"], "altitude": 3.0}
+        return city, synthetic.make_met(sp["seed"]), loc, sp["seed"]
+    side, seed, h_max = spec
+    city = synthetic.make_city(side, side, seed=seed, h_max=h_max, with_walls=False)
+    return city, synthetic.make_met(seed), dict(synthetic.DEFAULT_LOCATION), seed
+
+
+def run_case(name, spec, ref):
     import torch
     import solweig_gpu.calculate_utci as rcu
     import solweig_gpu.shadow as rshadow
@@ -111,10 +133,12 @@ def run_case(name, side, seed, h_max, ref):
     import solweig_gpu.utci_process as rup
     import solweig_gpu.walls_aspect as rwa
 
-    city = synthetic.make_city(side, side, seed=seed, h_max=h_max, with_walls=False)
-    rows = cols = side
+    city, met, loc, seed = make_case_inputs(spec)
+    rows, cols = city.shape
     scale = 1.0
-    out = {"side": side, "seed": seed, "h_max": h_max}
+    out = {"spec": np.array([str(x) for x in spec]), "seed": seed}
+    if spec[0] != "multi":
+        out.update(side=spec[0], h_max=spec[2])
     t0 = time.time()
     walls = rwa.findwalls(city.dsm, 3.0).astype(np.float32)
     aspect = rwa.filter1Goodwin_as_aspect_v3(walls.astype(np.float64), scale, city.dsm).astype(np.float32)
@@ -123,14 +147,13 @@ def run_case(name, side, seed, h_max, ref):
                  ("walls", walls), ("aspect", aspect)):
         out["digest_in_" + k] = digest(v)
 
-    met = synthetic.make_met(seed)
-    loc = dict(synthetic.DEFAULT_LOCATION)
     _, altitude, azimuth, zen, jday, _, dectime, altmax = rsun.Solweig_2015a_metdata_noload(
         met, loc, synthetic.DEFAULT_UTC)
     geo = dict(altitude=altitude, azimuth=azimuth, zen=zen, jday=jday, dectime=dectime, altmax=altmax)
     for k, v in geo.items():
         out[k] = np.asarray(v, np.float64)
     out["met"] = met
+    out["latitude"], out["longitude"], out["site_altitude"] = loc["latitude"], loc["longitude"], loc["altitude"]
     lc_class = np.loadtxt(os.path.join(ref, "solweig_gpu", "landcoverclasses_2016a.txt"),
                           skiprows=1, usecols=range(1, 7))
 
@@ -276,8 +299,7 @@ def main():
     import torch
     torch.set_num_threads(max(1, os.cpu_count() or 1))
     for name in args.cases:
-        side, seed, h_max = CASES[name]
-        data = run_case(name, side, seed, h_max, ref)
+        data = run_case(name, CASES[name], ref)
         path = os.path.join(HERE, f"large_{name}.npz")
         np.savez_compressed(path, **data)
         print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)", flush=True)

@@ -31,7 +31,10 @@ from conftest import GOLDEN
 
 TMRT_TOL = 1e-3    # K
 UTCI_TOL = 1e-3    # C
-LARGE_CASES = ("c1_200", "c2_500")
+# 200 x 200 and 500 x 500 (the benchmarked city), three sites of the 64-site
+# batched workload and a 512 x 512 city of the 4096 x 4096 tile's generator
+# (buildings up to 120 m)
+LARGE_CASES = ("c1_200", "c2_500", "c3_site37", "c3_site47", "c3_site17", "c4_proxy512")
 SVF_ORDER = ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg", "svfNveg", "svfS", "svfSaveg",
              "svfSveg", "svfveg", "svfW", "svfWaveg", "svfWveg")
 LOCATION = {"latitude": 30.3, "longitude": -97.7, "altitude": 3.0}
@@ -48,11 +51,29 @@ def digest(a, dtype=np.float32):
     return hashlib.sha256(a.tobytes()).hexdigest()
 
 
+def _multi_index(d):
+    spec = [str(x) for x in d["spec"]] if "spec" in d else []
+    return int(spec[1]) if spec and spec[0] == "multi" else None
+
+
 def make_inputs(d):
     from solweig_project_b200 import synthetic
-    side = int(d["side"])
-    city = synthetic.make_city(side, side, seed=int(d["seed"]), h_max=float(d["h_max"]))
+    i = _multi_index(d)
+    if i is not None:
+        sp = synthetic.multi_site_specs()[i]
+        city = synthetic.make_city(sp["side"], sp["side"], seed=sp["seed"], density=sp["density"],
+                                   canopy_cover=sp["canopy"])
+    else:
+        side = int(d["side"])
+        city = synthetic.make_city(side, side, seed=int(d["seed"]), h_max=float(d["h_max"]))
     return city, synthetic.default_lc_class()
+
+
+def location(d):
+    if "latitude" in d:
+        return {"latitude": float(d["latitude"]), "longitude": float(d["longitude"]),
+                "altitude": float(d["site_altitude"])}
+    return dict(LOCATION)
 
 
 def error_stats(got, want):
@@ -74,7 +95,8 @@ def test_generator_reproduces_reference_inputs(case):
 def test_sun_geometry_of_fixture_is_the_workloads(case):
     from solweig_project_b200 import synthetic
     d = load_large(case)
-    geo = synthetic.load_sun_geometry("single")
+    i = _multi_index(d)
+    geo = synthetic.load_sun_geometry("single" if i is None else f"multi{i}")
     for k, v in geo.items():
         assert np.array_equal(v, d[k]), k
     assert np.array_equal(synthetic.make_met(int(d["seed"])), d["met"])
@@ -100,7 +122,7 @@ class _Run:
                           landcover=city.landcover, lc_class=lc_class)
         self.res = site.run_svf()
         self.ser = site.build_series(d["met"], d["altitude"], d["azimuth"], d["zen"], d["jday"], d["dectime"],
-                                     d["altmax"], LOCATION)
+                                     d["altmax"], location(d))
         _, dbg = site.run_sun_march(self.ser)
         self.march = dbg.cpu().numpy()
         out = site.run_time_loop(self.ser, requested=("utci", "tmrt", "shadow"))
@@ -121,7 +143,7 @@ def test_large_svf_bit_exact(case, cuda):
             pytest.fail(f"{case} {name}: digest differs (max |diff| at the sample pixels {diff.max():.3g})")
     assert digest(r.planes[15]) == str(d["digest_svf_svftotal"]), "svftotal"
     assert not r.single.any()          # no one-step patches on these grids: the cubes are 0/1
-    rows = cols = int(d["side"])
+    rows, cols = r.planes.shape[1:]
     for c, name in enumerate(("shmat", "vegshmat", "vbshvegshmat")):
         # word-planar 32-bit words -> per pixel little-endian bytes = packbits(little) along the patch axis
         packed = np.ascontiguousarray(r.words[c].transpose(1, 2, 0)).view(np.uint8).reshape(rows, cols, 20)
@@ -187,7 +209,7 @@ def test_large_chain_drop_in_call(case, cuda):
     city, lc_class = make_inputs(d)
     geo = {k: d[k] for k in ("altitude", "azimuth", "zen", "jday", "dectime", "altmax")}
     out = api.run_exact_chain(dsm=city.dsm, trees=city.trees, dem=city.dem, walls=city.walls, aspect=city.aspect,
-                              scale=city.scale, met_file=d["met"], location=dict(synthetic.DEFAULT_LOCATION),
+                              scale=city.scale, met_file=d["met"], location=location(d),
                               landcover=city.landcover, lc_class=lc_class,
                               requested=("utci", "tmrt", "shadow"), **geo)
     _check_outputs(case, d, out["tmrt"], out["utci"], out.get("shadow"), "run_exact_chain")

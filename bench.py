@@ -545,6 +545,8 @@ def main():
     mask = N.OUT_UTCI | N.OUT_TMRT
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream()
+    from solweig_project_b200 import engine as E
+    sums = torch.empty((N_STEPS_DAY, 4, rows, cols), dtype=torch.float32, device=dev) if E.TENSOR_SUMS else None
 
     def step(ev=None):
         if ev is not None:
@@ -555,8 +557,12 @@ def main():
         site.launch_sun_march(series, gsrc)
         if ev is not None:
             ev[2].record(stream)
+        if sums is not None:
+            site.launch_patch_sums(series, sums)
+        if ev is not None:
+            ev[4].record(stream)
         site.state.zero_()
-        site.launch_flux_loop(series, gsrc, mask, outputs)
+        site.launch_flux_loop(series, gsrc, mask, outputs, sums=sums)
         if ev is not None:
             ev[3].record(stream)
 
@@ -567,7 +573,7 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    events = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
     launches0 = N.launch_count()
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
@@ -576,9 +582,11 @@ def main():
             step(events[k])
         torch.cuda.synchronize()
     launches = N.launch_count() - launches0
+    site.check_tensor_error()
     svf_ms = [e[0].elapsed_time(e[1]) for e in events]
     march_ms = [e[1].elapsed_time(e[2]) for e in events]
-    loop_ms = [e[2].elapsed_time(e[3]) for e in events]
+    sums_ms = [e[2].elapsed_time(e[4]) for e in events]
+    loop_ms = [e[4].elapsed_time(e[3]) for e in events]
     step_ms = sum(e[0].elapsed_time(e[3]) for e in events) / args.steps
     t_max = torch.tensor([step_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -632,6 +640,7 @@ def main():
         loop_t = sum(loop_ms) / len(loop_ms)
         svf_t = sum(svf_ms) / len(svf_ms)
         march_t = sum(march_ms) / len(march_ms)
+        sums_t = sum(sums_ms) / len(sums_ms)
         from solweig_project_b200.synthetic import DEFAULT_LOCATION  # noqa: F401
         peaks = {}
         try:
@@ -647,6 +656,11 @@ def main():
                           "active_lanes_ncu": NCU_ACTIVE_LANES["svf_sweep"]},
             "sun_march": {"ms": march_t, "issue_active_frac_ncu": NCU_ISSUE_ACTIVE["sun_march"],
                           "active_lanes_ncu": NCU_ACTIVE_LANES["sun_march"]},
+            "patch_sums_tc": {"ms": sums_t,
+                              "tflops_bf16": (2.0 * npix * 640 * 96 * ((N_STEPS_DAY + 7) // 8) / (sums_t * 1e9)
+                                              if sums is not None and sums_t > 0 else None),
+                              "note": "dense 153-patch sums as a one-hot x weight product on tcgen05 (BF16 in 3 "
+                                      "parts, FP32 accumulate); includes the weight split kernel"},
             "flux_loop": {"ms": loop_t,
                           "gbs_compulsory": FLUX_BYTES_PER_PX_STEP * npix * N_STEPS_DAY / (loop_t * 1e6),
                           "issue_active_frac_ncu": NCU_ISSUE_ACTIVE["flux_loop"],

@@ -545,6 +545,32 @@ int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw1
 int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
                     const float* gsrc, float* state, uint32_t out_mask, float* outputs, void* stream);
 
+/* The dense 153-patch sums of the time loop on the tensor cores
+ * (solweig.py:683-724 diffuse Kside and anisotropic luminance,
+ * :1514-1541 sky longwave): for every step t of the series and pixel p,
+ *   sums[(t * 4 + 0) * npix + p] = diffuse Kside (0 at night),
+ *   sums[(t * 4 + 1) * npix + p] = anisotropic luminance sum (0 at night),
+ *   sums[(t * 4 + 2) * npix + p] = sky longwave down,
+ *   sums[(t * 4 + 3) * npix + p] = sky longwave side,
+ * as a product of the pixel's one-hot (sh, vegsh) patch codes (from
+ * site->bits) with the series' per-patch increments, each split into three
+ * bf16 parts that add up to the float32 increment; FP32 accumulation
+ * (tcgen05.mma, accumulator in tensor memory).  The sums equal the
+ * reference's patch-ordered float32 sums to about one rounding.
+ * `err` (device int32, may be NULL) is set to 1 when a bounded wait of the
+ * kernel expired (then the block writes nothing), 2 when its drain did too.
+ * Workspace: sw100_patch_sums_workspace_bytes (the bf16 weights). */
+int sw100_patch_sums_workspace_bytes(int n_t, int64_t* bytes);
+int sw100_patch_sums(const sw100_site_planes* site, int rows, int cols, const sw100_series* series, float* sums,
+                     int32_t* err, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* sw100_flux_loop with the dense patch sums taken from `sums` (as written
+ * by sw100_patch_sums for the same series) instead of computed in the
+ * loop. */
+int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
+                         const float* gsrc, const float* sums, float* state, uint32_t out_mask, float* outputs,
+                         void* stream);
+
 /* ---------------------------------------------------------------- UTCI -- */
 /* ---------------------------------------------------- learned preview -- */
 /* Kernels of the learned SVF preview (a small U-Net, BF16 on the tensor

@@ -39,7 +39,8 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_coun
            "sw100_batch_skipmap", "sw100_batch_svf", "sw100_batch_sun_march", "sw100_batch_flux_loop",
            "sw100_utci_steps", "sw100_nn_conv3x3_wgrad", "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2",
            "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc",
-           "sw100_prepare_site", "sw100_march_tables", "sw100_set_wait_limit")
+           "sw100_prepare_site", "sw100_march_tables", "sw100_set_wait_limit",
+           "sw100_patch_sums_workspace_bytes", "sw100_patch_sums", "sw100_flux_loop_sums")
 ABI_VERSION = 2  # SW100_ABI_VERSION of include/solweig_b200.h
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
@@ -188,6 +189,11 @@ def load(path: str = LIB_PATH):
                                       vp, vp, C.c_int64, vp]),
         "sw100_flux_loop": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, C.c_uint32,
                                       vp, vp]),
+        "sw100_patch_sums_workspace_bytes": (C.c_int, [C.c_int, i64p]),
+        "sw100_patch_sums": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, vp,
+                                       C.c_int64, vp]),
+        "sw100_flux_loop_sums": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, vp,
+                                           C.c_uint32, vp, vp]),
         "sw100_utci": (C.c_int, [vp, vp, vp, vp, C.c_int64, vp, vp]),
         "sw100_svf_window_workspace_bytes": (C.c_int, [C.c_int, C.c_int, i64p]),
         "sw100_svf_window": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, vp, C.c_int, vp,

@@ -22,7 +22,8 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(REPO, "include")
 LIB_NAME = "libsolweig_b200.so"
 LIB_PATH = os.path.join(PKG, LIB_NAME)
-SOURCES = ("api.cu", "prepare.cu", "svf_sweep.cu", "sun_march.cu", "time_loop.cu", "utci.cu", "nn.cu")
+SOURCES = ("api.cu", "prepare.cu", "svf_sweep.cu", "sun_march.cu", "time_loop.cu", "utci.cu", "nn.cu",
+           "patch_sums.cu")
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "--prec-div=true", "--prec-sqrt=true",
          "--ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-Xptxas", "-v"]

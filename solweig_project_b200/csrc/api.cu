@@ -52,6 +52,14 @@ __global__ void time_loop_kernel(SitePlanes site, int rows, int cols, const sw10
                                  const sw100_patch_step* patch_steps, int n_patches,
                                  const sw100_gvf_azimuth* gvf_az, const float4* gsrc, int n_day, float* state,
                                  uint32_t out_mask, float* outputs);
+__global__ void time_loop_sums_kernel(SitePlanes site, int rows, int cols, const sw100_time_step* tsteps, int n_t,
+                                      const sw100_patch_step* patch_steps, int n_patches,
+                                      const sw100_gvf_azimuth* gvf_az, const float4* gsrc, int n_day, float* state,
+                                      uint32_t out_mask, float* outputs, const float* sums);
+__global__ void patch_weights_kernel(const sw100_time_step* steps, int n_t, const sw100_patch_step* patch,
+                                     int n_patches, __nv_bfloat16* W, int n_groups);
+__global__ void patch_sums_tc_kernel(const uint32_t* bits, int64_t npix, int n_patches, const __nv_bfloat16* W,
+                                     int n_groups, int n_t, float* sums, int* err, int wait_limit);
 __global__ void pack_cubes_kernel(const float* sh, const float* veg, const float* vb, size_t npix, int n_patches,
                                   Single5 single, uint32_t* bits);
 __global__ void utci_steps_kernel(const sw100_time_step* steps, int n_steps, const float* tmrt,
@@ -624,6 +632,70 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
       make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
       reinterpret_cast<const float4*>(gsrc), series->n_day, state, out_mask, outputs);
   return check_launch("time_loop_kernel");
+}
+
+int sw100_patch_sums_workspace_bytes(int n_t, int64_t* bytes) {
+  int rc;
+  if ((rc = check_ptr(bytes, "bytes"))) return rc;
+  if (n_t < 0) return fail(SW100_E_ARG, "n_t must be >= 0");
+  *bytes = align_up((int64_t)((n_t + 7) / 8) * 96 * 640 * 2);
+  return 0;
+}
+
+int sw100_patch_sums(const sw100_site_planes* site, int rows, int cols, const sw100_series* series, float* sums,
+                     int32_t* err, void* workspace, int64_t workspace_bytes, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_loop(site))) return rc;
+  if ((rc = validate_series(series))) return rc;
+  if ((rc = check_ptr(sums, "sums"))) return rc;
+  if (series->n_patches > 160) return fail(SW100_E_ARG, "at most 160 patches (n_patches %d)", series->n_patches);
+  int64_t need = 0;
+  if ((rc = sw100_patch_sums_workspace_bytes(series->n_t, &need))) return rc;
+  if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
+  if (series->n_t == 0) return 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int n_groups = (series->n_t + 7) / 8;
+  __nv_bfloat16* W = static_cast<__nv_bfloat16*>(workspace);
+  const int64_t nw = (int64_t)n_groups * 96 * 640;
+  patch_weights_kernel<<<(unsigned)std::min<int64_t>((nw + 255) / 256, 148 * 8), 256, 0, st>>>(
+      series->steps, series->n_t, series->patch, series->n_patches, W, n_groups);
+  if ((rc = check_launch("patch_weights_kernel"))) return rc;
+  const int smem = 2 * (16384 + 12288);   // two stages of A (16 KB) and B (12 KB) chunks
+  // the attributes are per function and process: set them once (the largest
+  // shared-memory carveout, so that several 56 KB CTAs share an SM)
+  static std::once_flag attr_once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(attr_once, [&] {
+    attr_err = cudaFuncSetAttribute(patch_sums_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (attr_err == cudaSuccess)
+      attr_err = cudaFuncSetAttribute(patch_sums_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared);
+  });
+  if (attr_err != cudaSuccess) return fail((int)attr_err, "cudaFuncSetAttribute: %s", cudaGetErrorString(attr_err));
+  const int64_t npix = (int64_t)rows * cols;
+  patch_sums_tc_kernel<<<(unsigned)((npix + 127) / 128), 128, smem, st>>>(
+      site->bits, npix, series->n_patches, W, n_groups, series->n_t, sums, err, g_tc_wait_limit.load());
+  return check_launch("patch_sums_tc_kernel");
+}
+
+int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
+                         const float* gsrc, const float* sums, float* state, uint32_t out_mask, float* outputs,
+                         void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = validate_site_loop(site))) return rc;
+  if ((rc = validate_series(series))) return rc;
+  if ((rc = check_ptr(state, "state")) || (rc = check_ptr(sums, "sums"))) return rc;
+  if (series->n_day > 0 && (rc = check_ptr(gsrc, "gsrc"))) return rc;
+  if (out_mask & ~0x7Fu) return fail(SW100_E_ARG, "unknown output bits 0x%x", out_mask);
+  if (out_mask && !outputs) return fail(SW100_E_ARG, "outputs must not be NULL");
+  dim3 block(32, 4);
+  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  time_loop_sums_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
+      make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
+      reinterpret_cast<const float4*>(gsrc), series->n_day, state, out_mask, outputs, sums);
+  return check_launch("time_loop_sums_kernel");
 }
 
 int sw100_utci(const float* ta, const float* rh, const float* tmrt, const float* va, int64_t n, float* out,

@@ -268,12 +268,17 @@ struct GvfSums {
 // KNOWN_N0: reuse each walk's first-building step after the first daytime
 // step (faster for one site; the batch kernel, with more live registers,
 // does not gain).
-template <class Site, bool KNOWN_N0>
+// SUMS: the four dense patch sums of each step come precomputed (the
+// tensor-core product of patch_sums.cu, sums[(t * 4 + j) * npix + p], j =
+// diffuse Kside, anisotropic luminance, sky longwave down, side) instead of
+// the dense pass below.
+template <class Site, bool KNOWN_N0, bool SUMS = false>
 __device__ __forceinline__ void time_loop_tile(
     const Site& site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
-    float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs, int bx, int by) {
+    float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs, int bx, int by,
+    const float* __restrict__ sums = nullptr) {
   // PP is filled with 16-byte vector stores: the array must be 16-byte
   // aligned (the struct itself only requires 8)
   __shared__ __align__(16) sw100_time_step P;
@@ -482,10 +487,19 @@ __device__ __forceinline__ void time_loop_tile(
     float ld_sky = 0.f, ld_veg = 0.f, ld_sh = 0.f, ld_sun = 0.f, ld_ref = 0.f;
     float ls_sky = 0.f, ls_veg = 0.f, ls_sh = 0.f, ls_sun = 0.f, ls_ref = 0.f;
     const bool day = is_day;
+    if (SUMS) {
+      const float* sp = sums + (size_t)t * 4 * npix + p;
+      if (day) {
+        ksideD = sp[0];
+        anilum = sp[npix];
+      }
+      ld_sky = sp[2 * npix];
+      ls_sky = sp[3 * npix];
+    }
     // dense: sky-visible longwave (sh == 1 & vegsh == 1); by day the diffuse
     // Kside term and the anisotropic luminance, indexed by (sh, vegsh)
 #pragma unroll
-    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
+    for (int w = 0; w < (SUMS ? 0 : SW100_CUBE_WORDS); ++w) {
       const int q0 = w * 32;
       const int nq = min(32, n_patches - q0);
       const uint32_t sw = CB[w][ctid], vw = CB[SW100_CUBE_WORDS + w][ctid];
@@ -606,6 +620,17 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_kernel(
     float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs) {
   time_loop_tile<SitePlanes, true>(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day, state, out_mask, outputs,
                  blockIdx.x, blockIdx.y);
+}
+
+// The same time loop with the dense patch sums precomputed on the tensor
+// cores (patch_sums_tc_kernel).
+__global__ void __launch_bounds__(kTileThreads, 6) time_loop_sums_kernel(
+    SitePlanes site, int rows, int cols, const sw100_time_step* __restrict__ tsteps, int n_t,
+    const sw100_patch_step* __restrict__ patch_steps, int n_patches,
+    const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
+    float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs, const float* __restrict__ sums) {
+  time_loop_tile<SitePlanes, true, true>(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day,
+                                         state, out_mask, outputs, blockIdx.x, blockIdx.y, sums);
 }
 
 // The time loop of every site of a batch, tiles taken in list order.

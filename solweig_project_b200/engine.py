@@ -73,6 +73,10 @@ class Timeline:
         return out
 
 
+# the time loop's dense patch sums on the tensor cores (sw100_patch_sums)
+# rather than in the loop kernel
+TENSOR_SUMS = True
+
 # chunks of the chunked time loop whose device buffers are alive at once
 CHUNKS_IN_FLIGHT = 3
 
@@ -551,8 +555,11 @@ class DeviceSite:
         s.n_t, s.n_day, s.n_patches = len(ser.steps), len(ser.sun), ser.patch.shape[1]
         return s, {"tables": dev, "staging": host}
 
-    def run_time_loop(self, ser: TS.Series, requested=("utci",), series_dev=None, workspace=None):
-        """All steps of the series in one library call; returns
+    def run_time_loop(self, ser: TS.Series, requested=("utci",), series_dev=None, workspace=None,
+                      tensor_sums=None):
+        """All steps of the series: the sun marches, the dense patch sums on
+        the tensor cores (sw100_patch_sums; with ``tensor_sums=False`` the
+        loop kernel computes them itself) and the time loop; returns
         {name: (n_t, rows, cols) device tensor}."""
         if self.svf_result is None:
             raise RuntimeError("run_svf() (or set_svf()) must come before the time loop")
@@ -564,14 +571,49 @@ class DeviceSite:
         d = self.device
         out = torch.empty((len(names), n_t, self.rows, self.cols), dtype=torch.float32, device=d)
         s, dev = series_dev if series_dev is not None else self.upload_series(ser)
-        ws_bytes = N.workspace_bytes("sw100_time_loop_workspace_bytes", self.rows, self.cols, s.n_day)
-        ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else \
-            torch.empty(ws_bytes, dtype=torch.uint8, device=d)
-        site = self.site_struct()
-        N.call("sw100_time_loop", C.byref(site), self.rows, self.cols, C.byref(s), _ptr(self.state), mask,
-               _ptr(out), _ptr(ws), ws.numel(), _stream())
-        self._keep = [dev, ws]
+        tensor_sums = TENSOR_SUMS if tensor_sums is None else tensor_sums
+        if not tensor_sums:
+            ws_bytes = N.workspace_bytes("sw100_time_loop_workspace_bytes", self.rows, self.cols, s.n_day)
+            ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else \
+                torch.empty(ws_bytes, dtype=torch.uint8, device=d)
+            site = self.site_struct()
+            N.call("sw100_time_loop", C.byref(site), self.rows, self.cols, C.byref(s), _ptr(self.state), mask,
+                   _ptr(out), _ptr(ws), ws.numel(), _stream())
+            self._keep = [dev, ws]
+            return {k: out[i] for i, k in enumerate(names)}
+        gsrc = torch.empty((max(1, s.n_day), self.rows, self.cols, 4), dtype=torch.float32, device=d)
+        if s.n_day:
+            self.launch_sun_march(s, gsrc)
+        sums = self.launch_patch_sums(s)
+        self.launch_flux_loop(s, gsrc, mask, out, sums=sums)
+        self._keep = [dev, gsrc, sums]
         return {k: out[i] for i, k in enumerate(names)}
+
+    def launch_patch_sums(self, series: N.Series, sums=None):
+        """The dense patch sums of every step of the series on the tensor
+        cores (sw100_patch_sums) into `sums` ((n_t, 4, rows, cols) float32,
+        allocated when None); returns it."""
+        if sums is None:
+            sums = torch.empty((series.n_t, 4, self.rows, self.cols), dtype=torch.float32, device=self.device)
+        ws_bytes = N.workspace_bytes("sw100_patch_sums_workspace_bytes", series.n_t)
+        key = "sums_ws"
+        if self._cache.get(key) is None or self._cache[key].numel() < ws_bytes:
+            self._cache[key] = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
+        if getattr(self, "tc_err", None) is None:
+            self.tc_err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        site = self.site_struct()
+        N.call("sw100_patch_sums", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(sums), _ptr(self.tc_err),
+               _ptr(self._cache[key]), self._cache[key].numel(), _stream())
+        return sums
+
+    def check_tensor_error(self):
+        """Raise NativeError when a tensor-core kernel of this site gave up a
+        bounded wait (reads the device flag: synchronises)."""
+        err = getattr(self, "tc_err", None)
+        if err is not None and int(err.item()) != 0:
+            code = int(err.item())
+            err.zero_()
+            raise N.NativeError("sw100_patch_sums", code, "a bounded wait of the tensor-core patch sums expired")
 
     def run_sun_march(self, ser: TS.Series):
         """Sun-march records and the 8 reference planes per daytime row
@@ -595,10 +637,17 @@ class DeviceSite:
         N.call("sw100_sun_march", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc), _ptr(debug8),
                _ptr(ws), ws_bytes, _stream())
 
-    def launch_flux_loop(self, series: N.Series, gsrc, out_mask, outputs):
+    def launch_flux_loop(self, series: N.Series, gsrc, out_mask, outputs, sums=None):
+        """The loop kernel over sun-march records `gsrc`; with `sums` (from
+        launch_patch_sums) it reads the dense patch sums instead of
+        computing them."""
         site = self.site_struct()
-        N.call("sw100_flux_loop", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc),
-               _ptr(self.state), out_mask, _ptr(outputs), _stream())
+        if sums is None:
+            N.call("sw100_flux_loop", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc),
+                   _ptr(self.state), out_mask, _ptr(outputs), _stream())
+        else:
+            N.call("sw100_flux_loop_sums", C.byref(site), self.rows, self.cols, C.byref(series), _ptr(gsrc),
+                   _ptr(sums), _ptr(self.state), out_mask, _ptr(outputs), _stream())
 
     def copy_stream(self) -> torch.cuda.Stream:
         """Stream of the chunked loop's device-to-host output copies."""
@@ -682,7 +731,8 @@ class DeviceSite:
                 marched.record(side)
             main.wait_event(marched)
             out = torch.empty((len(names), t1 - t0, self.rows, self.cols), dtype=torch.float32, device=self.device)
-            self.launch_flux_loop(s, gsrc, mask, out)
+            sums = self.launch_patch_sums(s) if TENSOR_SUMS else None
+            self.launch_flux_loop(s, gsrc, mask, out, sums=sums)
             # outputs go back on a copy stream, overlapping the next chunk
             fluxed = torch.cuda.Event()
             fluxed.record(main)
@@ -696,7 +746,7 @@ class DeviceSite:
             # once the event recorded after its copies has completed
             done = torch.cuda.Event()
             done.record(copy)
-            ring.append((done, out, dev, gsrc))
+            ring.append((done, out, dev, gsrc, sums))
             tl.mark(f"launch {t0}-{t1}", main)
             if len(ring) > CHUNKS_IN_FLIGHT:
                 old = ring.popleft()
@@ -706,6 +756,7 @@ class DeviceSite:
         copy.synchronize()
         tl.mark("wait for the GPU")
         ring.clear()
+        self.check_tensor_error()
         return {k: v.numpy() for k, v in host.items()}, scalars
 
     def load_state(self, state: dict):

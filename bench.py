@@ -657,7 +657,7 @@ def main():
             "sun_march": {"ms": march_t, "issue_active_frac_ncu": NCU_ISSUE_ACTIVE["sun_march"],
                           "active_lanes_ncu": NCU_ACTIVE_LANES["sun_march"]},
             "patch_sums_tc": {"ms": sums_t,
-                              "tflops_bf16": (2.0 * npix * 640 * 96 * ((N_STEPS_DAY + 7) // 8) / (sums_t * 1e9)
+                              "tflops_bf16": (2.0 * npix * 624 * 96 * ((N_STEPS_DAY + 7) // 8) / (sums_t * 1e9)
                                               if sums is not None and sums_t > 0 else None),
                               "note": "dense 153-patch sums as a one-hot x weight product on tcgen05 (BF16 in 3 "
                                       "parts, FP32 accumulate); includes the weight split kernel"},

@@ -638,7 +638,7 @@ int sw100_patch_sums_workspace_bytes(int n_t, int64_t* bytes) {
   int rc;
   if ((rc = check_ptr(bytes, "bytes"))) return rc;
   if (n_t < 0) return fail(SW100_E_ARG, "n_t must be >= 0");
-  *bytes = align_up((int64_t)((n_t + 7) / 8) * 96 * 640 * 2);
+  *bytes = align_up((int64_t)((n_t + 7) / 8) * 96 * 624 * 2);
   return 0;
 }
 
@@ -649,7 +649,7 @@ int sw100_patch_sums(const sw100_site_planes* site, int rows, int cols, const sw
   if ((rc = validate_site_loop(site))) return rc;
   if ((rc = validate_series(series))) return rc;
   if ((rc = check_ptr(sums, "sums"))) return rc;
-  if (series->n_patches > 160) return fail(SW100_E_ARG, "at most 160 patches (n_patches %d)", series->n_patches);
+  if (series->n_patches > 156) return fail(SW100_E_ARG, "at most 156 patches (n_patches %d)", series->n_patches);
   int64_t need = 0;
   if ((rc = sw100_patch_sums_workspace_bytes(series->n_t, &need))) return rc;
   if ((rc = check_workspace(workspace, workspace_bytes, need))) return rc;
@@ -657,11 +657,13 @@ int sw100_patch_sums(const sw100_site_planes* site, int rows, int cols, const sw
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int n_groups = (series->n_t + 7) / 8;
   __nv_bfloat16* W = static_cast<__nv_bfloat16*>(workspace);
-  const int64_t nw = (int64_t)n_groups * 96 * 640;
+  const int64_t nw = (int64_t)n_groups * 96 * 624;
   patch_weights_kernel<<<(unsigned)std::min<int64_t>((nw + 255) / 256, 148 * 8), 256, 0, st>>>(
       series->steps, series->n_t, series->patch, series->n_patches, W, n_groups);
   if ((rc = check_launch("patch_weights_kernel"))) return rc;
-  const int smem = 2 * (16384 + 12288);   // two stages of A (16 KB) and B (12 KB) chunks
+  // three stages of A (12 KB) and B (9 KB) chunks: 63 KB, at most 3 CTAs
+  // (3 x 128 TMEM columns) per SM
+  const int smem = 3 * (12288 + 9216);
   // the attributes are per function and process: set them once (the largest
   // shared-memory carveout, so that several 56 KB CTAs share an SM)
   static std::once_flag attr_once;

@@ -9,7 +9,7 @@
 // Per pixel and step these four sums take every patch, each patch adding a
 // per-step increment chosen by the pixel's (sh, vegsh) code.  Written as a
 // matrix product: A[pixel][(patch, code)] is one-hot (1.0 at the pixel's
-// code of each patch; 160 patches x 4 codes = K 640), B[(patch, code)][n]
+// code of each patch; 156 patches x 4 codes = K 624), B[(patch, code)][n]
 // holds the per-step increments, n = (step, sum, part): each float32
 // increment split into three bf16 parts hi + mid + lo that add up to it
 // exactly, so the products are exact and the FP32 accumulation sums the
@@ -17,13 +17,13 @@
 // the reference: the sums agree to about one float32 rounding).
 //
 // One CTA (4 warps) owns 128 pixels (M = 128) and one group of 8 steps
-// (N = 8 x 4 sums x 3 parts = 96) at a time; K runs in chunks of 16 patches
-// (64 columns): the A chunk is built in shared memory by the threads from
+// (N = 8 x 4 sums x 3 parts = 96) at a time; K runs in chunks of 12 patches
+// (48 columns): the A chunk is built in shared memory by the threads from
 // the pixel's bit words, the B chunk is copied from global memory
 // (cp.async, prefetched one chunk ahead), both in the no-swizzle K-major
-// core-matrix layout; one thread issues 4 tcgen05.mma (kind::f16, BF16 x
+// core-matrix layout; one thread issues 3 tcgen05.mma (kind::f16, BF16 x
 // BF16 -> FP32 in TMEM, 128 columns) per chunk and commits them to the
-// chunk's mbarrier; two stages rotate.  The epilogue reads the accumulator
+// chunk's mbarrier; three stages rotate, two chunks' MMAs in flight.  The epilogue reads the accumulator
 // with tcgen05.ld (warp w owns TMEM lanes 32 w .. 32 w + 31 = its pixels),
 // adds the three parts and writes sums[(step * 4 + sum) * npix + pixel].
 // Every wait is bounded: on expiry the CTA stops issuing, drains what it
@@ -38,12 +38,13 @@ namespace sw100 {
 
 constexpr int kPsSteps = 8;                       // steps per group
 constexpr int kPsN = kPsSteps * 4 * 3;            // 96 accumulator columns
-constexpr int kPsK = 640;                         // 160 patches x 4 codes
-constexpr int kPsChunkK = 64;                     // 16 patches per chunk
-constexpr int kPsChunks = kPsK / kPsChunkK;       // 10
-constexpr int kPsABytes = 128 * kPsChunkK * 2;    // 16 KB (4 K steps of 4 KB)
-constexpr int kPsBBytes = kPsN * kPsChunkK * 2;   // 12 KB (4 K steps of 3 KB)
+constexpr int kPsK = 624;                         // 156 patches x 4 codes
+constexpr int kPsChunkK = 48;                     // 12 patches per chunk (3 K steps)
+constexpr int kPsChunks = kPsK / kPsChunkK;       // 13
+constexpr int kPsABytes = 128 * kPsChunkK * 2;    // 12 KB (3 K steps of 4 KB)
+constexpr int kPsBBytes = kPsN * kPsChunkK * 2;   // 9 KB (3 K steps of 3 KB)
 constexpr int kPsStageBytes = kPsABytes + kPsBBytes;
+constexpr int kPsStages = 3;                      // stages of [A | B] chunks in flight
 
 // B = the per-step increments in bf16 parts: W[g][n][k], n = (step in the
 // group * 4 + sum) * 3 + part, k = patch * 4 + code (code = sh * 2 + vegsh).
@@ -88,31 +89,49 @@ __device__ __forceinline__ void cp_async16_ps(uint32_t dst, const void* src) {
 
 // one-hot bf16 codes of two patches (8 columns = one 16-byte core-matrix row)
 __device__ __forceinline__ uint4 onehot_pair(int code_a, int code_b) {
-  uint32_t w[4] = {0u, 0u, 0u, 0u};
-  if (code_a >= 0) w[code_a >> 1] |= 0x3F80u << ((code_a & 1) * 16);
-  if (code_b >= 0) w[2 + (code_b >> 1)] |= 0x3F80u << ((code_b & 1) * 16);
-  return make_uint4(w[0], w[1], w[2], w[3]);
+  const unsigned long long a = code_a >= 0 ? 0x3F80ull << (16 * code_a) : 0ull;   // columns 0-3
+  const unsigned long long b = code_b >= 0 ? 0x3F80ull << (16 * code_b) : 0ull;   // columns 4-7
+  return make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+}
+
+// B chunk i of the whole sequence (group i / kPsChunks, chunk i % kPsChunks)
+// into a stage: 96 rows x 48 columns = 576 16-byte pieces (6 per row)
+__device__ __forceinline__ void ps_load_b(const __nv_bfloat16* __restrict__ W, uint32_t base, int tid, int i,
+                                          int stage) {
+  const uint32_t b_st = base + stage * kPsStageBytes + kPsABytes;
+  const __nv_bfloat16* wg = W + (size_t)(i / kPsChunks) * kPsN * kPsK + (i % kPsChunks) * kPsChunkK;
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    const int j = tid + 128 * m;
+    if (j < kPsN * 6) {
+      const int n = j / 6, u = j % 6;
+      cp_async16_ps(b_st + (u >> 1) * (kPsN * 32) + tc::core_off(n, u & 1), wg + (size_t)n * kPsK + u * 8);
+    }
+  }
 }
 
 __global__ void __launch_bounds__(128) patch_sums_tc_kernel(const uint32_t* __restrict__ bits, int64_t npix,
                                                             int n_patches, const __nv_bfloat16* __restrict__ W,
                                                             int n_groups, int n_t, float* __restrict__ sums,
                                                             int* __restrict__ err, int wait_limit) {
-  // dynamic shared memory: two stages of [A chunk | B chunk]; 56 KB per CTA
-  // keeps at most 4 CTAs on an SM, so their TMEM (128 columns each) fits
-  extern __shared__ __align__(1024) uint8_t ps_smem[];
-  __shared__ __align__(8) uint64_t mbar[2];
+  // dynamic shared memory: three stages of [A chunk | B chunk] (63 KB): at
+  // most 3 CTAs share an SM, so their TMEM (128 columns each) fits in the
+  // SM's 512 columns
+  extern __shared__ __align__(128) uint8_t ps_smem[];
+  __shared__ __align__(8) uint64_t mbar[kPsStages];
   __shared__ uint32_t tmem_base;
   const uint32_t base = tc::smem_u32(ps_smem);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int64_t p = (int64_t)blockIdx.x * 128 + tid;
   const bool live = p < npix;
-  uint32_t sw[SW100_CUBE_WORDS], vw[SW100_CUBE_WORDS];
-#pragma unroll
-  for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
-    sw[w] = live ? bits[(size_t)w * npix + p] : 0u;
-    vw[w] = live ? bits[(size_t)(SW100_CUBE_WORDS + w) * npix + p] : 0u;
-  }
+  // the pixel's sh and vegsh bit words (patches 32 w .. 32 w + 31), as scalars
+  static_assert(SW100_CUBE_WORDS == 5, "five 32-bit words per patch cube");
+  const uint32_t* bp = bits + (live ? p : 0);
+  const size_t np = (size_t)npix;
+  const uint32_t s0 = live ? bp[0 * np] : 0u, s1 = live ? bp[1 * np] : 0u, s2 = live ? bp[2 * np] : 0u,
+                 s3 = live ? bp[3 * np] : 0u, s4 = live ? bp[4 * np] : 0u;
+  const uint32_t v0 = live ? bp[5 * np] : 0u, v1 = live ? bp[6 * np] : 0u, v2 = live ? bp[7 * np] : 0u,
+                 v3 = live ? bp[8 * np] : 0u, v4 = live ? bp[9 * np] : 0u;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_base)),
                  "r"(128)
@@ -120,8 +139,7 @@ __global__ void __launch_bounds__(128) patch_sums_tc_kernel(const uint32_t* __re
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    tc::mbar_init(tc::smem_u32(&mbar[0]), 1);
-    tc::mbar_init(tc::smem_u32(&mbar[1]), 1);
+    for (int k = 0; k < kPsStages; ++k) tc::mbar_init(tc::smem_u32(&mbar[k]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -129,54 +147,49 @@ __global__ void __launch_bounds__(128) patch_sums_tc_kernel(const uint32_t* __re
   const uint32_t tmem = tmem_base;
   const uint32_t idesc = tc::instr_desc(128, kPsN);
 
-  // B chunk i of the whole sequence (group i / kPsChunks, chunk i % kPsChunks)
-  // into a stage: 96 rows x 64 columns = 768 16-byte pieces, 6 per thread
-  auto load_b = [&](int i, int stage) {
-    const uint32_t b_st = base + stage * kPsStageBytes + kPsABytes;
-    const __nv_bfloat16* wg = W + (size_t)(i / kPsChunks) * kPsN * kPsK + (i % kPsChunks) * kPsChunkK;
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-      const int j = tid + 128 * m;
-      const int n = j >> 3, u = j & 7;
-      cp_async16_ps(b_st + (u >> 1) * (kPsN * 32) + tc::core_off(n, u & 1), wg + (size_t)n * kPsK + u * 8);
-    }
-  };
 
-  // Iteration it (chunk c of group g): A(it) is built in its stage while
-  // the previous chunk's MMAs run, then B(it + 1) is prefetched into the
-  // other stage once those MMAs are done, and B(it), prefetched one
-  // iteration earlier, is waited for.  Commits complete in order, so the
-  // wait on MMA(it - 1) also covers every earlier chunk.
+  // Iteration it (chunk c of group g) uses stage it % 3: A(it) is built
+  // there (its last reader, MMA(it - 3), was waited for in the previous
+  // iteration); then MMA(it - 2) is waited for and B(it + 1) prefetched
+  // into its stage, and B(it), prefetched one iteration earlier, is waited
+  // for, so MMA(it - 1) may still run while MMA(it) is issued.  Commits
+  // complete in order: a wait on MMA(j) covers every earlier chunk.
   const int total = n_groups * kPsChunks;
   bool ok = true;
   int last_commit = -1;
-  load_b(0, 0);
+  ps_load_b(W, base, tid, 0, 0);
   asm volatile("cp.async.commit_group;" ::: "memory");
   for (int it = 0; it < total; ++it) {
-    const int stage = it & 1, g = it / kPsChunks, c = it % kPsChunks;
+    const int stage = it % kPsStages, g = it / kPsChunks, c = it % kPsChunks;
     const uint32_t a_st = base + stage * kPsStageBytes, b_st = a_st + kPsABytes;
-    // A(it): this pixel's row, 4 K steps of 4 patches (the stage's last
-    // reader, MMA(it - 2), was waited for in the previous iteration)
+    // A(it): this pixel's row, 3 K steps of 4 patches (see above); the
+    // chunk's 12 patch bits are taken from the two words holding them,
+    // selected into registers (no dynamic indexing)
+    const int q0 = c * 12, cw = q0 >> 5, sh = q0 & 31;
+    const uint32_t sa = cw == 0 ? s0 : cw == 1 ? s1 : cw == 2 ? s2 : cw == 3 ? s3 : s4;
+    const uint32_t sb = cw == 0 ? s1 : cw == 1 ? s2 : cw == 2 ? s3 : cw == 3 ? s4 : 0u;
+    const uint32_t va = cw == 0 ? v0 : cw == 1 ? v1 : cw == 2 ? v2 : cw == 3 ? v3 : v4;
+    const uint32_t vb = cw == 0 ? v1 : cw == 1 ? v2 : cw == 2 ? v3 : cw == 3 ? v4 : 0u;
+    const uint32_t ws = (uint32_t)((((unsigned long long)sb << 32) | sa) >> sh);   // bits of patches q0 ..
+    const uint32_t wv = (uint32_t)((((unsigned long long)vb << 32) | va) >> sh);
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < 3; ++s) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int qa = c * 16 + s * 4 + h * 2, qb = qa + 1;
-        int ca = -1, cb = -1;
-        if (live && qa < n_patches)
-          ca = (int)((sw[qa >> 5] >> (qa & 31)) & 1u) * 2 + (int)((vw[qa >> 5] >> (qa & 31)) & 1u);
-        if (live && qb < n_patches)
-          cb = (int)((sw[qb >> 5] >> (qb & 31)) & 1u) * 2 + (int)((vw[qb >> 5] >> (qb & 31)) & 1u);
+        const int ja = s * 4 + h * 2, jb = ja + 1;
+        const int ca = (live && q0 + ja < n_patches) ? (int)((ws >> ja) & 1u) * 2 + (int)((wv >> ja) & 1u) : -1;
+        const int cb = (live && q0 + jb < n_patches) ? (int)((ws >> jb) & 1u) * 2 + (int)((wv >> jb) & 1u) : -1;
         st_shared_v4(a_st + s * 4096 + tc::core_off(tid, h), onehot_pair(ca, cb));
       }
     }
-    // MMA(it - 1) read the other stage: wait for it before refilling that stage
-    if (it >= 1) {
-      const bool w = tc::mbar_wait(tc::smem_u32(&mbar[(it - 1) & 1]), ((it - 1) >> 1) & 1, wait_limit);
+    // the stage of B(it + 1) was last read by MMA(it - 2)
+    if (it >= 2) {
+      const int j = it - 2;
+      const bool w = tc::mbar_wait(tc::smem_u32(&mbar[j % kPsStages]), (j / kPsStages) & 1, wait_limit);
       ok = __syncthreads_and(w) != 0;
       if (!ok) break;
     }
-    if (it + 1 < total) load_b(it + 1, stage ^ 1);
+    if (it + 1 < total) ps_load_b(W, base, tid, it + 1, (it + 1) % kPsStages);
     asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group 1;" ::: "memory");   // B(it) has landed
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -184,7 +197,7 @@ __global__ void __launch_bounds__(128) patch_sums_tc_kernel(const uint32_t* __re
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-      for (int s = 0; s < 4; ++s) {
+      for (int s = 0; s < 3; ++s) {
         const uint64_t ad = tc::smem_desc(a_st + s * 4096, 128, 256);
         const uint64_t bd = tc::smem_desc(b_st + s * (kPsN * 32), 128, 256);
         tc::mma_f16(tmem, ad, bd, idesc, (c > 0 || s > 0) ? 1u : 0u);
@@ -195,7 +208,7 @@ __global__ void __launch_bounds__(128) patch_sums_tc_kernel(const uint32_t* __re
     if (c + 1 < kPsChunks) continue;
     // the group's last chunk: its commit covers every MMA of the group
     {
-      const bool w = tc::mbar_wait(tc::smem_u32(&mbar[stage]), (it >> 1) & 1, wait_limit);
+      const bool w = tc::mbar_wait(tc::smem_u32(&mbar[stage]), (it / kPsStages) & 1, wait_limit);
       ok = __syncthreads_and(w) != 0;
       if (!ok) break;
     }
@@ -235,7 +248,7 @@ __global__ void __launch_bounds__(128) patch_sums_tc_kernel(const uint32_t* __re
     asm volatile("cp.async.wait_all;" ::: "memory");
     bool drained = true;
     if (tid == 0 && last_commit >= 0)
-      drained = tc::mbar_wait(tc::smem_u32(&mbar[last_commit & 1]), (last_commit >> 1) & 1,
+      drained = tc::mbar_wait(tc::smem_u32(&mbar[last_commit % kPsStages]), (last_commit / kPsStages) & 1,
                               wait_limit > (1 << 22) ? wait_limit : (1 << 22));
     drained = __syncthreads_and(drained) != 0;
     if (tid == 0 && err) atomicExch(err, drained ? 1 : 2);

@@ -692,6 +692,15 @@ int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, cons
   if (series->n_day > 0 && (rc = check_ptr(gsrc, "gsrc"))) return rc;
   if (out_mask & ~0x7Fu) return fail(SW100_E_ARG, "unknown output bits 0x%x", out_mask);
   if (out_mask && !outputs) return fail(SW100_E_ARG, "outputs must not be NULL");
+  // six 33 KB blocks per SM (the register bound) need the largest
+  // shared-memory carveout; set once per process
+  static std::once_flag attr_once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(attr_once, [&] {
+    attr_err = cudaFuncSetAttribute(time_loop_sums_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared);
+  });
+  if (attr_err != cudaSuccess) return fail((int)attr_err, "cudaFuncSetAttribute: %s", cudaGetErrorString(attr_err));
   dim3 block(32, 4);
   dim3 grid((cols + 31) / 32, (rows + 3) / 4);
   time_loop_sums_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(

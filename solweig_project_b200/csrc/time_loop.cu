@@ -22,6 +22,8 @@
 // constants evaluated in the reference's association, so each sum is the
 // same sequence of float32 additions (float64 where the reference promotes).
 #include <cmath>
+#include <cstddef>
+#include <type_traits>
 
 #include "sw_common.cuh"
 #include "sw_internal.cuh"
@@ -31,6 +33,24 @@ namespace sw100 {
 
 constexpr int kMaxPatchSmem = 153;
 constexpr int kTileThreads = 128;  // threads of a time-loop block (every launch shape)
+
+// The last 96 bytes of sw100_patch_step (kref_veg onwards): everything the
+// set-bit walk reads.  With the dense sums precomputed the loop stages only
+// these, 96-byte records instead of 128 (a smaller block, and lanes reading
+// different patches spread over more banks).
+struct PatchTail {
+  float kref_veg, kref_sun, kref_sh, yi_k, yi_l, thr_sun, thr_shd, ld_sky, ls_sky, ster, cos_alt, sin_alt, sun_cos,
+      sun_sin;
+  int32_t flags, pad;
+  double veg_cos, veg_sin, sh_cos, sh_sin;
+};
+constexpr int kPatchTailOffset = (int)offsetof(sw100_patch_step, kref_veg);
+static_assert(kPatchTailOffset == 32 && sizeof(PatchTail) == 96 &&
+                  sizeof(sw100_patch_step) == kPatchTailOffset + sizeof(PatchTail),
+              "PatchTail is the tail of sw100_patch_step");
+static_assert(offsetof(PatchTail, veg_cos) + kPatchTailOffset == offsetof(sw100_patch_step, veg_cos) &&
+                  offsetof(PatchTail, flags) + kPatchTailOffset == offsetof(sw100_patch_step, flags),
+              "PatchTail fields sit where sw100_patch_step has them");
 
 struct GvfAzSmem {
   int8_t dx[SW100_MAX_GVF_STEPS];
@@ -282,7 +302,8 @@ __device__ __forceinline__ void time_loop_tile(
   // PP is filled with 16-byte vector stores: the array must be 16-byte
   // aligned (the struct itself only requires 8)
   __shared__ __align__(16) sw100_time_step P;
-  __shared__ __align__(16) sw100_patch_step PP[kMaxPatchSmem];
+  using PatchRec = typename std::conditional<SUMS, PatchTail, sw100_patch_step>::type;
+  __shared__ __align__(16) PatchRec PP[kMaxPatchSmem];
   __shared__ GvfAzSmem AZ[SW100_N_GVF_AZ];
   __shared__ int AZOFF[SW100_N_GVF_AZ][SW100_MAX_GVF_STEPS];  // dx * cols + dy
   // Lwall / albedo_b added k times in float32, k = 0..second (this step)
@@ -350,8 +371,15 @@ __device__ __forceinline__ void time_loop_tile(
       for (int i = tid; i < (int)(sizeof(sw100_time_step) / 4); i += nthr) d[i] = s[i];
       const int4* ps = reinterpret_cast<const int4*>(patch_steps + (size_t)t * n_patches);
       int4* pd = reinterpret_cast<int4*>(PP);
-      const int n16 = n_patches * (int)(sizeof(sw100_patch_step) / 16);
-      for (int i = tid; i < n16; i += nthr) pd[i] = ps[i];
+      // 16-byte pieces per staged record, and where the record starts in
+      // the 128-byte global one
+      constexpr int kPieces = (int)(sizeof(PatchRec) / 16);
+      constexpr int kSkip = (int)((sizeof(sw100_patch_step) - sizeof(PatchRec)) / 16);
+      const int n16 = n_patches * kPieces;
+      for (int i = tid; i < n16; i += nthr) {
+        const int rec = i / kPieces, piece = i - rec * kPieces;
+        pd[i] = ps[rec * (kPieces + kSkip) + kSkip + piece];
+      }
       if (tsteps[t].is_day) {
         const float lw = tsteps[t].lwall, ab = tsteps[t].albedo_b;
         for (int i = tid; i <= SW100_MAX_GVF_STEPS; i += nthr) {
@@ -498,8 +526,9 @@ __device__ __forceinline__ void time_loop_tile(
     }
     // dense: sky-visible longwave (sh == 1 & vegsh == 1); by day the diffuse
     // Kside term and the anisotropic luminance, indexed by (sh, vegsh)
+    if constexpr (!SUMS) {
 #pragma unroll
-    for (int w = 0; w < (SUMS ? 0 : SW100_CUBE_WORDS); ++w) {
+    for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
       const int nq = min(32, n_patches - q0);
       const uint32_t sw = CB[w][ctid], vw = CB[SW100_CUBE_WORDS + w][ctid];
@@ -523,6 +552,7 @@ __device__ __forceinline__ void time_loop_tile(
         }
       }
     }
+    }
     // One ascending set-bit walk over the reflected-longwave patches
     // (solweig.py:1613-1633, temp_sh = (sh == 0) | (vegsh == 0) |
     // (vbshvegsh == 0)), a superset of the vegetation-facing patches
@@ -545,7 +575,7 @@ __device__ __forceinline__ void time_loop_tile(
         const int j = __ffs(m) - 1;
         m &= m - 1u;
         const uint32_t bit = 1u << j;
-        const sw100_patch_step& Q = PP[q0 + j];
+        const PatchRec& Q = PP[q0 + j];
         if (mveg & bit) {
           ls_veg = add64(ls_veg, Q.veg_cos);
           ld_veg = add64(ld_veg, Q.veg_sin);

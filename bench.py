@@ -17,7 +17,8 @@ synthetic city of the workload (500 x 500 px at 1 m by default).
 * With torchrun (N > 1) every rank runs its own site (weak scaling, no
   collective on the data path); the time is the max over ranks.
 * ``--impl reference`` times the CPU oracle (the reference's algorithm
-  restated on the host cores) on a bounded crop of the same workload.
+  restated on the host cores) over the whole workload: one full pass whose
+  K timed steps are its K pieces.
 """
 from __future__ import annotations
 
@@ -56,7 +57,7 @@ SVF_GATHER_BYTES_PER_STEP = 12    # 3 float32 gathers per march step
 # each kernel, from ncu captures: the flux loop at 500 x 500 x 24 (the default
 # workload), the SVF sweep and sun march at 1024 x 1024 scaled to a launch of
 # the measured size by pixel count (their traffic is per pixel).
-NCU_TRAFFIC = {"flux_loop": (500 * 500, 119_174_400), "svf_sweep": (1024 * 1024, 206_271_744),
+NCU_TRAFFIC = {"flux_loop": (500 * 500, 215_858_176), "svf_sweep": (1024 * 1024, 206_271_744),
                "sun_march": (1024 * 1024, 340_633_088)}
 # issue-slot utilisation (smsp__issue_active) of the same captures: the
 # binding roofline of these integer / FP32 kernels is instruction issue
@@ -64,9 +65,11 @@ NCU_TRAFFIC = {"flux_loop": (500 * 500, 119_174_400), "svf_sweep": (1024 * 1024,
 # call is host-bound at small sizes, so one slow call from other host load
 # should not move the figure)
 E2E_TIMED = 7
-NCU_ISSUE_ACTIVE = {"flux_loop": 0.541, "svf_sweep": 0.758, "sun_march": 0.791}
+NCU_ISSUE_ACTIVE = {"flux_loop": 0.547, "svf_sweep": 0.758, "sun_march": 0.791, "patch_sums_tc": 0.386}
 # active lanes per issued warp instruction (of 32) in the same captures
-NCU_ACTIVE_LANES = {"flux_loop": 21.16, "svf_sweep": 24.42, "sun_march": 26.50}
+NCU_ACTIVE_LANES = {"flux_loop": 19.42, "svf_sweep": 24.42, "sun_march": 26.50, "patch_sums_tc": 30.67}
+# tensor-pipe activity (sm__pipe_tensor_cycles_active) of the patch-sum product at 500 x 500 x 24
+NCU_TENSOR_ACTIVE = {"patch_sums_tc": 0.142}
 # reference pins of the 500 x 500 city (seed 1234): Tmrt / UTCI of the
 # unmodified reference and of an FP64 re-evaluation at seeded sample pixels
 PINS = {"exact500": os.path.join(REPO, "tests", "golden", "large_c2_500.npz")}
@@ -232,64 +235,146 @@ def error_vs_fp64(pin_path, tmrt, utci):
             "reference_all_px_utci_C": {"max": float(d["ref_fp64_utci_max"]), "rms": float(d["ref_fp64_utci_rms"])}}
 
 
-def cpu_baseline(city, met, geo, lc_class, crop=64):
-    """The CPU oracle on a bounded crop (crop x crop px, all 24 steps, SVF
-    sweep included), single thread."""
-    import torch
-    torch.set_num_threads(1)
+# the CPU baseline of the default run: a crop of the workload small enough
+# for 10-30 s of host work next to the GPU bench
+CPU_BASELINE_CROP = 200
+
+
+def oracle_pass(city, met, geo, lc_class, n_pieces, march_map):
+    """One pass of the CPU oracle over a whole site -- the 153-patch SVF
+    sweep, then the 24-step window -- cut into `n_pieces` pieces timed one
+    after another; returns the piece times (s), which add up to the pass,
+    and the window's outputs.
+    The sweep is one piece (its patch marches through `march_map`, the sums
+    in patch order) and the window's steps are split over the other pieces
+    (one generator, so the window is set up once, as in a single call);
+    beyond 1 + 24 pieces the sweep is split into patch groups too.  With one
+    piece the whole pass is one."""
     from oracle import svf as osvf, window as ow
-    sl = (slice(0, crop), slice(0, crop))
-    dsm, trees, dem = city.dsm[sl], city.trees[sl], city.dem[sl]
-    t0 = time.perf_counter()
-    vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(dsm, trees, dem)
-    bundle = osvf.svf_calculator(2, amax, dsm, vegdsm, vegdsm2, bush, city.scale)
-    ow.run_utci_window(a=dsm, temp1=trees, temp2=dem, walls=city.walls[sl], dirwalls=city.aspect[sl],
-                       svf_bundle=bundle, met_file=met, location={"latitude": 30.3, "longitude": -97.7,
-                                                                  "altitude": 3.0}, scale=city.scale,
-                       landcover_grid=city.landcover[sl], lc_class=lc_class, requested_variables=("utci", "tmrt"),
-                       **geo)
-    dt = time.perf_counter() - t0
-    return {"value": crop * crop * N_STEPS_DAY / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{crop}x{crop} px crop of the workload, 24 steps, SVF sweep included, {dt:.2f} s"}
+    from solweig_project_b200.synthetic import DEFAULT_LOCATION
+    vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(city.dsm, city.trees, city.dem)
+    tasks = osvf.patch_tasks(2)
+    n_t = met.shape[0]
+    n_svf = min(len(tasks), max(1, n_pieces - n_t))
+    n_win = max(0, n_pieces - n_svf)
+    acc = osvf.SvfAccumulator(2, *city.dsm.shape, vegdsm2)
+    window = {}
+
+    def svf_part(group):
+        def run():
+            for t, res in march_map([tasks[j] for j in group]):
+                acc.add(t, *res)
+        return run
+
+    def window_part(n, last):
+        def run():
+            if "steps" not in window:
+                window["steps"] = ow.iter_utci_window(
+                    a=city.dsm, temp1=city.trees, temp2=city.dem, walls=city.walls, dirwalls=city.aspect,
+                    svf_bundle=acc.result(), met_file=met, location=dict(DEFAULT_LOCATION), scale=city.scale,
+                    landcover_grid=city.landcover, lc_class=lc_class, requested_variables=("utci", "tmrt"), **geo)
+            for _ in range(n):
+                next(window["steps"])
+            if last:
+                try:
+                    next(window["steps"])
+                except StopIteration as done:
+                    window["out"] = done.value
+        return run
+
+    svf_runs = [svf_part(g) for g in np.array_split(np.arange(len(tasks)), n_svf)]
+    chunks = np.array_split(np.arange(n_t), max(1, n_win))
+    win_runs = [window_part(len(c), k == len(chunks) - 1) for k, c in enumerate(chunks)]
+    pieces = [[r] for r in svf_runs + win_runs] if n_win else [svf_runs + win_runs]
+    times = []
+    for piece in pieces:
+        t0 = time.perf_counter()
+        for run in piece:
+            run()
+        times.append(time.perf_counter() - t0)
+    if "out" not in window:
+        raise RuntimeError("the oracle window did not finish")
+    return times, window["out"]
+
+
+def _crop(city, n):
+    import dataclasses
+    sl = (slice(0, n), slice(0, n))
+    return dataclasses.replace(city, **{k: getattr(city, k)[sl] for k in
+                                        ("dsm", "trees", "dem", "walls", "aspect", "landcover")})
+
+
+def _march_map(city, processes):
+    """(march_map, close) for oracle_pass: the patch marches of this city
+    in a spawn pool of `processes` workers, or in this process."""
+    from oracle import svf as osvf
+    vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(city.dsm, city.trees, city.dem)
+    if processes <= 1:
+        def serial(tasks):
+            for t in tasks:
+                yield t, osvf.shadow_patch(amax, city.dsm, vegdsm, vegdsm2, bush, t[2], t[3], city.scale)
+        return serial, lambda: None
+    pool, one = osvf.march_pool(processes, amax, city.dsm, vegdsm, vegdsm2, bush, city.scale)
+
+    def close():
+        pool.close()
+        pool.join()
+    return (lambda tasks: pool.imap(one, tasks)), close
+
+
+def cpu_baseline(city, met, geo, lc_class, crop=CPU_BASELINE_CROP):
+    """The CPU oracle on a crop x crop px corner of the workload, all 24
+    steps, SVF sweep included: the patch marches on every host core (spawn
+    pool), the window in this process with all cores as torch threads."""
+    import torch
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    sub = _crop(city, crop)
+    march_map, close = _march_map(sub, cores)
+    try:
+        dt = sum(oracle_pass(sub, met, geo, lc_class, 1, march_map)[0])
+    finally:
+        close()
+    return {"value": crop * crop * N_STEPS_DAY / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{crop}x{crop} px corner of the {city.shape[0]}x{city.shape[1]} workload, 24 steps, SVF "
+                      f"sweep included, {dt:.1f} s: patch marches in a {cores}-process pool, window numpy in one "
+                      f"process ({cores} torch threads)"}
 
 
 def run_reference(args):
-    """--impl reference: the CPU oracle with all host threads on a bounded crop."""
+    """--impl reference: one pass of the CPU oracle over the whole workload
+    (every pixel, the full march lengths), its K timed steps the K pieces of
+    that pass (oracle_pass); W warm-up passes over a 32 x 32 corner first."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import torch
     cores = os.cpu_count() or 1
     torch.set_num_threads(cores)
-    from oracle import svf as osvf, window as ow
     city, met, geo, lc_class = make_workload(args.workload, 0, args.side)
-    crop = 96
-    sl = (slice(0, crop), slice(0, crop))
-    times = []
-    for it in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        dsm, trees, dem = city.dsm[sl], city.trees[sl], city.dem[sl]
-        vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(dsm, trees, dem)
-        bundle = osvf.svf_calculator(2, amax, dsm, vegdsm, vegdsm2, bush, city.scale)
-        ow.run_utci_window(a=dsm, temp1=trees, temp2=dem, walls=city.walls[sl], dirwalls=city.aspect[sl],
-                           svf_bundle=bundle, met_file=met,
-                           location={"latitude": 30.3, "longitude": -97.7, "altitude": 3.0}, scale=city.scale,
-                           landcover_grid=city.landcover[sl], lc_class=lc_class,
-                           requested_variables=("utci", "tmrt"), **geo)
-        if it >= args.warmup:
-            times.append(time.perf_counter() - t0)
-    t = sum(times) / len(times)
-    value = crop * crop * N_STEPS_DAY / t
-    side = city.shape[0]
+    small = _crop(city, 32)
+    serial, _ = _march_map(small, 1)
+    for _ in range(args.warmup):
+        oracle_pass(small, met, geo, lc_class, 1, serial)
+    march_map, close = _march_map(city, cores)
+    try:
+        times, _ = oracle_pass(city, met, geo, lc_class, args.steps, march_map)
+    finally:
+        close()
+    total = sum(times)
+    rows, cols = city.shape
+    value = rows * cols * N_STEPS_DAY / total
+    sample = (f"one full pass of the {rows}x{cols} workload (SVF sweep + 24 steps) in {args.steps} timed pieces "
+              f"(sweep, then the window's steps), {total:.1f} s: patch marches in a {cores}-process spawn pool, "
+              f"window numpy in one process ({cores} torch threads)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded city, 24 h forcing)",
-        "config": {"workload": args.workload, "rows": side, "cols": side, "timesteps": N_STEPS_DAY,
-                   "sample": f"{crop}x{crop} px crop"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{crop}x{crop} px crop of the {side}x{side} workload, 24 steps, SVF included, "
-                                   f"CPU oracle with {cores} torch threads"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded city, 24 h forcing)",
+        "config": {"workload": args.workload, "rows": rows, "cols": cols, "timesteps": N_STEPS_DAY,
+                   "sample": sample, "piece_s": [round(t, 3) for t in times]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -641,7 +726,6 @@ def main():
         svf_t = sum(svf_ms) / len(svf_ms)
         march_t = sum(march_ms) / len(march_ms)
         sums_t = sum(sums_ms) / len(sums_ms)
-        from solweig_project_b200.synthetic import DEFAULT_LOCATION  # noqa: F401
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
@@ -659,6 +743,8 @@ def main():
             "patch_sums_tc": {"ms": sums_t,
                               "tflops_bf16": (2.0 * npix * 624 * 96 * ((N_STEPS_DAY + 7) // 8) / (sums_t * 1e9)
                                               if sums is not None and sums_t > 0 else None),
+                              "issue_active_frac_ncu": NCU_ISSUE_ACTIVE["patch_sums_tc"],
+                              "tensor_active_frac_ncu": NCU_TENSOR_ACTIVE["patch_sums_tc"],
                               "note": "dense 153-patch sums as a one-hot x weight product on tcgen05 (BF16 in 3 "
                                       "parts, FP32 accumulate); includes the weight split kernel"},
             "flux_loop": {"ms": loop_t,

@@ -571,7 +571,6 @@ int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, cons
                          const float* gsrc, const float* sums, float* state, uint32_t out_mask, float* outputs,
                          void* stream);
 
-/* ---------------------------------------------------------------- UTCI -- */
 /* ---------------------------------------------------- learned preview -- */
 /* Kernels of the learned SVF preview (a small U-Net, BF16 on the tensor
  * cores with FP32 accumulation).  No counterpart in the reference: the
@@ -637,6 +636,7 @@ int sw100_nn_adam(float* param, const float* grad, float* m, float* v, int64_t n
 int sw100_nn_input(const float* dsm, const float* vegdsm, const float* vegdsm2, const float* dem, int rows, int cols,
                    const int32_t* origins, int n, int size, void* x, void* stream);
 
+/* ---------------------------------------------------------------- UTCI -- */
 /* UTCI-only recompute of whole steps: the met fast path of
  * utci_process.py:1093-1196 (recompute_utci_steps), for wind speed / urban
  * heat island edits that leave Tmrt unchanged.  steps: n_steps records whose

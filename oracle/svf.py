@@ -5,7 +5,8 @@
 * :func:`shadow_step_table` -- the scalar part of ``shadow.py:166-247``
   (per-step shifts and height drops of one patch march)
 * :func:`shadow_patch` -- ``shadow.py:166-322`` (one patch march over planes)
-* :func:`svf_calculator` -- ``shadow.py:409-625`` (153-patch sweep + sums)
+* :func:`svf_calculator` -- ``shadow.py:409-625`` (153-patch sweep + sums),
+  split into :func:`patch_tasks`, the marches and :class:`SvfAccumulator`
 """
 from __future__ import annotations
 
@@ -190,89 +191,159 @@ SVF_ORDER = ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg"
              "vegshmat", "vbshvegshmat", "shmat", "svftotal")
 
 
-def svf_calculator(patch_option, amaxvalue, a, vegdem, vegdem2, bush, scale, return_steps=False):
+def patch_tasks(patch_option=2):
+    """The patches of the sweep in the reference's order (shadow.py:447-620):
+    (index, band, azimuth, altitude) per patch, the values passed to the
+    march exactly as svf_calculator passes them."""
+    annulino, altint, _, nband = _PATCH_LAYOUT[patch_option]
+    iaz = patch_azimuths(patch_option)
+    out, index = [], 0
+    for i in range(len(altint)):
+        for _ in range(nband[i]):
+            out.append((index, i, iaz[index], altint[i]))
+            index += 1
+    return out
+
+
+class SvfAccumulator:
+    """The sums of svf_calculator (shadow.py:447-625) fed one patch at a time,
+    in patch order; the marches themselves (shadow_patch) are independent and
+    may run anywhere, in any order."""
+
+    def __init__(self, patch_option, rows, cols, vegdem2):
+        z = lambda: np.zeros((rows, cols), F32)  # noqa: E731
+        self.planes = {k: z() for k in ("svf", "svfE", "svfS", "svfW", "svfN", "svfveg", "svfEveg", "svfSveg",
+                                        "svfWveg", "svfNveg", "svfaveg", "svfEaveg", "svfSaveg", "svfWaveg",
+                                        "svfNaveg")}
+        self.annulino, self.altint, _, self.nband = _PATCH_LAYOUT[patch_option]
+        P = int(sum(self.nband))
+        self.shmat = np.zeros((rows, cols, P), F32)
+        self.vegshmat = np.zeros((rows, cols, P), F32)
+        self.vbshmat = np.zeros((rows, cols, P), F32)
+        nband_t = torch.tensor(self.nband)
+        aniso_t = torch.ceil(nband_t / 2.0)
+        an = self.annulino
+        self.w_iso = [{k: annulus_weight(k, nband_t[i]) for k in range(an[i] + 1, an[i + 1] + 1)}
+                      for i in range(len(self.altint))]
+        self.w_an = [{k: annulus_weight(k, aniso_t[i]) for k in range(an[i] + 1, an[i + 1] + 1)}
+                     for i in range(len(self.altint))]
+        self.vegdem2 = vegdem2
+        self.next = 0
+        self.steps = []
+
+    def add(self, task, sh, vegsh, vbsh, nst):
+        index, i, az, _ = task
+        if index != self.next:
+            raise ValueError(f"patch {index} added out of order (expected {self.next})")
+        self.next += 1
+        self.steps.append(nst)
+        self.shmat[:, :, index] = sh
+        self.vegshmat[:, :, index] = vegsh
+        self.vbshmat[:, :, index] = vbsh
+        P = self.planes
+        inE = 0 <= az < 180
+        inS = 90 <= az < 270
+        inW = 180 <= az < 360
+        inN = az >= 270 or az < 90
+        for k in range(self.annulino[i] + 1, self.annulino[i + 1] + 1):
+            wi, wa = self.w_iso[i][k], self.w_an[i][k]
+            P["svf"] = P["svf"] + wi * sh
+            wsh = wa * sh
+            if inE:
+                P["svfE"] = P["svfE"] + wsh
+            if inS:
+                P["svfS"] = P["svfS"] + wsh
+            if inW:
+                P["svfW"] = P["svfW"] + wsh
+            if inN:
+                P["svfN"] = P["svfN"] + wsh
+            P["svfveg"] = P["svfveg"] + wi * vegsh
+            P["svfaveg"] = P["svfaveg"] + wi * vbsh
+            for d, on in (("E", inE), ("S", inS), ("W", inW), ("N", inN)):
+                if on:
+                    P[f"svf{d}veg"] = P[f"svf{d}veg"] + wa * vegsh
+                    P[f"svf{d}aveg"] = P[f"svf{d}aveg"] + wa * vbsh
+
+    def result(self):
+        """The reference's 19-tuple once every patch has been added."""
+        if self.next != self.shmat.shape[2]:
+            raise ValueError(f"{self.next} of {self.shmat.shape[2]} patches added")
+        P = dict(self.planes)
+        tail = F32(3.0459e-004)
+        P["svfS"] = P["svfS"] + tail
+        P["svfW"] = P["svfW"] + tail
+        for k in ("svf", "svfE", "svfS", "svfW", "svfN"):
+            P[k][P[k] > 1.] = 1.
+        last = np.zeros_like(P["svf"])
+        last[self.vegdem2 == 0.] = tail
+        for k in ("svfSveg", "svfWveg", "svfSaveg", "svfWaveg"):
+            P[k] = P[k] + last
+        for k in ("svfveg", "svfEveg", "svfSveg", "svfWveg", "svfNveg", "svfaveg", "svfEaveg", "svfSaveg",
+                  "svfWaveg", "svfNaveg"):
+            P[k][P[k] > 1.] = 1.
+        trans = F32(0.03)
+        svftotal = P["svf"] - (F32(1) - P["svfveg"]) * (F32(1) - trans)
+        return tuple(P[k] for k in ("svf", "svfaveg", "svfE", "svfEaveg", "svfEveg", "svfN", "svfNaveg",
+                                    "svfNveg", "svfS", "svfSaveg", "svfSveg", "svfveg", "svfW", "svfWaveg",
+                                    "svfWveg")) + (self.vegshmat, self.vbshmat, self.shmat, svftotal)
+
+
+def svf_calculator(patch_option, amaxvalue, a, vegdem, vegdem2, bush, scale, return_steps=False, march_map=None):
     """153-patch sweep (shadow.py:409-625); returns the reference's 19-tuple
-    (15 SVF planes, 3 (rows, cols, P) cubes, SVFtotal)."""
+    (15 SVF planes, 3 (rows, cols, P) cubes, SVFtotal).  ``march_map(tasks)``
+    (optional) yields (task, (sh, vegsh, vbsh, n_steps)) in task order for
+    the scene of this call -- e.g. a process pool set up by march_pool --
+    instead of marching the patches here one after another."""
     a = np.asarray(a, F32)
     vegdem = np.asarray(vegdem, F32)
     vegdem2 = np.asarray(vegdem2, F32)
     bush = np.asarray(bush, F32)
     rows, cols = a.shape
-    z = lambda: np.zeros((rows, cols), F32)  # noqa: E731
-    svf, svfE, svfS, svfW, svfN = z(), z(), z(), z(), z()
-    svfveg, svfEveg, svfSveg, svfWveg, svfNveg = z(), z(), z(), z(), z()
-    svfaveg, svfEaveg, svfSaveg, svfWaveg, svfNaveg = z(), z(), z(), z(), z()
-    annulino, altint, _, nband = _PATCH_LAYOUT[patch_option]
-    P = int(sum(nband))
-    iaz = patch_azimuths(patch_option)
-    shmat = np.zeros((rows, cols, P), F32)
-    vegshmat = np.zeros((rows, cols, P), F32)
-    vbshmat = np.zeros((rows, cols, P), F32)
-    nband_t = torch.tensor(nband)
-    aniso_t = torch.ceil(nband_t / 2.0)
-    steps = []
-    index = 0
-    for i in range(len(altint)):
-        w_iso = {k: annulus_weight(k, nband_t[i]) for k in range(annulino[i] + 1, annulino[i + 1] + 1)}
-        w_an = {k: annulus_weight(k, aniso_t[i]) for k in range(annulino[i] + 1, annulino[i + 1] + 1)}
-        for _ in range(nband[i]):
-            az = iaz[index]
-            sh, vegsh, vbsh, nst = shadow_patch(amaxvalue, a, vegdem, vegdem2, bush, az, altint[i], scale)
-            steps.append(nst)
-            shmat[:, :, index] = sh
-            vegshmat[:, :, index] = vegsh
-            vbshmat[:, :, index] = vbsh
-            inE = 0 <= az < 180
-            inS = 90 <= az < 270
-            inW = 180 <= az < 360
-            inN = az >= 270 or az < 90
-            for k in range(annulino[i] + 1, annulino[i + 1] + 1):
-                wi, wa = w_iso[k], w_an[k]
-                svf = svf + wi * sh
-                wsh = wa * sh
-                if inE:
-                    svfE = svfE + wsh
-                if inS:
-                    svfS = svfS + wsh
-                if inW:
-                    svfW = svfW + wsh
-                if inN:
-                    svfN = svfN + wsh
-                svfveg = svfveg + wi * vegsh
-                svfaveg = svfaveg + wi * vbsh
-                if inE:
-                    svfEveg = svfEveg + wa * vegsh
-                    svfEaveg = svfEaveg + wa * vbsh
-                if inS:
-                    svfSveg = svfSveg + wa * vegsh
-                    svfSaveg = svfSaveg + wa * vbsh
-                if inW:
-                    svfWveg = svfWveg + wa * vegsh
-                    svfWaveg = svfWaveg + wa * vbsh
-                if inN:
-                    svfNveg = svfNveg + wa * vegsh
-                    svfNaveg = svfNaveg + wa * vbsh
-            index += 1
-    tail = F32(3.0459e-004)
-    svfS = svfS + tail
-    svfW = svfW + tail
-    for p in (svf, svfE, svfS, svfW, svfN):
-        p[p > 1.] = 1.
-    last = z()
-    last[vegdem2 == 0.] = tail
-    svfSveg = svfSveg + last
-    svfWveg = svfWveg + last
-    svfSaveg = svfSaveg + last
-    svfWaveg = svfWaveg + last
-    for p in (svfveg, svfEveg, svfSveg, svfWveg, svfNveg, svfaveg, svfEaveg, svfSaveg, svfWaveg, svfNaveg):
-        p[p > 1.] = 1.
-    trans = F32(0.03)
-    svftotal = svf - (F32(1) - svfveg) * (F32(1) - trans)
-    out = (svf, svfaveg, svfE, svfEaveg, svfEveg, svfN, svfNaveg, svfNveg, svfS, svfSaveg, svfSveg,
-           svfveg, svfW, svfWaveg, svfWveg, vegshmat, vbshmat, shmat, svftotal)
+    acc = SvfAccumulator(patch_option, rows, cols, vegdem2)
+    tasks = patch_tasks(patch_option)
+    if march_map is None:
+        for t in tasks:
+            acc.add(t, *shadow_patch(amaxvalue, a, vegdem, vegdem2, bush, t[2], t[3], scale))
+    else:
+        for t, res in march_map(tasks):
+            acc.add(t, *res)
+    out = acc.result()
     if return_steps:
-        return out, np.array(steps)
+        return out, np.array(acc.steps)
     return out
+
+
+# ---- patch marches in worker processes (the CPU timing of the sweep on all
+# host cores; the sums stay in the parent, in patch order, so the result is
+# the serial sweep's bit for bit)
+_SCENE = None
+
+
+def _march_init(scene):
+    global _SCENE
+    torch.set_num_threads(1)   # one process per core
+    _SCENE = scene
+
+
+def _ready(_):
+    import os
+    return os.getpid()
+
+
+def _march_one(task):
+    amaxvalue, a, vegdem, vegdem2, bush, scale = _SCENE
+    return task, shadow_patch(amaxvalue, a, vegdem, vegdem2, bush, task[2], task[3], scale)
+
+
+def march_pool(processes, amaxvalue, a, vegdem, vegdem2, bush, scale):
+    """A spawn-started process pool holding one scene; ``pool.imap(
+    march_one, tasks)`` marches its patches.  Returns (pool, march_one)."""
+    import multiprocessing as mp
+    scene = (amaxvalue, np.asarray(a, F32), np.asarray(vegdem, F32), np.asarray(vegdem2, F32),
+             np.asarray(bush, F32), scale)
+    pool = mp.get_context("spawn").Pool(processes, initializer=_march_init, initargs=(scene,))
+    pool.map(_ready, range(4 * processes), chunksize=1)   # every worker started and holding the scene
+    return pool, _march_one
 
 
 def scene_from_rasters(dsm, trees, dem):

@@ -42,7 +42,7 @@ def clean_landcover(lc):
     return lc
 
 
-def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, altitude, azimuth,
+def iter_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, altitude, azimuth,
                     zen, jday, dectime, altmax, location, scale, amaxvalue=None, landcover_grid=None,
                     lc_class=None, windcoeff=None, time_start=0, time_stop=None,
                     requested_variables=("utci",), initial_state=None, return_final_state=False,
@@ -51,7 +51,10 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
     in the reference's 19-tuple order (cubes (rows, cols, P) float32 or uint8),
     ``met_file`` float64 rows and the float64 (1, T) sun-geometry arrays of
     ``Solweig_2015a_metdata_noload``.  Returns ``{name: (T, rows, cols)}``.
-    ``capture`` (a list) receives per-step intermediate planes."""
+    ``capture`` (a list) receives per-step intermediate planes.
+
+    A generator: yields each step's index after the step, and returns what
+    run_utci_window returns (the CPU timing cuts the loop between steps)."""
     requested = set(requested_variables) | {"utci"}
     unknown = requested - set(VARIABLES)
     if unknown:
@@ -270,6 +273,7 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
                        timeadd=float(timeadd), firstdaytime=float(firstdaytime),
                        Tgmap1=state["Tgmap1"].copy(), TgOut1=state["TgOut1"].copy())
             capture.append(cap)
+        yield i
     if return_final_state:
         # water temperature (utci_process.py:841-846, 917-922): with land
         # cover on, the mean air temperature of the day at every midnight row
@@ -284,3 +288,14 @@ def run_utci_window(*, a, temp1, temp2, walls, dirwalls, svf_bundle, met_file, a
                      Twater=twater, next_step=int(time_stop))
         return outputs, final
     return outputs
+
+
+def run_utci_window(**kwargs):
+    """Full-window time loop (utci_process.py:477-1090); the arguments and
+    return value of iter_utci_window, run to the end."""
+    steps = iter_utci_window(**kwargs)
+    while True:
+        try:
+            next(steps)
+        except StopIteration as done:
+            return done.value

@@ -22,6 +22,26 @@ def test_oracle_svf_bit_exact(case):
         assert_bits_equal(v, d["svf_" + name].astype(np.float32), f"{case} {name}")
 
 
+def test_oracle_svf_march_pool_bit_exact():
+    """The CPU timing's form of the sweep: the patch marches in a spawn pool
+    of two processes, the sums in this process in patch order."""
+    case = "bush24" if "bush24" in SVF_CASES else SVF_CASES[0]
+    d = load_golden(case)
+    vegdsm, vegdsm2, bush, amax = osvf.scene_from_rasters(d["dsm"], d["trees"], d["dem"])
+    pool, one = osvf.march_pool(2, amax, d["dsm"], vegdsm, vegdsm2, bush, float(d["scale"]))
+    try:
+        out = osvf.svf_calculator(2, amax, d["dsm"], vegdsm, vegdsm2, bush, float(d["scale"]),
+                                  march_map=lambda tasks: pool.imap(one, tasks))
+    finally:
+        pool.close()
+        pool.join()
+    for name, v in zip(osvf.SVF_ORDER, out):
+        assert_bits_equal(v, d["svf_" + name].astype(np.float32), f"{case} {name}")
+    acc = osvf.SvfAccumulator(2, *d["dsm"].shape, vegdsm2)
+    with pytest.raises(ValueError, match="out of order"):
+        acc.add(osvf.patch_tasks(2)[1], *out[15:18], 0)
+
+
 @pytest.mark.parametrize("case", FULL_CASES)
 def test_oracle_sun_march_bit_exact(case):
     d = load_golden(case)

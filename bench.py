@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--side", type=int, default=None, help="override the workload's square side (px)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--edits", type=int, default=None,
+                    help="preview1024: seeded edits in all (default 20 x steps)")
+    ap.add_argument("--sites", type=int, default=1, help="preview1024: held-out 1024 x 1024 cities the edits share")
     ap.add_argument("--timeline", action="store_true",
                     help="print the host timeline of one end-to-end call (after the bench line)")
     return ap.parse_args()
@@ -529,8 +532,9 @@ def run_batched(args, world, rank, local):
 
 def run_preview(args, world, rank, local):
     """The learned-preview workload: per seeded edit, the preview's device
-    latency against the exact windowed recompute, and SVF / Tmrt errors
-    against the exact chain (with the stale SVF as the method without it)."""
+    latency against the exact windowed recompute and the full sweep, and SVF
+    / Tmrt errors against the exact chain (with the stale SVF as the method
+    without it), the edits spread over `--sites` held-out cities."""
     import torch
     from solweig_project_b200 import build, synthetic
     from solweig_project_b200 import preview as PV
@@ -539,43 +543,59 @@ def run_preview(args, world, rank, local):
     if rank != 0:
         return
     net = PV.load_pretrained()
-    c = synthetic.make_city(1024, 1024, seed=4242, density=0.3, canopy_cover=0.15)
-    site = DeviceSite(c.dsm, c.trees, c.dem, c.walls, c.aspect, c.scale, landcover=c.landcover,
-                      lc_class=synthetic.default_lc_class(), amaxvalue=48.0)
-    site.run_svf()
     met = synthetic.make_met(1234)
     geo = synthetic.load_sun_geometry("single")
-    ser = site.build_series(met, geo["altitude"], geo["azimuth"], geo["zen"], geo["jday"], geo["dectime"],
-                            geo["altmax"], dict(synthetic.DEFAULT_LOCATION))
-    PV.evaluate_edits(net, site, ser, n_edits=max(1, args.warmup), seed=99)      # warm-up (graph capture etc.)
-    n_edits = max(20, 20 * args.steps)
+    n_edits = args.edits or max(20, 20 * args.steps)
+    n_sites = max(1, min(args.sites, n_edits))
+    rows, per_site, full_all = [], [], []
     with ClockSampler(local) as clocks:
-        rows = PV.evaluate_edits(net, site, ser, n_edits=n_edits, seed=5)
-    full = []
-    for _ in range(3):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        site.launch_svf(site.svf_result.planes, site.svf_result.bits)
-        e1.record()
-        torch.cuda.synchronize()
-        full.append(e0.elapsed_time(e1))
+        for i in range(n_sites):
+            c = synthetic.make_city(1024, 1024, seed=4242 + i, density=0.3, canopy_cover=0.15)
+            site = DeviceSite(c.dsm, c.trees, c.dem, c.walls, c.aspect, c.scale, landcover=c.landcover,
+                              lc_class=synthetic.default_lc_class(), amaxvalue=48.0)
+            site.run_svf()
+            ser = site.build_series(met, geo["altitude"], geo["azimuth"], geo["zen"], geo["jday"], geo["dectime"],
+                                    geo["altmax"], dict(synthetic.DEFAULT_LOCATION))
+            if i == 0:   # warm-up (graph capture etc.)
+                PV.evaluate_edits(net, site, ser, n_edits=max(1, args.warmup), seed=99)
+            n = n_edits // n_sites + (1 if i < n_edits % n_sites else 0)
+            got = PV.evaluate_edits(net, site, ser, n_edits=n, seed=5 + i)
+            full = []
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                site.launch_svf(site.svf_result.planes, site.svf_result.bits)
+                e1.record()
+                torch.cuda.synchronize()
+                full.append(e0.elapsed_time(e1))
+            full_all.append(float(np.median(full)))
+            per_site.append({"seed": 4242 + i, "edits": n, "full_sweep_ms": full_all[-1],
+                             "preview_ms": float(np.median([r["ms_preview"] for r in got])),
+                             "exact_window_ms": float(np.median([r["ms_exact"] for r in got])),
+                             "tmrt_rmse_K": {"preview": float(np.mean([r["tmrt_rmse_preview"] for r in got])),
+                                             "stale": float(np.mean([r["tmrt_rmse_stale"] for r in got]))}})
+            rows += got
+            del site
+            torch.cuda.empty_cache()
     mean = lambda k: float(np.mean([r[k] for r in rows]))  # noqa: E731
     med = lambda k: float(np.median([r[k] for r in rows]))  # noqa: E731
-    full_ms = float(np.median(full))
+    full_ms = float(np.median(full_all))
     clk = clocks.summary()
     print(json.dumps({
         "metric": "SVF edit latency, learned preview (device ms per edit)", "value": med("ms_preview"), "unit": "ms",
         "n_gpus": 1, "steps": n_edits, "warmup": args.warmup, "ms_per_step": med("ms_preview"),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
-        "data": "synthetic (held-out seeded 1024x1024 city, seeded edits)",
+        "data": f"synthetic ({n_sites} held-out seeded 1024x1024 cities, seeded edits)",
         "config": {"workload": "preview1024", "description": WORKLOADS["preview1024"][2], "edits": n_edits,
-                   "net_params": net.n_params, "window": "256x256 (128x128 block + 64 px context)"},
+                   "sites": n_sites, "net_params": net.n_params,
+                   "window": "256x256 (128x128 block + 64 px context)"},
         "exact_window_ms": med("ms_exact"), "full_sweep_ms": full_ms,
         "speedup_vs_exact_window": med("ms_exact") / med("ms_preview"),
         "speedup_vs_full_sweep": full_ms / med("ms_preview"),
         "svf_mae": {"preview": mean("svf_mae_preview"), "stale": mean("svf_mae_stale")},
         "tmrt_rmse_K": {"preview": mean("tmrt_rmse_preview"), "stale": mean("tmrt_rmse_stale")},
         "modes": {m: sum(r["mode"] == m for r in rows) for m in ("preview", "exact")},
+        "per_site": per_site,
         "gpu_launches": None,
         "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "e2e": {"value": med("ms_preview"), "unit": "ms", "h2d_bytes_per_step": 5 * 4 * 40 * 40,

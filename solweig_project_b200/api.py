@@ -365,15 +365,23 @@ def run_exact_chain(*, dsm, trees, dem, walls, aspect, scale, met_file, altitude
     site = E.DeviceSite(dsm, trees, dem, walls, aspect, scale, landcover=landcover, lc_class=lc_class,
                         windcoeff=windcoeff, params=_model_params(model_parameters))
     tl.mark("upload + prepare site", torch.cuda.current_stream())
-    rasters_ready = torch.cuda.Event()   # the sun marches need the rasters only, not the SVF
-    rasters_ready.record()
-    site.run_svf()
-    tl.mark("svf tables + sweep launch", torch.cuda.current_stream())
     if return_device:
+        site.run_svf()
         ser = site.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location)
         return site.run_time_loop(ser, requested=[k for k in N.OUT_BITS if k in requested])
-    # host tables of later steps are built while the GPU runs earlier ones
-    out, _ = site.run_chain_chunked(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
-                                    requested=requested, rasters_ready=rasters_ready, timeline=timeline,
-                                    chunk_steps=chunk_steps)
+    # the host tables depend on the forcing, amaxvalue and the land-cover
+    # classes only: they are built from here on (in the helper process)
+    # while the SVF sweep and the earlier chunks run
+    tables = site.start_tables(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
+                               chunk_steps=chunk_steps)
+    try:
+        rasters_ready = torch.cuda.Event()   # the sun marches need the rasters only, not the SVF
+        rasters_ready.record()
+        site.run_svf()
+        tl.mark("svf tables + sweep launch", torch.cuda.current_stream())
+        out, _ = site.run_chain_chunked(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
+                                        requested=requested, rasters_ready=rasters_ready, timeline=timeline,
+                                        chunk_steps=chunk_steps, tables=tables)
+    finally:
+        tables.finish()
     return out

@@ -22,6 +22,7 @@ import numpy as np
 import torch
 
 from . import _native as N
+from . import hostwork
 from . import tables as T
 from . import timeseries as TS
 
@@ -79,6 +80,11 @@ TENSOR_SUMS = True
 
 # chunks of the chunked time loop whose device buffers are alive at once
 CHUNKS_IN_FLIGHT = 3
+
+# Build the chunked time loop's host tables in the helper process of
+# `hostwork` (overlapping this process's launches and the GPU) rather than in
+# this process between the launches.
+TABLE_PROCESS = False
 
 # host <-> device bytes moved by this module (inputs, tables, results)
 TRANSFER = {"h2d": 0, "d2h": 0}
@@ -664,7 +670,7 @@ class DeviceSite:
 
     def run_chain_chunked(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
                           requested=("utci",), time_start=0, time_stop=None, initial_scalars=None, chunk_steps=8,
-                          rasters_ready=None, timeline=None):
+                          rasters_ready=None, timeline=None, tables=None):
         """The time loop of steps [time_start, time_stop) with the host tables
         built chunk by chunk while the GPU works: the tables of `chunk_steps`
         steps are built, their sun march and flux loop launched and their
@@ -697,22 +703,46 @@ class DeviceSite:
             mask |= N.OUT_BITS[k]
         n_t = time_stop - time_start
         host = {k: torch.empty((n_t, self.rows, self.cols), dtype=torch.float32, pin_memory=True) for k in names}
-        scalars, ring = initial_scalars, collections.deque()
+        ring = collections.deque()
         main, side, copy = torch.cuda.current_stream(), self.side_stream(), self.copy_stream()
         if rasters_ready is None:
             rasters_ready = torch.cuda.Event()
             rasters_ready.record(main)
         side.wait_event(rasters_ready)
         tl = timeline if timeline is not None else Timeline(enabled=False)
-        dc = TS.day_chain(met_file, altitude, azimuth, zen, jday, location, time_start, time_stop)
-        tl.mark("day chain")
+        if tables is None:
+            tables = self.start_tables(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
+                                       time_start, time_stop, chunk_steps, initial_scalars)
+        elif tables.span != (time_start, time_stop, chunk_steps):
+            tables.finish()
+            raise ValueError(f"tables were started for steps / chunks {tables.span}, "
+                             f"not {(time_start, time_stop, chunk_steps)}")
+        try:
+            return self._chunks(tables, names, mask, host, ring, main, side, copy, tl, time_start, time_stop,
+                                chunk_steps)
+        finally:
+            tables.finish()
+
+    def start_tables(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, time_start=0,
+                     time_stop=None, chunk_steps=8, initial_scalars=None):
+        """The host tables of run_chain_chunked's chunks, built from now on:
+        in the helper process of `hostwork` when TABLE_PROCESS is set (so a
+        caller can start them before launching the SVF sweep), else in this
+        process as each chunk is read."""
+        if time_stop is None:
+            time_stop = met_file.shape[0]
+        kw = dict(met_file=met_file, altitude=altitude, azimuth=azimuth, zen=zen, jday=jday, dectime=dectime,
+                  altmax=altmax, location=location, scale=self.scale, amax=self.amax, rows=self.rows,
+                  cols=self.cols, props=self.props, params=self.params)
+        if TABLE_PROCESS:
+            return hostwork.builder().submit(kw, time_start, time_stop, chunk_steps, initial_scalars)
+        return hostwork.LocalTables(kw, time_start, time_stop, chunk_steps, initial_scalars)
+
+    def _chunks(self, tables, names, mask, host, ring, main, side, copy, tl, time_start, time_stop, chunk_steps):
+        scalars = None
         for t0 in range(time_start, time_stop, chunk_steps):
             t1 = min(time_stop, t0 + chunk_steps)
-            ser = TS.build_series(met_file=met_file, altitude=altitude, azimuth=azimuth, zen=zen, jday=jday,
-                                  dectime=dectime, altmax=altmax, location=location, scale=self.scale,
-                                  amax=self.amax, rows=self.rows, cols=self.cols, props=self.props,
-                                  params=self.params, time_start=t0, time_stop=t1, initial_scalars=scalars,
-                                  day_chain=dc)
+            ser = tables.next()
             if ser.class_idx is not None:
                 # the device planes of this site index the tables by the
                 # cleaned land-cover code (device_props); a per-pixel class

@@ -369,9 +369,7 @@ def run_exact_chain(*, dsm, trees, dem, walls, aspect, scale, met_file, altitude
         site.run_svf()
         ser = site.build_series(met_file, altitude, azimuth, zen, jday, dectime, altmax, location)
         return site.run_time_loop(ser, requested=[k for k in N.OUT_BITS if k in requested])
-    # the host tables depend on the forcing, amaxvalue and the land-cover
-    # classes only: they are built from here on (in the helper process)
-    # while the SVF sweep and the earlier chunks run
+    # host tables of later steps are built while the GPU runs earlier ones
     tables = site.start_tables(met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
                                chunk_steps=chunk_steps)
     try:

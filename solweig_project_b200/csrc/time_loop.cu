@@ -326,34 +326,8 @@ __device__ __forceinline__ void time_loop_tile(
     AZ[tid].facesh_hi = gvf_az[tid].facesh_hi;
     AZ[tid].dir_flags = gvf_az[tid].dir_flags;
   }
-  // The tile's pixels, ground pixels first (in tile order), then building
-  // and out-of-grid pixels: a building pixel walks no ground-view ray (its
-  // f is 0 from the first step), so grouping the walking pixels keeps the
-  // walks' warps full.  A stable partition of the 128 slots by warp ballots;
-  // every pixel is still owned by exactly one thread.
-  __shared__ uint8_t ORDER[kTileThreads];
-  __shared__ int WALKERS[kTileThreads / 32];
-  {
-    const int c0 = bx * blockDim.x + threadIdx.x, r0 = by * blockDim.y + threadIdx.y;
-    const bool walks = r0 < rows && c0 < cols && !(site.buildings[(size_t)r0 * cols + c0] == 0.f);
-    const int lane = tid & 31, warp = tid >> 5;
-    const unsigned ball = __ballot_sync(0xffffffffu, walks);
-    const int before = __popc(ball & ((1u << lane) - 1u));
-    __syncthreads();  // the previous tile of a persistent block is done with ORDER
-    if (lane == 0) WALKERS[warp] = __popc(ball);
-    __syncthreads();
-    int total = 0, woff = 0;
-    for (int w = 0; w < nthr / 32; ++w) {
-      total += WALKERS[w];
-      if (w < warp) woff += WALKERS[w];
-    }
-    const int dest = walks ? woff + before : total + (warp * 32 - woff) + (lane - before);
-    ORDER[dest] = (uint8_t)tid;
-    __syncthreads();
-  }
-  const int slot = ORDER[tid];
-  const int c = bx * blockDim.x + slot % blockDim.x;
-  const int r = by * blockDim.y + slot / blockDim.x;
+  const int c = bx * blockDim.x + threadIdx.x;
+  const int r = by * blockDim.y + threadIdx.y;
   const bool live = (r < rows) && (c < cols);
   const size_t npix = (size_t)rows * cols;
   const size_t p = live ? (size_t)r * cols + c : 0;

@@ -22,7 +22,6 @@ import numpy as np
 import torch
 
 from . import _native as N
-from . import hostwork
 from . import tables as T
 from . import timeseries as TS
 
@@ -80,11 +79,6 @@ TENSOR_SUMS = True
 
 # chunks of the chunked time loop whose device buffers are alive at once
 CHUNKS_IN_FLIGHT = 3
-
-# Build the chunked time loop's host tables in the helper process of
-# `hostwork` (overlapping this process's launches and the GPU) rather than in
-# this process between the launches.
-TABLE_PROCESS = False
 
 # host <-> device bytes moved by this module (inputs, tables, results)
 TRANSFER = {"h2d": 0, "d2h": 0}
@@ -725,18 +719,14 @@ class DeviceSite:
 
     def start_tables(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, time_start=0,
                      time_stop=None, chunk_steps=8, initial_scalars=None):
-        """The host tables of run_chain_chunked's chunks, built from now on:
-        in the helper process of `hostwork` when TABLE_PROCESS is set (so a
-        caller can start them before launching the SVF sweep), else in this
-        process as each chunk is read."""
+        """The host tables of run_chain_chunked's chunks, in order, each built
+        when it is read (ChunkTables)."""
         if time_stop is None:
             time_stop = met_file.shape[0]
         kw = dict(met_file=met_file, altitude=altitude, azimuth=azimuth, zen=zen, jday=jday, dectime=dectime,
                   altmax=altmax, location=location, scale=self.scale, amax=self.amax, rows=self.rows,
                   cols=self.cols, props=self.props, params=self.params)
-        if TABLE_PROCESS:
-            return hostwork.builder().submit(kw, time_start, time_stop, chunk_steps, initial_scalars)
-        return hostwork.LocalTables(kw, time_start, time_stop, chunk_steps, initial_scalars)
+        return ChunkTables(kw, time_start, time_stop, chunk_steps, initial_scalars)
 
     def _chunks(self, tables, names, mask, host, ring, main, side, copy, tl, time_start, time_stop, chunk_steps):
         scalars = None
@@ -798,6 +788,35 @@ class DeviceSite:
 
     def state_dict(self):
         return {name: self.state[k].clone() for k, name in enumerate(STATE_NAMES)}
+
+
+class ChunkTables:
+    """The host tables (timeseries.build_series) of steps [time_start,
+    time_stop) in chunks of `chunk_steps`, built in order as next() is
+    called, the carried scalars passed from chunk to chunk and the daytime
+    scalar chain evaluated once for the whole range."""
+
+    def __init__(self, kw, time_start, time_stop, chunk_steps, initial_scalars=None):
+        self.span = (time_start, time_stop, chunk_steps)
+        self._kw, self._scalars, self._dc = kw, initial_scalars, None
+        self._starts = list(range(time_start, time_stop, chunk_steps))
+
+    def next(self):
+        if not self._starts:
+            raise StopIteration
+        kw = self._kw
+        t_start, time_stop, chunk_steps = self.span
+        if self._dc is None:
+            self._dc = TS.day_chain(kw["met_file"], kw["altitude"], kw["azimuth"], kw["zen"], kw["jday"],
+                                    kw["location"], t_start, time_stop)
+        t0 = self._starts.pop(0)
+        ser = TS.build_series(**kw, time_start=t0, time_stop=min(time_stop, t0 + chunk_steps),
+                              initial_scalars=self._scalars, day_chain=self._dc)
+        self._scalars = ser.final
+        return ser
+
+    def finish(self):
+        self._starts = []
 
 
 def utci(ta, rh, tmrt, va) -> torch.Tensor:

@@ -353,13 +353,13 @@ def recompute_utci_steps(met_file, time_indices, tmrt_planes, buildings_dsm, dem
 
 def run_exact_chain(*, dsm, trees, dem, walls, aspect, scale, met_file, altitude, azimuth, zen, jday, dectime,
                     altmax, location, landcover=None, lc_class=None, windcoeff=None, requested=("utci", "tmrt"),
-                    model_parameters=None, return_device=False, timeline=None, chunk_steps=8):
+                    model_parameters=None, return_device=False, timeline=None, chunk_steps=E.DEFAULT_CHUNKS):
     """SVF sweep + time loop for one site from host rasters: the work
     compute_utci does between reading and writing rasters
-    (utci_process.py:1376-1470).  The time loop runs in chunks of
-    ``chunk_steps`` steps whose host tables are built while the GPU runs the
-    previous chunk; ``timeline`` (an engine.Timeline) records the host
-    phases of the call."""
+    (utci_process.py:1376-1470).  The time loop runs in chunks
+    (``chunk_steps``: one length or a sequence of lengths) whose host tables
+    are built while the GPU runs the previous chunk; ``timeline`` (an
+    engine.Timeline) records the host phases of the call."""
     requested = _check_variables(requested)
     tl = timeline if timeline is not None else E.Timeline(enabled=False)
     site = E.DeviceSite(dsm, trees, dem, walls, aspect, scale, landcover=landcover, lc_class=lc_class,

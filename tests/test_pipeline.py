@@ -15,8 +15,21 @@ def _site():
                          lc_class=synthetic.default_lc_class())
 
 
+def test_chunk_bounds():
+    from solweig_project_b200.engine import chunk_bounds
+    assert chunk_bounds(0, 24, 8) == [(0, 8), (8, 16), (16, 24)]
+    assert chunk_bounds(3, 20, 5) == [(3, 8), (8, 13), (13, 18), (18, 20)]
+    assert chunk_bounds(0, 24, (12, 8, 4)) == [(0, 12), (12, 20), (20, 24)]
+    assert chunk_bounds(0, 30, (12, 8, 4)) == [(0, 12), (12, 20), (20, 24), (24, 28), (28, 30)]
+    assert chunk_bounds(0, 10, (12, 8)) == [(0, 10)]
+    assert chunk_bounds(5, 5, 8) == []
+    for bad in (0, (4, 0), ()):
+        with pytest.raises(ValueError):
+            chunk_bounds(0, 24, bad)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("chunk", [1, 5, 24])
+@pytest.mark.parametrize("chunk", [1, 5, 24, (12, 8, 4), (3, 9)])
 def test_chunked_time_loop_equals_single_launch(cuda, chunk):
     import torch
     from solweig_project_b200 import synthetic

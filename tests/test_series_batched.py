@@ -121,3 +121,24 @@ def test_utci_tables_equal_one_step_form():
     for j in range(len(ta)):
         pa, k = TS._utci_table(ta[j], rh[j])
         assert pa.tobytes() == pa_v[j].tobytes() and k.tobytes() == k_v[j].tobytes(), (j, ta[j], rh[j])
+
+
+@pytest.mark.parametrize("e", [4, 0.3, -1.6364])
+def test_float64_powers_match_torch_0dim(e):
+    """The float fast path of _pow_each / _rpow_each returns the 0-dim
+    torch bits (the C library's pow in both)."""
+    import torch
+    from solweig_project_b200 import timeseries as TS
+    rng = np.random.default_rng(7)
+    x = torch.tensor(rng.uniform(0.01, 400.0, 20000), dtype=torch.float64)
+    want = torch.stack([x[k] ** e for k in range(x.shape[0])])
+    assert torch.equal(TS._pow_each(x, e).view(torch.int64), want.view(torch.int64))
+    y = torch.tensor(rng.uniform(-3.0, 3.0, 20000), dtype=torch.float64)
+    for base in (10, 0.935):
+        want = torch.stack([base ** y[k] for k in range(y.shape[0])])
+        assert torch.equal(TS._rpow_each(base, y).view(torch.int64), want.view(torch.int64))
+    # values the float path leaves to torch: zero, negative, overflow
+    z = torch.tensor([0.0, -2.0, 1e300], dtype=torch.float64)
+    assert torch.equal(TS._pow_each(z, 4), torch.stack([z[k] ** 4 for k in range(3)]))
+    big = torch.tensor([400.0, 1.0], dtype=torch.float64)
+    assert torch.equal(TS._rpow_each(10, big), torch.stack([10 ** big[k] for k in range(2)]))

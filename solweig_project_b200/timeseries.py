@@ -1006,17 +1006,20 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     suntab = T.sun_tables([float(azimuth[0][i]) for i in rows_day], [float(altitude[0][i]) for i in rows_day],
                           scale, float(amax), rows, cols)
     lcyl_rows, kside_rows = [], []
+    # per-step fields that are elementwise roundings of the vectors above
+    ta32_v = np.asarray(Ta_all[idx_t], np.float64).astype(F32)
+    steps["ta32"] = ta32_v
+    steps["ta4"] = ta4_v.numpy().astype(F32)
+    steps["night_lup_base"] = ((F32(0) + ta32_v) + F32(0)) + F32(273.15)
+    esky_py = esky_v.tolist()
+    lag_rows, lag_timeadd = [], []    # thermal-lag exponent of each daytime step, evaluated after the loop
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
             CI = 1.
-        esky = esky_v[o]
-        ta32 = F32(float(Ta_all[i]))
-        S["ta32"] = ta32
-        S["ta4"] = F32(ta4_v[o].item())
-        S["night_lup_base"] = ((F32(0) + ta32) + F32(0)) + F32(273.15)
+        esky = esky_py[o]
         Q = patch[o]
-        if torch.tensor(altitude[0][i]) > 0:
+        if altitude[0][i] > 0:
             S["is_day"] = 1
             S["day_row"] = len(sun_rows)
             d = dc["pos"][i]
@@ -1052,15 +1055,15 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             S["lwall"] = lwall_d[kd]
             # thermal lag weights (solweig.py:451-488), one timeadd for all six planes
             S["tw_first"] = int(firstdaytime == 1)
+            lag_rows.append(o)
             if timeadd >= (59 / 1440):
-                w = torch.exp(-33.27 * torch.tensor(timeadd))
+                lag_timeadd.append(timeadd)
                 S["tw_mode"] = 1
                 timeadd = timestepdec if timestepdec > (59 / 1440) else 0
             else:
                 timeadd = timeadd + timestepdec
-                w = torch.exp(-33.27 * torch.tensor(timeadd))
+                lag_timeadd.append(timeadd)
                 S["tw_mode"] = 0
-            S["tw_a"], S["tw_b"] = F32((1 - w).item()), F32(w.item())
             firstdaytime = 0
             # shortwave scalars
             S["radI"], S["radD"], S["radG"] = F32(radI.item()), F32(radD.item()), F32(float(radG_all[i]))
@@ -1082,10 +1085,25 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
             L_patches = night_patches
             sun_surf = F32(0)
         if CI < 0.95:
-            esky = CI * esky + (1 - CI) * 1.
+            # the 0-dim form's promotions: CI (float32 tensor or float) times
+            # the float64 esky in float64; 1 - CI in CI's own precision
+            one_minus = float(F32(1) - F32(CI)) if isinstance(CI, torch.Tensor) else 1 - CI
+            esky = float(CI) * esky + one_minus * 1.
         # Lcyl per patch (solweig.py:1651-1760): evaluated after the loop for
         # all steps of each patch layout at once
-        lcyl_rows.append((o, L_patches[:, 0], esky, sun_surf))
+        lcyl_rows.append((o, L_patches[:, 0], torch.tensor(esky, dtype=torch.float64), sun_surf))
+    # TsWaveDelay weights (solweig.py:451-488): exp(-33.27 * timeadd) with
+    # timeadd made a tensor as the 0-dim form makes it (float32 from a
+    # Python float, float64 from a numpy float64 such as a dectime
+    # difference: torch.tensor's own dtype choice, per element) and rounded
+    # to float32 at the end; a vector element has the 0-dim bits
+    kinds = [torch.tensor(v).dtype for v in lag_timeadd]
+    for kind in set(kinds):
+        sel_ = [k for k, d in enumerate(kinds) if d == kind]
+        w = torch.exp(-33.27 * torch.tensor([lag_timeadd[k] for k in sel_], dtype=kind))
+        rows_ = [lag_rows[k] for k in sel_]
+        steps["tw_a"][rows_] = (1 - w).numpy().astype(F32)
+        steps["tw_b"][rows_] = w.numpy().astype(F32)
     _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t)
     _kside_tables(patch, kside_rows, diff_vals, params.albedo_b, azimuth, altitude)
     sun = np.array(sun_rows, N.SUN_STEP_DTYPE) if sun_rows else np.zeros(0, N.SUN_STEP_DTYPE)

@@ -174,11 +174,13 @@ def _diffuse(radG, altitude, Kt, Ta, RH):
 # 0-dim elements one at a time; and where two 0-dim tensors of different
 # dtypes meet, the vector form casts explicitly to the dtype torch's
 # promotion of the 0-dim pair gives.
-# A float64 0-dim torch power with a general exponent is the C library's
-# pow(), the function Python's float ** calls (torch special-cases only the
-# exponents below): for float64 operands with positive bases the Python
-# floats give the same bits, checked on 20k random inputs per exponent in
-# tests/test_series_batched.py, without a tensor per element.
+# 0-dim torch powers with a general exponent, reproduced without a tensor per
+# element (checked on 20k random inputs per case in
+# tests/test_series_batched.py; torch special-cases only the exponents
+# below): a float64 x ** e is the C library's pow(), which Python's float **
+# calls; a float32 x ** e is that double pow() of x and e rounded once to
+# float32; c ** x for a float32 x is powf of float32(c), which numpy's
+# float32 scalar ** calls.
 _TORCH_SPECIAL_EXPONENTS = (0.5, -0.5, 1.0, 2.0, 3.0, -1.0, -2.0, 0.0)
 
 
@@ -186,13 +188,17 @@ def _pow_each(x, e):
     """x ** e element by element on 0-dim tensors (e a number or a vector)."""
     if isinstance(e, torch.Tensor):
         return torch.stack([torch.pow(x[k], e[k]) for k in range(x.shape[0])]) if x.shape[0] else x
-    if x.dtype == torch.float64 and float(e) not in _TORCH_SPECIAL_EXPONENTS:
+    if x.dtype in (torch.float64, torch.float32) and float(e) not in _TORCH_SPECIAL_EXPONENTS:
         vals = x.tolist()
         if all(v > 0.0 and v != float("inf") for v in vals):
             try:
-                return torch.tensor([v ** e for v in vals], dtype=torch.float64)
+                r = [v ** e for v in vals]
             except OverflowError:   # torch gives inf there: its own path below
-                pass
+                r = None
+            if r is not None:
+                if x.dtype == torch.float64:
+                    return torch.tensor(r, dtype=torch.float64)
+                return torch.from_numpy(np.array(r, np.float64).astype(np.float32))
     return torch.stack([x[k] ** e for k in range(x.shape[0])]) if x.shape[0] else x
 
 
@@ -205,6 +211,12 @@ def _rpow_each(base, x):
                 return torch.tensor([float(base) ** v for v in vals], dtype=torch.float64)
             except OverflowError:
                 pass
+    if x.dtype == torch.float32 and isinstance(base, (int, float)) and base > 0:
+        xs = x.numpy()
+        if np.isfinite(xs).all():
+            b32 = np.float32(base)
+            with np.errstate(over="ignore", under="ignore"):
+                return torch.from_numpy(np.array([b32 ** v for v in xs], np.float32))
     return torch.stack([base ** x[k] for k in range(x.shape[0])]) if x.shape[0] else x
 
 

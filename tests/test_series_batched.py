@@ -142,3 +142,17 @@ def test_float64_powers_match_torch_0dim(e):
     assert torch.equal(TS._pow_each(z, 4), torch.stack([z[k] ** 4 for k in range(3)]))
     big = torch.tensor([400.0, 1.0], dtype=torch.float64)
     assert torch.equal(TS._rpow_each(10, big), torch.stack([10 ** big[k] for k in range(2)]))
+
+
+@pytest.mark.parametrize("e", [4, 0.3, -1.6364])
+def test_float32_powers_match_torch_0dim(e):
+    rng = np.random.default_rng(11)
+    x = torch.tensor(rng.uniform(0.01, 400.0, 20000), dtype=torch.float32)
+    want = torch.stack([x[k] ** e for k in range(x.shape[0])])
+    got = TS._pow_each(x, e)
+    assert got.dtype == torch.float32 and torch.equal(got.view(torch.int32), want.view(torch.int32))
+    y = torch.tensor(rng.uniform(-3.0, 40.0, 20000), dtype=torch.float32)
+    for base in (10, 0.935):
+        want = torch.stack([base ** y[k] for k in range(y.shape[0])])
+        got = TS._rpow_each(base, y)
+        assert got.dtype == torch.float32 and torch.equal(got.view(torch.int32), want.view(torch.int32))

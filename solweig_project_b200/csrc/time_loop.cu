@@ -276,6 +276,15 @@ constexpr float kR09 = 0x1.1c71c8p+0f;
 constexpr float kR18 = 0x1.c71c72p-5f;
 constexpr float kR9 = 0x1.c71c72p-4f;
 
+// a float64 term added to a sum: in float64 and rounded to float32 each
+// time (the reference's float32 array += float64 scalar), or kept in
+// float64 (HELD: the sum is a double)
+template <bool HELD, class A>
+__device__ __forceinline__ void acc64(A& acc, double term) {
+  if constexpr (HELD) acc = acc + term;
+  else acc = add64(acc, term);
+}
+
 struct GvfSums {
   float Lup, alb, albnosh;
   float LupE, albE, albnoshE, LupS, albS, albnoshS, LupW, albW, albnoshW, LupN, albN, albnoshN;
@@ -514,6 +523,13 @@ __device__ __forceinline__ void time_loop_tile(
     float ksideD = 0.f, kref_sun = 0.f, kref_sh = 0.f, kref_veg = 0.f, anilum = 0.f;
     float ld_sky = 0.f, ld_veg = 0.f, ld_sh = 0.f, ld_sun = 0.f, ld_ref = 0.f;
     float ls_sky = 0.f, ls_veg = 0.f, ls_sh = 0.f, ls_sun = 0.f, ls_ref = 0.f;
+    // The float64 increments (vegetation and shaded-wall longwave): the
+    // reference adds each to a float32 sum in float64 and rounds (add64).
+    // With the dense sums from the tensor cores the fluxes are already held
+    // to the Tmrt tolerance rather than to the reference's bits, and these
+    // four sums stay in float64 until the end: no conversion per term.
+    using Acc64 = typename std::conditional<SUMS, double, float>::type;
+    Acc64 ls_veg_a = 0, ld_veg_a = 0, ls_sh_a = 0, ld_sh_a = 0;
     const bool day = is_day;
     if (SUMS) {
       const float* sp = sums + (size_t)t * 4 * npix + p;
@@ -577,8 +593,8 @@ __device__ __forceinline__ void time_loop_tile(
         const uint32_t bit = 1u << j;
         const PatchRec& Q = PP[q0 + j];
         if (mveg & bit) {
-          ls_veg = add64(ls_veg, Q.veg_cos);
-          ld_veg = add64(ld_veg, Q.veg_sin);
+          acc64<SUMS>(ls_veg_a, Q.veg_cos);
+          acc64<SUMS>(ld_veg_a, Q.veg_sin);
           if (day) kref_veg = kref_veg + Q.kref_veg;
         }
         if (mwall & bit) {
@@ -590,10 +606,10 @@ __device__ __forceinline__ void time_loop_tile(
           if (Q.flags & 1) {
             const float td = hsvf + Q.yi_l;
             if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
-            if (td > Q.thr_shd) { ls_sh = add64(ls_sh, Q.sh_cos); ld_sh = add64(ld_sh, Q.sh_sin); }
+            if (td > Q.thr_shd) { acc64<SUMS>(ls_sh_a, Q.sh_cos); acc64<SUMS>(ld_sh_a, Q.sh_sin); }
           } else {
-            ls_sh = add64(ls_sh, Q.sh_cos);
-            ld_sh = add64(ld_sh, Q.sh_sin);
+            acc64<SUMS>(ls_sh_a, Q.sh_cos);
+            acc64<SUMS>(ld_sh_a, Q.sh_sin);
           }
         }
         const float rs = refl * Q.ster;
@@ -606,6 +622,7 @@ __device__ __forceinline__ void time_loop_tile(
       const float dRad = anilum * P.radD;
       Kdown = ((P.radI * shadow) * P.sin_alt + dRad) + albF_day;
     }
+    ls_veg = (float)ls_veg_a; ld_veg = (float)ld_veg_a; ls_sh = (float)ls_sh_a; ld_sh = (float)ld_sh_a;
     const float Lside = (((ls_sky + ls_veg) + ls_sh) + ls_sun) + ls_ref;
     const float Ldown = (((ld_sky + ld_veg) + ld_sh) + ld_sun) + ld_ref;
     // ---------------- Tmrt (cyl == 1, anisotropic sky)

@@ -247,7 +247,12 @@ __device__ __noinline__ GvfWalk gvf_walk_known_edge(const float4* __restrict__ G
 // x - q * d is exact in one FMA, and q + r * rd rounded once is the
 // correctly rounded quotient -- the IEEE float32 x / d -- for operands in the
 // normal range.  Three instructions instead of a full division.
+// FAST: x * rd alone (within one ulp of the quotient), for the loop variant
+// whose fluxes are held to the Tmrt tolerance rather than to the
+// reference's bits.
+template <bool FAST = false>
 __device__ __forceinline__ float div_by(float x, float d, float rd) {
+  if constexpr (FAST) return __fmul_rn(x, rd);
   const float q = __fmul_rn(x, rd);
   const float r = __fmaf_rn(-q, d, x);
   return __fmaf_rn(r, rd, q);
@@ -267,7 +272,9 @@ struct StepDiv {
 // `x / d * sel + y / e * (1 - sel)` of the reference with sel in {0, 1}:
 // one of the two products is an exact zero, so only one quotient is needed
 // (the zero is still added, keeping the float32 result identical)
+template <bool FAST = false>
 __device__ __forceinline__ float pick_div(bool sel, float x, float d, float rd, float y, float e, float re) {
+  if constexpr (FAST) return sel ? __fmul_rn(x, rd) : __fmul_rn(y, re);
   return sel ? (div_by(x, d, rd) + 0.f) : (0.f + div_by(y, e, re));
 }
 
@@ -460,15 +467,15 @@ __device__ __forceinline__ void time_loop_tile(
         if (keep == -1.f) keep = 0.f;
         const bool kz = keep == 1.f;
         if (kz) { wLwall = 0.f; walbwall = 0.f; }
-        const float gLup1 = pick_div(wsi_f, s_Lwall + W.qLup, D.f1, D.rf1, W.qLup, D.first, D.rfirst);
-        const float gLup2 = pick_div(wsi_s, wLwall + W.sLup, D.s1, D.rs1, W.sLup, D.second, D.rsecond);
-        const float galb1 = pick_div(wsi_f, s_albwall + W.qAlb, D.f1, D.rf1, W.qAlb, D.first, D.rfirst);
-        const float galb2 = pick_div(wsi_s, walbwall + W.sAlb, D.s1, D.rs1, W.sAlb, D.second, D.rsecond);
-        const float gan1 = pick_div(wi_f, s_albwallnosh + W.qNosh, D.f1, D.rf1, W.qNosh, D.first, D.rfirst);
-        const float gan2 = pick_div(wi_s, walbwallnosh + W.sNosh, D.second, D.rsecond, W.sNosh, D.second, D.rsecond);
-        const float gLup = div_by(gLup1 * 0.5f + gLup2 * 0.4f, 0.9f, kR09) + lup_own * nb;
-        const float galb = div_by(galb1 * 0.5f + galb2 * 0.4f, 0.9f, kR09) + (alb * nb) * shadow;
-        const float gan = div_by(gan1 * 0.5f + gan2 * 0.4f, 0.9f, kR09) * bld + alb * nb;
+        const float gLup1 = pick_div<SUMS>(wsi_f, s_Lwall + W.qLup, D.f1, D.rf1, W.qLup, D.first, D.rfirst);
+        const float gLup2 = pick_div<SUMS>(wsi_s, wLwall + W.sLup, D.s1, D.rs1, W.sLup, D.second, D.rsecond);
+        const float galb1 = pick_div<SUMS>(wsi_f, s_albwall + W.qAlb, D.f1, D.rf1, W.qAlb, D.first, D.rfirst);
+        const float galb2 = pick_div<SUMS>(wsi_s, walbwall + W.sAlb, D.s1, D.rs1, W.sAlb, D.second, D.rsecond);
+        const float gan1 = pick_div<SUMS>(wi_f, s_albwallnosh + W.qNosh, D.f1, D.rf1, W.qNosh, D.first, D.rfirst);
+        const float gan2 = pick_div<SUMS>(wi_s, walbwallnosh + W.sNosh, D.second, D.rsecond, W.sNosh, D.second, D.rsecond);
+        const float gLup = div_by<SUMS>(gLup1 * 0.5f + gLup2 * 0.4f, 0.9f, kR09) + lup_own * nb;
+        const float galb = div_by<SUMS>(galb1 * 0.5f + galb2 * 0.4f, 0.9f, kR09) + (alb * nb) * shadow;
+        const float gan = div_by<SUMS>(gan1 * 0.5f + gan2 * 0.4f, 0.9f, kR09) * bld + alb * nb;
         S.Lup = S.Lup + gLup;
         S.alb = S.alb + galb;
         S.albnosh = S.albnosh + gan;
@@ -480,14 +487,14 @@ __device__ __forceinline__ void time_loop_tile(
       }
       n0_second = second_i;
       const float lup_air = (P.sbc * emis) * P.ta4;
-      const float gvfLup = div_by(S.Lup, 18.f, kR18) + lup_air;
-      const float gvfalb = div_by(S.alb, 18.f, kR18), gvfalbnosh = div_by(S.albnosh, 18.f, kR18);
-      const float gvfLupE = div_by(S.LupE, 9.f, kR9) + lup_air, gvfLupS = div_by(S.LupS, 9.f, kR9) + lup_air;
-      const float gvfLupW = div_by(S.LupW, 9.f, kR9) + lup_air, gvfLupN = div_by(S.LupN, 9.f, kR9) + lup_air;
-      const float gvfalbE = div_by(S.albE, 9.f, kR9), gvfalbS = div_by(S.albS, 9.f, kR9);
-      const float gvfalbW = div_by(S.albW, 9.f, kR9), gvfalbN = div_by(S.albN, 9.f, kR9);
-      const float ganE = div_by(S.albnoshE, 9.f, kR9), ganS = div_by(S.albnoshS, 9.f, kR9);
-      const float ganW = div_by(S.albnoshW, 9.f, kR9), ganN = div_by(S.albnoshN, 9.f, kR9);
+      const float gvfLup = div_by<SUMS>(S.Lup, 18.f, kR18) + lup_air;
+      const float gvfalb = div_by<SUMS>(S.alb, 18.f, kR18), gvfalbnosh = div_by<SUMS>(S.albnosh, 18.f, kR18);
+      const float gvfLupE = div_by<SUMS>(S.LupE, 9.f, kR9) + lup_air, gvfLupS = div_by<SUMS>(S.LupS, 9.f, kR9) + lup_air;
+      const float gvfLupW = div_by<SUMS>(S.LupW, 9.f, kR9) + lup_air, gvfLupN = div_by<SUMS>(S.LupN, 9.f, kR9) + lup_air;
+      const float gvfalbE = div_by<SUMS>(S.albE, 9.f, kR9), gvfalbS = div_by<SUMS>(S.albS, 9.f, kR9);
+      const float gvfalbW = div_by<SUMS>(S.albW, 9.f, kR9), gvfalbN = div_by<SUMS>(S.albN, 9.f, kR9);
+      const float ganE = div_by<SUMS>(S.albnoshE, 9.f, kR9), ganS = div_by<SUMS>(S.albnoshS, 9.f, kR9);
+      const float ganW = div_by<SUMS>(S.albnoshW, 9.f, kR9), ganN = div_by<SUMS>(S.albnoshN, 9.f, kR9);
       // ---------------- thermal lag (state in registers)
       const float tgtemp = tg * shadow + P.ta32;
       const float g0[6] = {gvfLup, gvfLupE, gvfLupS, gvfLupW, gvfLupN, tgtemp};
@@ -578,6 +585,7 @@ __device__ __forceinline__ void time_loop_tile(
     // shaded_or_sunlit predicate).  Each accumulator still receives its
     // terms in patch order.
     const float refl = (((ld_sky + Lup) * P.refl_k) * 0.5f) / 3.14159274101257324f;
+    float ref_c = 0.f, ref_s = 0.f;   // sums of ster * cos / sin over the reflecting patches (SUMS)
 #pragma unroll
     for (int w = 0; w < SW100_CUBE_WORDS; ++w) {
       const int q0 = w * 32;
@@ -612,10 +620,19 @@ __device__ __forceinline__ void time_loop_tile(
             acc64<SUMS>(ld_sh_a, Q.sh_sin);
           }
         }
-        const float rs = refl * Q.ster;
-        ls_ref = ls_ref + rs * Q.cos_alt;
-        ld_ref = ld_ref + rs * Q.sin_alt;
+        if constexpr (SUMS) {   // refl * sum(ster * cos) once, below
+          ref_c = __fmaf_rn(Q.ster, Q.cos_alt, ref_c);
+          ref_s = __fmaf_rn(Q.ster, Q.sin_alt, ref_s);
+        } else {
+          const float rs = refl * Q.ster;
+          ls_ref = ls_ref + rs * Q.cos_alt;
+          ld_ref = ld_ref + rs * Q.sin_alt;
+        }
       }
+    }
+    if constexpr (SUMS) {
+      ls_ref = refl * ref_c;
+      ld_ref = refl * ref_s;
     }
     if (day) {
       Kside = (((ksideI + ksideD) + kref_sun) + kref_sh) + kref_veg;

@@ -566,7 +566,14 @@ int sw100_patch_sums(const sw100_site_planes* site, int rows, int cols, const sw
 
 /* sw100_flux_loop with the dense patch sums taken from `sums` (as written
  * by sw100_patch_sums for the same series) instead of computed in the
- * loop. */
+ * loop.  Its fluxes are held to the Tmrt / UTCI tolerance of the chain
+ * (1e-3 K / 1e-3 C against the reference) rather than to the reference's
+ * float32 operation order: besides the tensor-core sums, the vegetation and
+ * shaded-wall longwave sums stay in float64 to the end, the reflected
+ * longwave is refl x sum(ster x cos) by FMA, and the ground-view weights
+ * divide by multiplying with the step's reciprocals.  Shadows and every
+ * predicate (sunlit / shaded walls, the first-building walks) are the
+ * reference's. */
 int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
                          const float* gsrc, const float* sums, float* state, uint32_t out_mask, float* outputs,
                          void* stream);

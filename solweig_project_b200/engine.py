@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import collections
 import ctypes as C
+import threading
 from dataclasses import dataclass
 
 import numpy as np
@@ -88,6 +89,24 @@ DEFAULT_CHUNKS = (14, 6, 4, 8)
 
 # host <-> device bytes moved by this module (inputs, tables, results)
 TRANSFER = {"h2d": 0, "d2h": 0}
+
+
+# The chunked loop's side and copy streams, one of each per device for the
+# whole process.  The caching allocator keeps freed blocks per stream, so
+# buffers allocated on a stream of a site's own would never be reused by the
+# next site's: every call would go back to cudaMalloc, which can wait for
+# the device.
+_STREAMS = {}
+_STREAMS_LOCK = threading.Lock()
+
+
+def _shared_stream(device, role):
+    dev = torch.device(device)
+    key = (dev.index if dev.index is not None else torch.cuda.current_device(), role)
+    with _STREAMS_LOCK:
+        if key not in _STREAMS:
+            _STREAMS[key] = torch.cuda.Stream(device=key[0])
+        return _STREAMS[key]
 
 
 def _upload(host: torch.Tensor, device) -> torch.Tensor:
@@ -656,17 +675,15 @@ class DeviceSite:
                    _ptr(sums), _ptr(self.state), out_mask, _ptr(outputs), _stream())
 
     def copy_stream(self) -> torch.cuda.Stream:
-        """Stream of the chunked loop's device-to-host output copies."""
-        if getattr(self, "_copy", None) is None:
-            self._copy = torch.cuda.Stream(device=self.device)
-        return self._copy
+        """Stream of the chunked loop's device-to-host output copies (one per
+        device, shared by all sites)."""
+        return _shared_stream(self.device, "copy")
 
     def side_stream(self) -> torch.cuda.Stream:
-        """Second stream of this site: sun marches, which read only the
-        rasters, run there beside the SVF sweep and the flux loops."""
-        if getattr(self, "_side", None) is None:
-            self._side = torch.cuda.Stream(device=self.device)
-        return self._side
+        """Second stream: sun marches, which read only the rasters, run there
+        beside the SVF sweep and the flux loops (one per device, shared by
+        all sites)."""
+        return _shared_stream(self.device, "side")
 
     def run_chain_chunked(self, met_file, altitude, azimuth, zen, jday, dectime, altmax, location,
                           requested=("utci",), time_start=0, time_stop=None, initial_scalars=None,

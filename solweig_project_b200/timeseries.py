@@ -923,8 +923,6 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     P = int(sum(T.PATCH_LAYOUT[patch_option][3]))
     steps = np.zeros(n_t, N.TIME_STEP_DTYPE)
     patch = np.zeros((n_t, P), N.PATCH_STEP_DTYPE)
-    sun_rows, tables = [], []
-    sun_off = 0
     sbc_t = torch.tensor(SBC)
     ewall_t = torch.tensor(params.ewall)
     deg2rad_t = torch.tensor(np.pi / 180)
@@ -1025,46 +1023,26 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     steps["night_lup_base"] = ((F32(0) + ta32_v) + F32(0)) + F32(273.15)
     esky_py = esky_v.tolist()
     lag_rows, lag_timeadd = [], []    # thermal-lag exponent of each daytime step, evaluated after the loop
+    # the daytime clearness index min(CI, 1.0) of each daytime row: the
+    # float32 tensor element unless 1.0 < CI (then the float 1.0)
+    n_dr = len(rows_day)
+    pos_day = [dc["pos"][i] for i in rows_day]
+    ci_vals = dc["CI"][pos_day].tolist() if n_dr else []
+    day_o = [i - time_start for i in rows_day]
+    ci_f32 = False   # the carried CI is a float until a daytime row sets it
     for o, i in enumerate(range(time_start, time_stop)):
         S = steps[o]
         if (dectime[i] - np.floor(dectime[i])) == 0:
-            CI = 1.
+            CI, ci_f32 = 1., False
         esky = esky_py[o]
-        Q = patch[o]
         if altitude[0][i] > 0:
-            S["is_day"] = 1
-            S["day_row"] = len(sun_rows)
-            d = dc["pos"][i]
-            SNUP, I0, CI = dc["snup"][d], dc["I0"][d], dc["CI"][d]
-            CI = min(CI, 1.0)
-            radI, radD = dc["radI"][d], dc["radD"][d]
+            kd = day_k[i]
+            d = pos_day[kd]
+            CI, ci_f32 = (1.0, False) if 1.0 < ci_vals[kd] else (ci_vals[kd], True)
             lv = dc["lv"][d]
             if lv is None:   # sun below the horizon in the Perez geometry: the 0-dim form
                 lv = _perez((torch.tensor(zen[0][i]) * (180 / np.pi)).item(), torch.tensor(azimuth[0][i]).item(),
-                            radD, radI, jday[0][i].item())
-            # sun march table and wall-face bounds
-            dx, dy, dz, az_f, face = suntab[day_k[i]]
-            t = np.zeros(len(dz), N.STEP_DTYPE)
-            t["dx"], t["dy"], t["dz"] = dx, dy, dz
-            tables.append(t)
-            srow = np.zeros(1, N.SUN_STEP_DTYPE)[0]
-            srow["step_offset"], srow["step_count"], srow["t"] = sun_off, len(dz), o
-            srow["facesh_mode"], srow["facesh_lo"], srow["facesh_hi"] = face
-            srow["psi_term"] = F32(1) - psi[i]
-            sun_rows.append(srow)
-            sun_off += len(dz)
-            # ground temperature wave (solweig.py:2101-2122)
-            kd = day_k[i]
-            CI_TgG = min(cig_v[kd], 1.0)
-            S["cig"] = F32(float(CI_TgG))
-            S["altmax32"] = F32(float(altmax[0][i]))
-            fac_n = fac_v[kd]
-            if code_slot is None:
-                S["tg_factor"][:len(tvals)] = fac_n
-            else:
-                for code, k in code_slot.items():
-                    S["tg_factor"][code] = fac_n[k]
-            S["lwall"] = lwall_d[kd]
+                            dc["radD"][d], dc["radI"][d], jday[0][i].item())
             # thermal lag weights (solweig.py:451-488), one timeadd for all six planes
             S["tw_first"] = int(firstdaytime == 1)
             lag_rows.append(o)
@@ -1077,21 +1055,13 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
                 lag_timeadd.append(timeadd)
                 S["tw_mode"] = 0
             firstdaytime = 0
-            # shortwave scalars
-            S["radI"], S["radD"], S["radG"] = F32(radI.item()), F32(radD.item()), F32(float(radG_all[i]))
-            S["sin_alt"], S["cos_alt"] = sw_v["sin_alt"][kd], sw_v["cos_alt"][kd]
-            S["tan_beta"], S["qa"] = sw_v["tan_beta"][kd], sw_v["qa"][kd]
-            alt32 = sw_v["alt32"][kd]
             # Kside per patch (solweig.py:683-724): after the loop, all daytime
             # steps of each patch layout at once
-            kside_rows.append((o, i, lv, radD, radI, alt32))
+            kside_rows.append((o, i, lv, dc["radD"][d], dc["radI"][d], sw_v["alt32"][kd]))
             L_patches = lv
             # sunlit wall surface of define_patch_characteristics (solweig.py:1596)
             sun_surf = sunsurf_d[kd]
         else:
-            S["is_day"] = 0
-            S["day_row"] = -1
-            S["tg_factor"][:] = 0
             timeadd = 0
             firstdaytime = 1
             L_patches = night_patches
@@ -1099,11 +1069,45 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         if CI < 0.95:
             # the 0-dim form's promotions: CI (float32 tensor or float) times
             # the float64 esky in float64; 1 - CI in CI's own precision
-            one_minus = float(F32(1) - F32(CI)) if isinstance(CI, torch.Tensor) else 1 - CI
+            one_minus = float(F32(1) - F32(CI)) if ci_f32 else 1 - CI
             esky = float(CI) * esky + one_minus * 1.
         # Lcyl per patch (solweig.py:1651-1760): evaluated after the loop for
         # all steps of each patch layout at once
         lcyl_rows.append((o, L_patches[:, 0], torch.tensor(esky, dtype=torch.float64), sun_surf))
+    # the per-daytime-step fields, as columns (each element the value the
+    # step form stored: float32 roundings of the same float64 / float32 values)
+    steps["day_row"] = -1
+    if n_dr:
+        steps["is_day"][day_o] = 1
+        steps["day_row"][day_o] = np.arange(n_dr)
+        counts = np.array([len(suntab[k][2]) for k in range(n_dr)], np.int64)
+        offs = np.concatenate([[0], np.cumsum(counts)[:-1]])
+        sun_rows = np.zeros(n_dr, N.SUN_STEP_DTYPE)
+        sun_rows["step_offset"], sun_rows["step_count"], sun_rows["t"] = offs, counts, day_o
+        sun_rows["facesh_mode"] = [suntab[k][4][0] for k in range(n_dr)]
+        sun_rows["facesh_lo"] = [suntab[k][4][1] for k in range(n_dr)]
+        sun_rows["facesh_hi"] = [suntab[k][4][2] for k in range(n_dr)]
+        sun_rows["psi_term"] = F32(1) - np.asarray(psi, F32)[rows_day]
+        tables = [np.zeros(int(counts.sum()), N.STEP_DTYPE)]
+        tables[0]["dx"] = np.concatenate([suntab[k][0] for k in range(n_dr)])
+        tables[0]["dy"] = np.concatenate([suntab[k][1] for k in range(n_dr)])
+        tables[0]["dz"] = np.concatenate([suntab[k][2] for k in range(n_dr)])
+        # ground temperature wave (solweig.py:2101-2122)
+        cig = cig_v.numpy()
+        steps["cig"][day_o] = np.where(1.0 < cig, 1.0, cig).astype(F32)
+        steps["altmax32"][day_o] = np.asarray(altmax[0], np.float64)[rows_day].astype(F32)
+        if code_slot is None:
+            steps["tg_factor"][day_o, :len(tvals)] = fac_v
+        else:
+            for code, k in code_slot.items():
+                steps["tg_factor"][day_o, code] = fac_v[:, k]
+        steps["lwall"][day_o] = lwall_d
+        # shortwave scalars
+        steps["radI"][day_o] = dc["radI"][pos_day].numpy().astype(F32)
+        steps["radD"][day_o] = dc["radD"][pos_day].numpy().astype(F32)
+        steps["radG"][day_o] = np.asarray(radG_all, np.float64)[rows_day].astype(F32)
+        for k in ("sin_alt", "cos_alt", "tan_beta", "qa"):
+            steps[k][day_o] = sw_v[k]
     # TsWaveDelay weights (solweig.py:451-488): exp(-33.27 * timeadd) with
     # timeadd made a tensor as the 0-dim form makes it (float32 from a
     # Python float, float64 from a numpy float64 such as a dectime
@@ -1118,7 +1122,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
         steps["tw_b"][rows_] = w.numpy().astype(F32)
     _lcyl_tables(patch, lcyl_rows, ta4_v, ewall_t, sbc_t)
     _kside_tables(patch, kside_rows, diff_vals, params.albedo_b, azimuth, altitude)
-    sun = np.array(sun_rows, N.SUN_STEP_DTYPE) if sun_rows else np.zeros(0, N.SUN_STEP_DTYPE)
-    table = np.concatenate(tables) if tables else np.zeros(0, N.STEP_DTYPE)
+    sun = sun_rows if n_dr else np.zeros(0, N.SUN_STEP_DTYPE)
+    table = tables[0] if n_dr else np.zeros(0, N.STEP_DTYPE)
     final = {"CI": float(CI), "firstdaytime": float(firstdaytime), "timeadd": float(timeadd)}
     return Series(steps, sun, table, patch, T.gvf_table(int(second_f)), final, class_idx)

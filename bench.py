@@ -813,7 +813,7 @@ def main():
         pin = PINS.get(args.workload) if args.side is None else None
         if pin is not None and os.path.exists(pin):
             line["error_vs_fp64"] = error_vs_fp64(pin, outputs[1].cpu().numpy(), outputs[0].cpu().numpy())
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:   # rank 0 at N = 1 only
             line["cpu_baseline"] = cpu_baseline(city, met, geo, lc_class)
         print(json.dumps(line), flush=True)
         if args.timeline and e2e is not None:

@@ -374,24 +374,25 @@ typedef struct {
 typedef struct {
   float kside_d[4];         /* ((diffsh * lumChi) * anglIncC) * ster; index sh * 2 + vegsh */
   float anilum[4];          /* diffsh * lv */
-  float kref_veg;           /* (shaded_surface * ster) * cos(alt) */
-  float kref_sun;           /* (sunlit_surface * ster) * cos(alt) */
-  float kref_sh;            /* (shaded_surface * ster) * cos(alt) */
-  float yi_k;               /* yi_ of shaded_or_sunlit, Kside call (float32) */
-  float yi_l;               /* yi_ of shaded_or_sunlit, Lcyl call (float32) */
-  float thr_sun;            /* sunlit <=> hsvf + yi < thr_sun */
-  float thr_shd;            /* shaded <=> hsvf + yi > thr_shd */
-  float ld_sky;             /* Lsky_down[p] */
-  float ls_sky;             /* Lsky_side[p] */
+  /* the rest in 16-byte groups that the loop's set-bit walk reads together */
   float ster;
   float cos_alt;
   float sin_alt;
-  float sun_cos;            /* (sunlit wall surface * ster) * cos(alt) */
-  float sun_sin;
-  int32_t flags;            /* bit0: Lcyl sunlit/shaded branch taken */
-  int32_t pad;
+  float kref_veg;           /* (shaded_surface * ster) * cos(alt) */
   double veg_cos;           /* (vegetation_surface * ster) * cos(alt), float64 */
   double veg_sin;
+  float yi_k;               /* yi_ of shaded_or_sunlit, Kside call (float32) */
+  float thr_sun;            /* sunlit <=> hsvf + yi < thr_sun */
+  float thr_shd;            /* shaded <=> hsvf + yi > thr_shd */
+  int32_t flags;            /* bit0: Lcyl sunlit/shaded branch taken */
+  float kref_sun;           /* (sunlit_surface * ster) * cos(alt) */
+  float kref_sh;            /* (shaded_surface * ster) * cos(alt) */
+  float yi_l;               /* yi_ of shaded_or_sunlit, Lcyl call (float32) */
+  float ld_sky;             /* Lsky_down[p] */
+  float sun_cos;            /* (sunlit wall surface * ster) * cos(alt) */
+  float sun_sin;
+  float ls_sky;             /* Lsky_side[p] */
+  int32_t pad;
   double sh_cos;            /* (shaded_surface * ster) * cos(alt), float64 */
   double sh_sin;
 } sw100_patch_step;

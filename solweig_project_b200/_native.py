@@ -85,11 +85,13 @@ GVF_AZ_DTYPE = np.dtype([
 ], align=True)
 
 PATCH_STEP_DTYPE = np.dtype([
-    ("kside_d", "<f4", (4,)), ("anilum", "<f4", (4,)), ("kref_veg", "<f4"), ("kref_sun", "<f4"),
-    ("kref_sh", "<f4"), ("yi_k", "<f4"), ("yi_l", "<f4"), ("thr_sun", "<f4"), ("thr_shd", "<f4"),
-    ("ld_sky", "<f4"), ("ls_sky", "<f4"), ("ster", "<f4"), ("cos_alt", "<f4"), ("sin_alt", "<f4"),
-    ("sun_cos", "<f4"), ("sun_sin", "<f4"), ("flags", "<i4"), ("pad", "<i4"),
-    ("veg_cos", "<f8"), ("veg_sin", "<f8"), ("sh_cos", "<f8"), ("sh_sin", "<f8"),
+    ("kside_d", "<f4", (4,)), ("anilum", "<f4", (4,)),
+    ("ster", "<f4"), ("cos_alt", "<f4"), ("sin_alt", "<f4"), ("kref_veg", "<f4"),
+    ("veg_cos", "<f8"), ("veg_sin", "<f8"),
+    ("yi_k", "<f4"), ("thr_sun", "<f4"), ("thr_shd", "<f4"), ("flags", "<i4"),
+    ("kref_sun", "<f4"), ("kref_sh", "<f4"), ("yi_l", "<f4"), ("ld_sky", "<f4"),
+    ("sun_cos", "<f4"), ("sun_sin", "<f4"), ("ls_sky", "<f4"), ("pad", "<i4"),
+    ("sh_cos", "<f8"), ("sh_sin", "<f8"),
 ], align=True)
 
 TIME_STEP_DTYPE = np.dtype([

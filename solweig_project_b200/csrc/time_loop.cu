@@ -34,23 +34,34 @@ namespace sw100 {
 constexpr int kMaxPatchSmem = 153;
 constexpr int kTileThreads = 128;  // threads of a time-loop block (every launch shape)
 
-// The last 96 bytes of sw100_patch_step (kref_veg onwards): everything the
-// set-bit walk reads.  With the dense sums precomputed the loop stages only
-// these, 96-byte records instead of 128 (a smaller block, and lanes reading
-// different patches spread over more banks).
+// The last 96 bytes of sw100_patch_step (ster onwards): everything the
+// set-bit walk reads, in the record's 16-byte groups.  With the dense sums
+// precomputed the loop stages only these, 96-byte records instead of 128 (a
+// smaller block, and lanes reading different patches spread over more
+// banks).
 struct PatchTail {
-  float kref_veg, kref_sun, kref_sh, yi_k, yi_l, thr_sun, thr_shd, ld_sky, ls_sky, ster, cos_alt, sin_alt, sun_cos,
-      sun_sin;
-  int32_t flags, pad;
-  double veg_cos, veg_sin, sh_cos, sh_sin;
+  float ster, cos_alt, sin_alt, kref_veg;
+  double veg_cos, veg_sin;
+  float yi_k, thr_sun, thr_shd;
+  int32_t flags;
+  float kref_sun, kref_sh, yi_l, ld_sky;
+  float sun_cos, sun_sin, ls_sky;
+  int32_t pad;
+  double sh_cos, sh_sin;
 };
-constexpr int kPatchTailOffset = (int)offsetof(sw100_patch_step, kref_veg);
+constexpr int kPatchTailOffset = (int)offsetof(sw100_patch_step, ster);
 static_assert(kPatchTailOffset == 32 && sizeof(PatchTail) == 96 &&
                   sizeof(sw100_patch_step) == kPatchTailOffset + sizeof(PatchTail),
               "PatchTail is the tail of sw100_patch_step");
-static_assert(offsetof(PatchTail, veg_cos) + kPatchTailOffset == offsetof(sw100_patch_step, veg_cos) &&
-                  offsetof(PatchTail, flags) + kPatchTailOffset == offsetof(sw100_patch_step, flags),
+#define SW100_TAIL_AT(f) (offsetof(PatchTail, f) + kPatchTailOffset == offsetof(sw100_patch_step, f))
+static_assert(SW100_TAIL_AT(ster) && SW100_TAIL_AT(veg_cos) && SW100_TAIL_AT(yi_k) && SW100_TAIL_AT(flags) &&
+                  SW100_TAIL_AT(kref_sun) && SW100_TAIL_AT(sun_cos) && SW100_TAIL_AT(sh_cos),
               "PatchTail fields sit where sw100_patch_step has them");
+#undef SW100_TAIL_AT
+static_assert(offsetof(sw100_patch_step, ster) % 16 == 0 && offsetof(sw100_patch_step, veg_cos) % 16 == 0 &&
+                  offsetof(sw100_patch_step, yi_k) % 16 == 0 && offsetof(sw100_patch_step, kref_sun) % 16 == 0 &&
+                  offsetof(sw100_patch_step, sun_cos) % 16 == 0 && offsetof(sw100_patch_step, sh_cos) % 16 == 0,
+              "the walk's 16-byte groups are 16-byte aligned in the record");
 
 struct GvfAzSmem {
   int8_t dx[SW100_MAX_GVF_STEPS];
@@ -600,33 +611,44 @@ __device__ __forceinline__ void time_loop_tile(
         m &= m - 1u;
         const uint32_t bit = 1u << j;
         const PatchRec& Q = PP[q0 + j];
+        // the record's 16-byte groups (16-byte aligned in PP): one shared
+        // load each
+        const float4 R = *reinterpret_cast<const float4*>(&Q.ster);   // ster, cos_alt, sin_alt, kref_veg
         if (mveg & bit) {
-          acc64<SUMS>(ls_veg_a, Q.veg_cos);
-          acc64<SUMS>(ld_veg_a, Q.veg_sin);
-          if (day) kref_veg = kref_veg + Q.kref_veg;
+          const double2 V = *reinterpret_cast<const double2*>(&Q.veg_cos);
+          acc64<SUMS>(ls_veg_a, V.x);
+          acc64<SUMS>(ld_veg_a, V.y);
+          if (day) kref_veg = kref_veg + R.w;
         }
         if (mwall & bit) {
+          const float4 W = *reinterpret_cast<const float4*>(&Q.yi_k);       // yi_k, thr_sun, thr_shd, flags
+          const float4 K = *reinterpret_cast<const float4*>(&Q.kref_sun);   // kref_sun, kref_sh, yi_l, ld_sky
           if (day) {
-            const float td = hsvf + Q.yi_k;
-            if (td < Q.thr_sun) kref_sun = kref_sun + Q.kref_sun;
-            if (td > Q.thr_shd) kref_sh = kref_sh + Q.kref_sh;
+            const float td = hsvf + W.x;
+            if (td < W.y) kref_sun = kref_sun + K.x;
+            if (td > W.z) kref_sh = kref_sh + K.y;
           }
-          if (Q.flags & 1) {
-            const float td = hsvf + Q.yi_l;
-            if (td < Q.thr_sun) { ls_sun = ls_sun + Q.sun_cos; ld_sun = ld_sun + Q.sun_sin; }
-            if (td > Q.thr_shd) { acc64<SUMS>(ls_sh_a, Q.sh_cos); acc64<SUMS>(ld_sh_a, Q.sh_sin); }
+          const double2 H = *reinterpret_cast<const double2*>(&Q.sh_cos);
+          if (__float_as_int(W.w) & 1) {
+            const float td = hsvf + K.z;
+            if (td < W.y) {
+              const float2 U = *reinterpret_cast<const float2*>(&Q.sun_cos);
+              ls_sun = ls_sun + U.x;
+              ld_sun = ld_sun + U.y;
+            }
+            if (td > W.z) { acc64<SUMS>(ls_sh_a, H.x); acc64<SUMS>(ld_sh_a, H.y); }
           } else {
-            acc64<SUMS>(ls_sh_a, Q.sh_cos);
-            acc64<SUMS>(ld_sh_a, Q.sh_sin);
+            acc64<SUMS>(ls_sh_a, H.x);
+            acc64<SUMS>(ld_sh_a, H.y);
           }
         }
         if constexpr (SUMS) {   // refl * sum(ster * cos) once, below
-          ref_c = __fmaf_rn(Q.ster, Q.cos_alt, ref_c);
-          ref_s = __fmaf_rn(Q.ster, Q.sin_alt, ref_s);
+          ref_c = __fmaf_rn(R.x, R.y, ref_c);
+          ref_s = __fmaf_rn(R.x, R.z, ref_s);
         } else {
-          const float rs = refl * Q.ster;
-          ls_ref = ls_ref + rs * Q.cos_alt;
-          ld_ref = ld_ref + rs * Q.sin_alt;
+          const float rs = refl * R.x;
+          ls_ref = ls_ref + rs * R.y;
+          ld_ref = ld_ref + rs * R.z;
         }
       }
     }

@@ -438,9 +438,19 @@ def run_batched(args, world, rank, local):
     step_ms = float(t_max.item())
     total_px = sum(s["side"] ** 2 for s in specs)
     value = total_px * N_STEPS_DAY / (step_ms / 1e3)
-    # stage breakdown (one launch per stage, outside the graph)
+    batch.check_tensor_errors()
+    # stage breakdown (one launch per stage, outside the graph; the patch-sum
+    # products one per site)
     stage_ms = {}
     for st in B.STAGES:
+        if st == "flux" and batch.tensor_sums:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for m in batch.members:
+                m.site.launch_patch_sums(m.series_struct, m.sums)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            stage_ms["patch_sums_tc"] = e0.elapsed_time(e1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         batch.launch(st)

@@ -484,6 +484,9 @@ typedef struct {
   float* skipmap;               /* ((rows + 7) / 8) * ((cols + 7) / 8) source bounds of the SVF
                                    sweep, written by sw100_batch_skipmap after the pack; NULL:
                                    march every step */
+  const float* sums;            /* n_t * 4 * npix dense patch sums of the site's series, written by
+                                   sw100_patch_sums after the sweep; read by
+                                   sw100_batch_flux_loop_sums (NULL for sw100_batch_flux_loop) */
 } sw100_batch_site;
 
 /* Tile list entry {site index, tile column, tile row, daytime row}: the
@@ -517,6 +520,11 @@ int sw100_batch_sun_march(const sw100_batch_site* sites, const sw100_tile* tiles
                           int block_y, int grid, void* stream);
 int sw100_batch_flux_loop(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
                           int block_y, int grid, void* stream);
+/* sw100_batch_flux_loop with every site's dense patch sums read from its
+ * `sums` (sw100_flux_loop_sums per site: fluxes held to the Tmrt / UTCI
+ * tolerance); every listed site must have `sums` set. */
+int sw100_batch_flux_loop_sums(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                               int block_y, int grid, void* stream);
 
 /* Sun march for every daytime row of the series in one launch.  Writes the
  * per-row ground-view-factor source records (4 floats per pixel:

@@ -37,7 +37,8 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_coun
            "sw100_svf_window_workspace_bytes", "sw100_svf_window", "sw100_diff_bbox_workspace_bytes",
            "sw100_diff_bbox", "sw100_batch_validate", "sw100_batch_pack", "sw100_batch_bush_flags",
            "sw100_batch_skipmap", "sw100_batch_svf", "sw100_batch_sun_march", "sw100_batch_flux_loop",
-           "sw100_utci_steps", "sw100_nn_conv3x3_wgrad", "sw100_nn_weights", "sw100_nn_relu_bwd", "sw100_nn_pool2",
+           "sw100_batch_flux_loop_sums", "sw100_utci_steps", "sw100_nn_conv3x3_wgrad", "sw100_nn_weights",
+           "sw100_nn_relu_bwd", "sw100_nn_pool2",
            "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc",
            "sw100_prepare_site", "sw100_march_tables", "sw100_set_wait_limit",
            "sw100_patch_sums_workspace_bytes", "sw100_patch_sums", "sw100_flux_loop_sums")
@@ -217,7 +218,7 @@ def load(path: str = LIB_PATH):
         "sw100_nn_input": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp]),
         **{name: (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]) for name in (
             "sw100_batch_pack", "sw100_batch_bush_flags", "sw100_batch_svf", "sw100_batch_sun_march",
-            "sw100_batch_flux_loop")},
+            "sw100_batch_flux_loop", "sw100_batch_flux_loop_sums")},
         "sw100_batch_skipmap": (C.c_int, [vp, C.c_int, vp]),
         "sw100_set_wait_limit": (C.c_int, [C.c_int]),
         "sw100_prepare_site": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(ClassTable), C.c_int, C.c_int] + [vp] * 12),

@@ -49,6 +49,7 @@ class BatchSite(C.Structure):
         ("steps", C.c_void_p), ("series", N.Series), ("svf_planes", C.c_void_p), ("svf_bits", C.c_void_p),
         ("src4", C.c_void_p), ("bflags", C.c_void_p), ("gsrc", C.c_void_p), ("state", C.c_void_p),
         ("outputs", C.c_void_p), ("out_mask", C.c_uint32), ("svf_steps", C.c_int32), ("skipmap", C.c_void_p),
+        ("sums", C.c_void_p),
     ]
 
 
@@ -116,6 +117,7 @@ class _Member:
     outputs: torch.Tensor
     n_steps: int
     skipmap: torch.Tensor
+    sums: "torch.Tensor | None" = None
 
 
 class SiteBatch:
@@ -156,6 +158,12 @@ class SiteBatch:
                 skipmap=torch.empty(-(-rows // 8) * -(-cols // 8), dtype=torch.float32, device=d)))
             site._plan_steps = (plan_d, steps_d)
         self.mask = mask
+        # the dense patch sums of each site on the tensor cores, then the
+        # flux loop that reads them (as the single-site chain runs)
+        self.tensor_sums = E.TENSOR_SUMS
+        for m in self.members:
+            m.sums = (torch.empty((m.series_struct.n_t, 4, m.site.rows, m.site.cols), dtype=torch.float32,
+                                  device=self.device) if self.tensor_sums else None)
         host = (BatchSite * len(self.members))()
         for i, m in enumerate(self.members):
             b = host[i]
@@ -168,6 +176,7 @@ class SiteBatch:
             b.state, b.outputs, b.out_mask = m.site.state.data_ptr(), m.outputs.data_ptr(), mask
             b.svf_steps = m.n_steps
             b.skipmap = m.skipmap.data_ptr()
+            b.sums = m.sums.data_ptr() if m.sums is not None else 0
         N.call("sw100_batch_validate", C.cast(host, C.c_void_p), len(self.members))
         raw = np.frombuffer(bytes(host), np.uint8).copy()
         self.sites_dev = torch.from_numpy(raw).to(self.device)
@@ -211,7 +220,8 @@ class SiteBatch:
         if n == 0:
             return
         grid = n if m == "tiles" else min(n, SM_COUNT * 8)
-        N.call(ENTRY[stage], C.c_void_p(self.sites_dev.data_ptr()), C.c_void_p(dev.data_ptr()), n, bx, by, grid,
+        entry = "sw100_batch_flux_loop_sums" if stage == "flux" and self.tensor_sums else ENTRY[stage]
+        N.call(entry, C.c_void_p(self.sites_dev.data_ptr()), C.c_void_p(dev.data_ptr()), n, bx, by, grid,
                E._stream())
 
     def run(self, reset_state=True):
@@ -223,6 +233,9 @@ class SiteBatch:
             if reset_state:
                 m.site.state.zero_()
         for st in STAGES:
+            if st == "flux" and self.tensor_sums:
+                for m in self.members:   # after the sweep: the sums read its bit cubes
+                    m.site.launch_patch_sums(m.series_struct, m.sums)
             self.launch(st)
             if st == "pack":
                 N.call("sw100_batch_skipmap", C.c_void_p(self.sites_dev.data_ptr()), len(self.members),
@@ -245,6 +258,13 @@ class SiteBatch:
         if self.graph is None:
             self.capture()
         self.graph.replay()
+
+    def check_tensor_errors(self):
+        """Raise if a bounded wait of a site's patch-sum product ran out
+        (reads each site's error flag: synchronises)."""
+        if self.tensor_sums:
+            for m in self.members:
+                m.site.check_tensor_error()
 
     def outputs(self, i):
         """{name: (n_t, rows, cols) device tensor} of site i."""

@@ -43,6 +43,7 @@ __global__ void svf_sweep_batch_kernel(const sw100_batch_site* sites, const sw10
 __global__ void sun_march_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void skipmap_batch_kernel(const sw100_batch_site* sites);
 __global__ void time_loop_batch_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
+__global__ void time_loop_batch_sums_kernel(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles);
 __global__ void svf_bush_flags_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan,
                                       const sw100_step* steps, uint32_t* flags, int n_steps);
 __global__ void sun_march_kernel(const float4* src4, SitePlanes site, int rows, int cols,
@@ -507,6 +508,12 @@ int sw100_batch_flux_loop(const sw100_batch_site* sites, const sw100_tile* tiles
                           int block_y, int grid, void* stream) {
   return launch_batch(time_loop_batch_kernel, "time_loop_batch_kernel", sites, tiles, n_tiles, block_x, block_y,
                       grid, stream);
+}
+
+int sw100_batch_flux_loop_sums(const sw100_batch_site* sites, const sw100_tile* tiles, int n_tiles, int block_x,
+                               int block_y, int grid, void* stream) {
+  return launch_batch(time_loop_batch_sums_kernel, "time_loop_batch_sums_kernel", sites, tiles, n_tiles, block_x,
+                      block_y, grid, stream);
 }
 
 int sw100_prepare_site(const float* dsm, const float* trees, const float* dem, const float* aspect_deg,

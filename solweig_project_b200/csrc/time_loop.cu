@@ -733,4 +733,18 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_batch_kernel(const 
   }
 }
 
+// The same with each site's dense patch sums precomputed (S.sums).
+__global__ void __launch_bounds__(kTileThreads, 6) time_loop_batch_sums_kernel(
+    const sw100_batch_site* __restrict__ sites, const sw100_tile* __restrict__ tiles, int n_tiles) {
+  for (int i = blockIdx.x; i < n_tiles; i += gridDim.x) {
+    const sw100_tile T = tiles[i];
+    const sw100_batch_site& S = sites[T.site];
+    __syncthreads();  // the previous tile is done with the shared tables
+    time_loop_tile<sw100_site_planes, false, true>(S.site, S.rows, S.cols, S.series.steps, S.series.n_t,
+                                                   S.series.patch, S.series.n_patches, S.series.gvf,
+                                                   reinterpret_cast<const float4*>(S.gsrc), S.series.n_day, S.state,
+                                                   S.out_mask, S.outputs, T.tx, T.ty, S.sums);
+  }
+}
+
 }  // namespace sw100

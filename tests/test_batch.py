@@ -113,9 +113,9 @@ def test_batch_equals_single_site_runs(cuda, tmp_path):
     for mk, ser in specs:
         s = mk()
         res = s.run_svf()
-        # the batch kernels compute the dense patch sums in the loop kernel:
-        # compare with the single-site run that does the same
-        out = s.run_time_loop(ser(s), requested=REQ, tensor_sums=False)
+        # the batch takes the dense patch sums from the tensor cores, as the
+        # single-site run does (the in-loop form: tests/test_tiles.py)
+        out = s.run_time_loop(ser(s), requested=REQ, tensor_sums=True)
         singles.append((res.planes.cpu().numpy(), res.bits.cpu().numpy(),
                         {k: v.cpu().numpy() for k, v in out.items()}))
     sites = [mk() for mk, _ in specs]

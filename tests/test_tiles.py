@@ -45,8 +45,9 @@ def test_multiband_tiff_carries_time_metadata():
 def test_tiled_batch_equals_single_tile_runs(cuda, tmp_path, monkeypatch):
     from solweig_project_b200 import api, synthetic
     from solweig_project_b200 import engine as E
-    # the batch kernels compute the dense patch sums in the loop kernel:
-    # the single-tile runs do the same
+    # the in-loop patch sums (the reference's float32 order) in the batch
+    # kernels and in the single-tile runs alike; the tensor-core form is
+    # checked batch against single site in tests/test_batch.py
     monkeypatch.setattr(E, "TENSOR_SUMS", False)
     city = synthetic.make_city(150, 130, seed=9, n_buildings=20, n_trees=16, side_range=(5, 14))
     met = synthetic.make_met(9)

@@ -740,7 +740,7 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_batch_sums_kernel(
     const sw100_tile T = tiles[i];
     const sw100_batch_site& S = sites[T.site];
     __syncthreads();  // the previous tile is done with the shared tables
-    time_loop_tile<sw100_site_planes, false, true>(S.site, S.rows, S.cols, S.series.steps, S.series.n_t,
+    time_loop_tile<sw100_site_planes, true, true>(S.site, S.rows, S.cols, S.series.steps, S.series.n_t,
                                                    S.series.patch, S.series.n_patches, S.series.gvf,
                                                    reinterpret_cast<const float4*>(S.gsrc), S.series.n_day, S.state,
                                                    S.out_mask, S.outputs, T.tx, T.ty, S.sums);

@@ -313,8 +313,8 @@ struct GvfSums {
 // (a kernel parameter) or sw100_site_planes (a batch descriptor in global
 // memory): the same member names.
 // KNOWN_N0: reuse each walk's first-building step after the first daytime
-// step (faster for one site; the batch kernel, with more live registers,
-// does not gain).
+// step (faster for one site and for the batch with tensor-core sums; the
+// in-loop-sums batch kernel, with more live registers, does not gain).
 // SUMS: the four dense patch sums of each step come precomputed (the
 // tensor-core product of patch_sums.cu, sums[(t * 4 + j) * npix + p], j =
 // diffuse Kside, anisotropic luminance, sky longwave down, side) instead of

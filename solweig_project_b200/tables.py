@@ -295,7 +295,6 @@ def gvf_table(second: int) -> np.ndarray:
 def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03, all_finite=False):
     """SVF plan record + concatenated step table + single-step patch mask."""
     annulino, altint, _, nband = PATCH_LAYOUT[patch_option]
-    azs = sweep_azimuths(patch_option)
     w_iso, w_an, count = ring_weights(patch_option)
     plan = np.zeros(1, N.SVF_PLAN_DTYPE)
     P = int(sum(nband))
@@ -309,36 +308,52 @@ def svf_plan(rows, cols, scale, amax, bush_any, patch_option=2, trans_veg=0.03, 
     plan["tail"] = F32(3.0459e-004)
     plan["trans"] = F32(0.03)
     plan["trans_veg"] = F32(trans_veg)
-    ring = np.repeat(np.arange(len(altint)), nband)[:P]
-    steps, counts = _svf_steps_all(azs[:P], np.asarray(altint)[ring], scale, amax, rows, cols)
+    ring, consts, tan_alt, dir_flags = _svf_layout(patch_option)
+    steps, counts = _svf_steps_all(consts, tan_alt, scale, amax, rows, cols)
     single = np.zeros(N.CUBE_WORDS, np.uint32)
     offsets = np.concatenate([[0], np.cumsum(counts)[:-1]]) if P else np.zeros(0, np.int64)
     plan["step_offset"][0, :P] = offsets
     plan["step_count"][0, :P] = counts
     plan["ring"][0, :P] = ring
-    for q in range(P):
-        a = float(azs[q])
-        plan["dir_flags"][0, q] = ((1 if 0 <= a < 180 else 0) | (2 if 90 <= a < 270 else 0) |
-                                   (4 if 180 <= a < 360 else 0) | (8 if (a >= 270 or a < 90) else 0))
-        if counts[q] <= 1:
-            single[q >> 5] |= np.uint32(1 << (q & 31))
+    plan["dir_flags"][0, :P] = dir_flags
+    for q in np.flatnonzero(np.asarray(counts) <= 1):
+        single[q >> 5] |= np.uint32(1 << (int(q) & 31))
     return plan, steps, single
 
 
-def _svf_steps_all(azs, alts, scale, amax, rows, cols):
-    """Executed steps of every patch march at once, concatenated in patch
-    order with their SW100_STEP_SKIP8 flags (sw100_march_tables: the same
-    float32 values as svf_patch_table applied patch by patch); returns
-    (steps, counts)."""
-    trig = [_svf_patch_trig(float(a), int(h)) for a, h in zip(azs, alts)]
+@functools.lru_cache(maxsize=None)
+def _svf_layout(patch_option):
+    """The site-independent part of the SVF plan of a patch layout: each
+    patch's ring, march constants (float32 trigonometry and step-direction
+    branch, shadow.py:196-226) without the scale-dependent tan(altitude),
+    tan(altitude) itself, and its direction-sum flags (E, S, W, N)."""
+    _, altint, _, nband = PATCH_LAYOUT[patch_option]
+    P = int(sum(nband))
+    azs = sweep_azimuths(patch_option)[:P]
+    ring = np.repeat(np.arange(len(altint)), nband)[:P]
+    trig = [_svf_patch_trig(float(a), int(h)) for a, h in zip(azs, np.asarray(altint)[ring])]
     consts = np.zeros(len(trig), N.MARCH_CONST_DTYPE)
     consts["branch_y"] = [t[0] for t in trig]
     consts["ssin"] = [t[1] for t in trig]
     consts["scos"] = [t[2] for t in trig]
     consts["tan_a"] = [t[3] for t in trig]
     consts["ds"] = [t[4] for t in trig]
-    consts["tanalt"] = [F32(t[5] / F32(scale)) for t in trig]
-    return N.march_tables(consts, 1, amax, rows, cols)
+    tan_alt = np.array([t[5] for t in trig], np.float32)
+    dir_flags = np.array([((1 if 0 <= a < 180 else 0) | (2 if 90 <= a < 270 else 0) | (4 if 180 <= a < 360 else 0) |
+                           (8 if (a >= 270 or a < 90) else 0)) for a in map(float, azs)], np.int32)
+    for a in (ring, consts, tan_alt, dir_flags):
+        a.setflags(write=False)
+    return ring, consts, tan_alt, dir_flags
+
+
+def _svf_steps_all(consts, tan_alt, scale, amax, rows, cols):
+    """Executed steps of every patch march at once, concatenated in patch
+    order with their SW100_STEP_SKIP8 flags (sw100_march_tables: the same
+    float32 values as svf_patch_table applied patch by patch); returns
+    (steps, counts)."""
+    c = consts.copy()
+    c["tanalt"] = tan_alt / F32(scale)      # float32 / float32, per element as F32(t / F32(scale))
+    return N.march_tables(c, 1, amax, rows, cols)
 
 
 # ------------------------------------------- windowed SVF recompute

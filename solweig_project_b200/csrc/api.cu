@@ -831,10 +831,14 @@ int sw100_nn_conv3x3_tc(const void* x, int n, int h, int w, int cin, int xstride
   if (cout > 128) return fail(SW100_E_ARG, "the tensor-core convolution takes at most 128 output channels");
   const int64_t total = (int64_t)n * h * w;
   const int64_t blocks = (total + 127) / 128;
-  const int smem = 3 * 2 * 4 * 4096;   // three stages of A and B tiles (4 K steps of 4 KB each)
-  static bool attr_set = false;    // the attribute is per function and process: set it once
+  // three stages of A tiles (4 K steps x 128 pixels x 32 B) and of B tiles
+  // (4 K steps x cout x 32 B): the fewer the output channels, the more CTAs
+  // share an SM
+  const int smem = 3 * 4 * 4096 + 3 * 4 * 32 * cout;
+  static bool attr_set = false;    // the attribute is per function and process: set it once, to the largest size
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(nn_conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(nn_conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         3 * 4 * 4096 + 3 * 4 * 32 * 128);
     if (e != cudaSuccess) return fail((int)e, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
     attr_set = true;
   }

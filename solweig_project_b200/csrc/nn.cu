@@ -75,14 +75,18 @@ __global__ void __launch_bounds__(128) nn_conv3x3_tc_kernel(const __nv_bfloat16*
                                                             const float* __restrict__ bias, int Cout, void* Yv,
                                                             int ystride, int ycoff, int relu, int out_f32,
                                                             int* __restrict__ err, int wait_limit) {
-  // dynamic shared memory: kTcStages A stage buffers, then kTcStages B
-  // stage buffers, 1024-byte aligned; 96 KB per CTA also caps the CTAs per
-  // SM at 2, so TMEM (<= 128 columns each) is never oversubscribed
+  // dynamic shared memory: kTcStages A stage buffers (128 pixels x 64 K),
+  // then kTcStages B stage buffers sized by the output channels (Cout x 64
+  // K), 1024-byte aligned: 60 KB for Cout <= 32, 72 KB for 64, 96 KB for
+  // 128, so 3, 3 and 2 CTAs per SM, whose TMEM allocations (32, 64 and 128
+  // columns each) never exceed the SM's 512 columns
   extern __shared__ __align__(1024) uint8_t tc_smem[];
   __shared__ __align__(8) uint64_t mbar[kTcStages];
   __shared__ uint32_t tmem_base;
   const uint32_t a_base = tc::smem_u32(tc_smem);
   const uint32_t b_base = a_base + kTcStages * kTcStageBytes;
+  const uint32_t b_step = 32u * (uint32_t)Cout;                   // one K step of B: Cout / 8 core matrices
+  const uint32_t b_stage = kTcStepsPerStage * b_step;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int64_t total = (int64_t)N * H * W;
   const int64_t p0 = (int64_t)blockIdx.x * 128;
@@ -132,7 +136,7 @@ __global__ void __launch_bounds__(128) nn_conv3x3_tc_kernel(const __nv_bfloat16*
       cp_async16(a + tc::core_off(tid, 1), src + 8, in ? 16 : 0);
       if (tid < Cout) {
         const __nv_bfloat16* wsrc = Wt + ((size_t)t * Cout + tid) * Cin + ci0;
-        const uint32_t b = b_base + buf * kTcStageBytes + j * 4096;
+        const uint32_t b = b_base + buf * b_stage + j * b_step;
         cp_async16(b + tc::core_off(tid, 0), wsrc, 16);
         cp_async16(b + tc::core_off(tid, 1), wsrc + 8, 16);
       }
@@ -161,7 +165,7 @@ __global__ void __launch_bounds__(128) nn_conv3x3_tc_kernel(const __nv_bfloat16*
       const int ns = min(kTcStepsPerStage, nsteps - s0);
       for (int j = 0; j < ns; ++j) {
         const uint64_t ad = tc::smem_desc(a_base + buf * kTcStageBytes + j * 4096, 128, 256);
-        const uint64_t bd = tc::smem_desc(b_base + buf * kTcStageBytes + j * 4096, 128, 256);
+        const uint64_t bd = tc::smem_desc(b_base + buf * b_stage + j * b_step, 128, 256);
         tc::mma_f16(tmem, ad, bd, idesc, (s0 + j) > 0 ? 1u : 0u);
       }
       tc::commit(tc::smem_u32(&mbar[buf]));

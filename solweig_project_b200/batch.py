@@ -12,7 +12,7 @@ records the stage launches in a CUDA graph that :meth:`SiteBatch.replay`
 re-issues with one call.
 
 Launch shapes come from :class:`Autotuner`: per stage, it times the block
-shapes of 128 threads (32 x 4, 16 x 8, 64 x 2, 128 x 1) with one tile per
+shapes of 128 threads (8 x 16, 32 x 4, 16 x 8, 4 x 32, 64 x 2, 128 x 1) with one tile per
 block or a persistent grid striding over the tile list, and stores the
 fastest per grid-size bucket (the batch's pixel-weighted median side) in a
 JSON file.
@@ -34,10 +34,11 @@ from . import timeseries as TS
 STAGES = ("pack", "bush", "svf", "sun", "flux")
 SHAPES = ((8, 16), (32, 4), (16, 8), (4, 32), (64, 2), (128, 1))
 SM_COUNT = 148
-# the march stages default to 8 x 16 tiles: a warp covers 8 x 4 pixels, whose
-# rays meet similar obstacles (less divergence than 32 x 1 rows)
+# the march and loop stages default to 8 x 16 tiles: a warp covers 8 x 4
+# pixels, whose rays and ground-view walks meet similar obstacles (less
+# divergence than 32 x 1 rows)
 DEFAULT_SHAPE = {"pack": ((32, 4), "tiles"), "bush": ((32, 4), "tiles"), "svf": ((8, 16), "tiles"),
-                 "sun": ((8, 16), "tiles"), "flux": ((32, 4), "tiles")}
+                 "sun": ((8, 16), "tiles"), "flux": ((8, 16), "tiles")}
 ENTRY = {"pack": "sw100_batch_pack", "bush": "sw100_batch_bush_flags", "svf": "sw100_batch_svf",
          "sun": "sw100_batch_sun_march", "flux": "sw100_batch_flux_loop"}
 

@@ -132,6 +132,11 @@ int64_t align_up(int64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 // Block shape of the march kernels (SVF sweep, windowed recompute): 128
 // threads, a warp covering 8 x 4 pixels.
 constexpr int kMarchBx = 8, kMarchBy = 16;
+// Block shape of the time / flux loops: 128 threads, a warp covering 8 x 4
+// pixels.  A warp's ground-view walks last as long as its longest one, and
+// the first-building step varies less over an 8 x 4 patch than along a row
+// of 32 (a quarter fewer walk steps per warp at 500 x 500, 8 % faster loop).
+constexpr int kLoopBx = 8, kLoopBy = 16;
 
 int check_grid(int rows, int cols) {
   if (rows <= 0 || cols <= 0) return fail(SW100_E_SIZE, "grid %d x %d must be positive", rows, cols);
@@ -615,8 +620,8 @@ int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw1
   float4* gsrc = reinterpret_cast<float4*>(static_cast<char*>(workspace) + plane4);
   if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
   if ((rc = launch_sun_march(*site, rows, cols, *series, src4, gsrc, nullptr, st))) return rc;
-  dim3 block(32, 4);
-  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  dim3 block(kLoopBx, kLoopBy);
+  dim3 grid((cols + kLoopBx - 1) / kLoopBx, (rows + kLoopBy - 1) / kLoopBy);
   time_loop_kernel<<<grid, block, 0, st>>>(make_site(*site), rows, cols, series->steps, series->n_t, series->patch,
                                            series->n_patches, series->gvf, gsrc, series->n_day, state, out_mask,
                                            outputs);
@@ -633,8 +638,8 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
   if (series->n_day > 0 && (rc = check_ptr(gsrc, "gsrc"))) return rc;
   if (out_mask & ~0x7Fu) return fail(SW100_E_ARG, "unknown output bits 0x%x", out_mask);
   if (out_mask && !outputs) return fail(SW100_E_ARG, "outputs must not be NULL");
-  dim3 block(32, 4);
-  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  dim3 block(kLoopBx, kLoopBy);
+  dim3 grid((cols + kLoopBx - 1) / kLoopBx, (rows + kLoopBy - 1) / kLoopBy);
   time_loop_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
       reinterpret_cast<const float4*>(gsrc), series->n_day, state, out_mask, outputs);
@@ -708,8 +713,8 @@ int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, cons
                                     (int)cudaSharedmemCarveoutMaxShared);
   });
   if (attr_err != cudaSuccess) return fail((int)attr_err, "cudaFuncSetAttribute: %s", cudaGetErrorString(attr_err));
-  dim3 block(32, 4);
-  dim3 grid((cols + 31) / 32, (rows + 3) / 4);
+  dim3 block(kLoopBx, kLoopBy);
+  dim3 grid((cols + kLoopBx - 1) / kLoopBx, (rows + kLoopBy - 1) / kLoopBy);
   time_loop_sums_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
       reinterpret_cast<const float4*>(gsrc), series->n_day, state, out_mask, outputs, sums);

@@ -83,9 +83,10 @@ CHUNKS_IN_FLIGHT = 3
 
 # default chunk lengths of the chunked time loop (then 8 while steps remain):
 # a long first chunk whose tables are built while the SVF sweep runs, a short
-# last one whose GPU work is the call's tail (500 x 500 x 24 on B200: 10.4 ms
-# per call against 10.9 ms with chunks of 8)
-DEFAULT_CHUNKS = (14, 6, 4, 8)
+# last one whose GPU work and copy-back are the call's tail (500 x 500 x 24 on
+# B200, median of 24 interleaved calls: 8.74 ms per call against 8.90 with
+# 16 + 8 and 9.21 with 14 + 6 + 4)
+DEFAULT_CHUNKS = (16, 6, 2, 8)
 
 # host <-> device bytes moved by this module (inputs, tables, results)
 TRANSFER = {"h2d": 0, "d2h": 0}

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define SW100_ABI_VERSION 2
+#define SW100_ABI_VERSION 3
 
 #define SW100_MAX_PATCHES 160   /* patch option 2 uses 153 */
 #define SW100_MAX_RINGS 16
@@ -140,6 +140,17 @@ typedef struct {
   /* patches whose SVF march ran at most one step: there vbshvegsh is 1 or 2
    * and its cube bit means "vbshvegsh == 1"; elsewhere it means "!= 0" */
   uint32_t single_step[SW100_CUBE_WORDS];
+  /* Optional order of the time / flux loops' work (NULL: 8 x 16 blocks in
+   * grid order).  The loops then run 128-thread blocks of four 8 x 4 pixel
+   * patches, one per warp, taken from this list in order; patch k covers
+   * rows 4 (k / pc) .. + 3 and columns 8 (k % pc) .. + 7, pc = ceil(cols / 8).
+   * n_patch_order must be ceil(rows / 4) * pc and the list a permutation of
+   * 0 .. n_patch_order - 1 (entries outside that range compute nothing; a
+   * repeated or missing patch computes a pixel twice or not at all).  The
+   * per-patch ground-view walk work of sw100_walk_work sorted descending
+   * gives blocks whose warps walk alike.  Results do not depend on it. */
+  const int32_t* patch_order;
+  int32_t n_patch_order;
 } sw100_site_planes;
 
 /* ------------------------------------------------- site preparation -- */
@@ -572,6 +583,16 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
 int sw100_patch_sums_workspace_bytes(int n_t, int64_t* bytes);
 int sw100_patch_sums(const sw100_site_planes* site, int rows, int cols, const sw100_series* series, float* sums,
                      int32_t* err, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* Ground-view walk work of each 8 x 4 pixel patch of the time / flux loops
+ * (patch numbering of sw100_site_planes.patch_order): for each of the 18
+ * azimuths of `gvf` (sw100_gvf_azimuth rows of the loops' series) the
+ * longest walk of the patch's pixels up to the first building sample
+ * (site->buildings == 0, in the grid) or `second` steps, summed over the
+ * azimuths.  `work` holds ceil(rows / 4) * ceil(cols / 8) int32.  No
+ * reference counterpart: a scheduling input. */
+int sw100_walk_work(const sw100_site_planes* site, int rows, int cols, const sw100_gvf_azimuth* gvf, int second,
+                    int32_t* work, void* stream);
 
 /* sw100_flux_loop with the dense patch sums taken from `sums` (as written
  * by sw100_patch_sums for the same series) instead of computed in the

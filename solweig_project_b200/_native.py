@@ -41,8 +41,8 @@ SYMBOLS = ("sw100_svf_workspace_bytes", "sw100_svf_sweep", "sw100_svf_sweep_coun
            "sw100_nn_relu_bwd", "sw100_nn_pool2",
            "sw100_nn_up2", "sw100_nn_mse", "sw100_nn_adam", "sw100_nn_input", "sw100_svf_box", "sw100_nn_conv3x3_tc",
            "sw100_prepare_site", "sw100_march_tables", "sw100_set_wait_limit",
-           "sw100_patch_sums_workspace_bytes", "sw100_patch_sums", "sw100_flux_loop_sums")
-ABI_VERSION = 2  # SW100_ABI_VERSION of include/solweig_b200.h
+           "sw100_patch_sums_workspace_bytes", "sw100_patch_sums", "sw100_flux_loop_sums", "sw100_walk_work")
+ABI_VERSION = 3  # SW100_ABI_VERSION of include/solweig_b200.h
 CORRIDOR_LOCAL = 2
 CORRIDOR_ALWAYS = 3
 
@@ -123,6 +123,7 @@ class SitePlanes(C.Structure):
         ("walls", C.c_void_p), ("aspect_rad", C.c_void_p), ("tgk", C.c_void_p), ("tstart", C.c_void_p),
         ("alb", C.c_void_p), ("emis", C.c_void_p), ("class_idx", C.c_void_p), ("windcoeff", C.c_void_p),
         ("bits", C.c_void_p), ("single_step", C.c_uint32 * CUBE_WORDS),
+        ("patch_order", C.c_void_p), ("n_patch_order", C.c_int32),
     ]
 
 
@@ -195,6 +196,7 @@ def load(path: str = LIB_PATH):
         "sw100_patch_sums_workspace_bytes": (C.c_int, [C.c_int, i64p]),
         "sw100_patch_sums": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, vp,
                                        C.c_int64, vp]),
+        "sw100_walk_work": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, vp, C.c_int, vp, vp]),
         "sw100_flux_loop_sums": (C.c_int, [C.POINTER(SitePlanes), C.c_int, C.c_int, C.POINTER(Series), vp, vp, vp,
                                            C.c_uint32, vp, vp]),
         "sw100_utci": (C.c_int, [vp, vp, vp, vp, C.c_int64, vp, vp]),

@@ -57,6 +57,8 @@ __global__ void time_loop_sums_kernel(SitePlanes site, int rows, int cols, const
                                       const sw100_patch_step* patch_steps, int n_patches,
                                       const sw100_gvf_azimuth* gvf_az, const float4* gsrc, int n_day, float* state,
                                       uint32_t out_mask, float* outputs, const float* sums);
+__global__ void walk_work_kernel(const float* buildings, int rows, int cols, const sw100_gvf_azimuth* gvf, int second,
+                                 int32_t* work, int n_patch);
 __global__ void patch_weights_kernel(const sw100_time_step* steps, int n_t, const sw100_patch_step* patch,
                                      int n_patches, __nv_bfloat16* W, int n_groups);
 __global__ void patch_sums_tc_kernel(const uint32_t* bits, int64_t npix, int n_patches, const __nv_bfloat16* W,
@@ -137,6 +139,7 @@ constexpr int kMarchBx = 8, kMarchBy = 16;
 // the first-building step varies less over an 8 x 4 patch than along a row
 // of 32 (a quarter fewer walk steps per warp at 500 x 500, 8 % faster loop).
 constexpr int kLoopBx = 8, kLoopBy = 16;
+constexpr int kTimeLoopThreads = 128;  // threads of a time-loop block (kTileThreads of time_loop.cu)
 
 int check_grid(int rows, int cols) {
   if (rows <= 0 || cols <= 0) return fail(SW100_E_SIZE, "grid %d x %d must be positive", rows, cols);
@@ -223,6 +226,23 @@ int launch_sun_march(const sw100_site_planes& site, int rows, int cols, const sw
   sun_march_kernel<<<grid, block, 0, st>>>(src4, make_site(site), rows, cols, ser.sun, ser.steps, ser.sun_table,
                                            site.vmax, gsrc, debug8);
   return check_launch("sun_march_kernel");
+}
+
+// Launch shape of the time / flux loops: four 8 x 4 pixel patches per block
+// in the site's patch order, or 8 x 16 blocks in grid order without one.
+int loop_shape(const sw100_site_planes& site, int rows, int cols, dim3& grid, dim3& block) {
+  if (site.patch_order == nullptr) {
+    block = dim3(kLoopBx, kLoopBy);
+    grid = dim3((cols + kLoopBx - 1) / kLoopBx, (rows + kLoopBy - 1) / kLoopBy);
+    return 0;
+  }
+  const int64_t n = (int64_t)((rows + 3) / 4) * ((cols + 7) / 8);
+  if (site.n_patch_order != n)
+    return fail(SW100_E_ARG, "n_patch_order %d must be %lld (8 x 4 patches of a %d x %d grid)", site.n_patch_order,
+                (long long)n, rows, cols);
+  block = dim3(kTimeLoopThreads);
+  grid = dim3((unsigned)((n + 3) / 4));
+  return 0;
 }
 
 }  // namespace
@@ -620,8 +640,8 @@ int sw100_time_loop(const sw100_site_planes* site, int rows, int cols, const sw1
   float4* gsrc = reinterpret_cast<float4*>(static_cast<char*>(workspace) + plane4);
   if ((rc = launch_pack(*site, rows, cols, src4, st))) return rc;
   if ((rc = launch_sun_march(*site, rows, cols, *series, src4, gsrc, nullptr, st))) return rc;
-  dim3 block(kLoopBx, kLoopBy);
-  dim3 grid((cols + kLoopBx - 1) / kLoopBx, (rows + kLoopBy - 1) / kLoopBy);
+  dim3 block, grid;
+  if ((rc = loop_shape(*site, rows, cols, grid, block))) return rc;
   time_loop_kernel<<<grid, block, 0, st>>>(make_site(*site), rows, cols, series->steps, series->n_t, series->patch,
                                            series->n_patches, series->gvf, gsrc, series->n_day, state, out_mask,
                                            outputs);
@@ -638,8 +658,8 @@ int sw100_flux_loop(const sw100_site_planes* site, int rows, int cols, const sw1
   if (series->n_day > 0 && (rc = check_ptr(gsrc, "gsrc"))) return rc;
   if (out_mask & ~0x7Fu) return fail(SW100_E_ARG, "unknown output bits 0x%x", out_mask);
   if (out_mask && !outputs) return fail(SW100_E_ARG, "outputs must not be NULL");
-  dim3 block(kLoopBx, kLoopBy);
-  dim3 grid((cols + kLoopBx - 1) / kLoopBx, (rows + kLoopBy - 1) / kLoopBy);
+  dim3 block, grid;
+  if ((rc = loop_shape(*site, rows, cols, grid, block))) return rc;
   time_loop_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
       reinterpret_cast<const float4*>(gsrc), series->n_day, state, out_mask, outputs);
@@ -693,6 +713,22 @@ int sw100_patch_sums(const sw100_site_planes* site, int rows, int cols, const sw
   return check_launch("patch_sums_tc_kernel");
 }
 
+int sw100_walk_work(const sw100_site_planes* site, int rows, int cols, const sw100_gvf_azimuth* gvf, int second,
+                    int32_t* work, void* stream) {
+  int rc;
+  if ((rc = check_grid(rows, cols))) return rc;
+  if ((rc = check_ptr(site, "site")) || (rc = check_ptr(site->buildings, "buildings")) ||
+      (rc = check_ptr(gvf, "gvf")) || (rc = check_ptr(work, "work")))
+    return rc;
+  if (second < 0 || second > SW100_MAX_GVF_STEPS)
+    return fail(SW100_E_ARG, "second %d outside 0 .. %d", second, SW100_MAX_GVF_STEPS);
+  const int64_t n = (int64_t)((rows + 3) / 4) * ((cols + 7) / 8);
+  const int64_t threads = n * 32;
+  walk_work_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      site->buildings, rows, cols, gvf, second, work, (int)n);
+  return check_launch("walk_work_kernel");
+}
+
 int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, const sw100_series* series,
                          const float* gsrc, const float* sums, float* state, uint32_t out_mask, float* outputs,
                          void* stream) {
@@ -713,8 +749,8 @@ int sw100_flux_loop_sums(const sw100_site_planes* site, int rows, int cols, cons
                                     (int)cudaSharedmemCarveoutMaxShared);
   });
   if (attr_err != cudaSuccess) return fail((int)attr_err, "cudaFuncSetAttribute: %s", cudaGetErrorString(attr_err));
-  dim3 block(kLoopBx, kLoopBy);
-  dim3 grid((cols + kLoopBx - 1) / kLoopBx, (rows + kLoopBy - 1) / kLoopBy);
+  dim3 block, grid;
+  if ((rc = loop_shape(*site, rows, cols, grid, block))) return rc;
   time_loop_sums_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
       make_site(*site), rows, cols, series->steps, series->n_t, series->patch, series->n_patches, series->gvf,
       reinterpret_cast<const float4*>(gsrc), series->n_day, state, out_mask, outputs, sums);

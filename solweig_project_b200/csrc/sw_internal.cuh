@@ -21,6 +21,8 @@ struct SitePlanes {
   const float* windcoeff;
   const uint32_t* bits;
   uint32_t single_step[SW100_CUBE_WORDS];
+  const int32_t* patch_order;
+  int32_t n_patch_order;
 };
 
 __host__ inline SitePlanes make_site(const sw100_site_planes& s) {
@@ -29,6 +31,8 @@ __host__ inline SitePlanes make_site(const sw100_site_planes& s) {
   d.walls = s.walls; d.aspect_rad = s.aspect_rad; d.tgk = s.tgk; d.tstart = s.tstart; d.alb = s.alb;
   d.emis = s.emis; d.class_idx = s.class_idx; d.windcoeff = s.windcoeff; d.bits = s.bits;
   for (int w = 0; w < SW100_CUBE_WORDS; ++w) d.single_step[w] = s.single_step[w];
+  d.patch_order = s.patch_order;
+  d.n_patch_order = s.n_patch_order;
   return d;
 }
 

@@ -309,7 +309,9 @@ struct GvfSums {
 };
 
 // All steps of the pixels of tile (bx, by); every thread of the block calls
-// it (the step tables are staged in shared memory).  `Site` is SitePlanes
+// it (the step tables are staged in shared memory).  With `order` (the
+// site's patch order, n_order patches) the block is instead four 8 x 4
+// pixel patches, warp w taking patch order[bx * 4 + w].  `Site` is SitePlanes
 // (a kernel parameter) or sw100_site_planes (a batch descriptor in global
 // memory): the same member names.
 // KNOWN_N0: reuse each walk's first-building step after the first daytime
@@ -325,7 +327,7 @@ __device__ __forceinline__ void time_loop_tile(
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
     float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs, int bx, int by,
-    const float* __restrict__ sums = nullptr) {
+    const float* __restrict__ sums = nullptr, const int32_t* __restrict__ order = nullptr, int n_order = 0) {
   // PP is filled with 16-byte vector stores: the array must be 16-byte
   // aligned (the struct itself only requires 8)
   __shared__ __align__(16) sw100_time_step P;
@@ -353,8 +355,15 @@ __device__ __forceinline__ void time_loop_tile(
     AZ[tid].facesh_hi = gvf_az[tid].facesh_hi;
     AZ[tid].dir_flags = gvf_az[tid].dir_flags;
   }
-  const int c = bx * blockDim.x + threadIdx.x;
-  const int r = by * blockDim.y + threadIdx.y;
+  int c = bx * blockDim.x + threadIdx.x;
+  int r = by * blockDim.y + threadIdx.y;
+  if (order != nullptr) {
+    const int k = bx * 4 + (tid >> 5), lane = tid & 31, pcols = (cols + 7) >> 3;
+    const int pt = k < n_order ? order[k] : -1;
+    const bool ok = pt >= 0 && pt < n_order;
+    r = ok ? (pt / pcols) * 4 + (lane >> 3) : rows;  // rows: no pixel
+    c = ok ? (pt % pcols) * 8 + (lane & 7) : cols;
+  }
   const bool live = (r < rows) && (c < cols);
   const size_t npix = (size_t)rows * cols;
   const size_t p = live ? (size_t)r * cols + c : 0;
@@ -704,8 +713,9 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_kernel(
     const sw100_patch_step* __restrict__ patch_steps, int n_patches,
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
     float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs) {
-  time_loop_tile<SitePlanes, true>(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day, state, out_mask, outputs,
-                 blockIdx.x, blockIdx.y);
+  time_loop_tile<SitePlanes, true>(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day, state,
+                                   out_mask, outputs, blockIdx.x, blockIdx.y, nullptr, site.patch_order,
+                                   site.n_patch_order);
 }
 
 // The same time loop with the dense patch sums precomputed on the tensor
@@ -716,7 +726,36 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_sums_kernel(
     const sw100_gvf_azimuth* __restrict__ gvf_az, const float4* __restrict__ gsrc, int n_day,
     float* __restrict__ state, uint32_t out_mask, float* __restrict__ outputs, const float* __restrict__ sums) {
   time_loop_tile<SitePlanes, true, true>(site, rows, cols, tsteps, n_t, patch_steps, n_patches, gvf_az, gsrc, n_day,
-                                         state, out_mask, outputs, blockIdx.x, blockIdx.y, sums);
+                                         state, out_mask, outputs, blockIdx.x, blockIdx.y, sums, site.patch_order,
+                                         site.n_patch_order);
+}
+
+// Ground-view walk work of the loops' 8 x 4 pixel patches, one warp per
+// patch: per azimuth the longest walk of its pixels to the first building
+// sample in the grid (at most `second` steps; 0 for a building pixel), as
+// gvf_walk stops, summed over the 18 azimuths.
+__global__ void __launch_bounds__(128) walk_work_kernel(const float* __restrict__ buildings, int rows, int cols,
+                                                         const sw100_gvf_azimuth* __restrict__ gvf, int second,
+                                                         int32_t* __restrict__ work, int n_patch) {
+  const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (k >= n_patch) return;  // whole warps: blocks of 128 threads
+  const int pcols = (cols + 7) >> 3;
+  const int r = (k / pcols) * 4 + (lane >> 3), c = (k % pcols) * 8 + (lane & 7);
+  const bool live = r < rows && c < cols;
+  const bool ground = live && buildings[(size_t)r * cols + c] != 0.f;
+  int total = 0;
+  for (int az = 0; az < SW100_N_GVF_AZ; ++az) {
+    int n0 = 0;
+    if (ground) {
+      n0 = second;
+      for (int n = 0; n < second; ++n) {
+        const int sr = r + gvf[az].dx[n], sc = c + gvf[az].dy[n];
+        if (in_grid(sr, sc, rows, cols) && buildings[(size_t)sr * cols + sc] == 0.f) { n0 = n; break; }
+      }
+    }
+    total += __reduce_max_sync(0xffffffffu, n0);
+  }
+  if (lane == 0) work[k] = total;
 }
 
 // The time loop of every site of a batch, tiles taken in list order.

@@ -860,6 +860,23 @@ class Series:
     class_idx: np.ndarray     # uint8 per pixel (None: the site's device plane holds the classes)
 
 
+def walk_steps(params: "ModelParams", scale) -> tuple:
+    """`first` and `second` of the ground-view walks in pixels, as float32:
+    the person height rounded (at least 1) and height * 20 rounded
+    (utci_process.py:847-853), each times the scale and rounded, first at
+    least 1 (solweig.py:143-146)."""
+    height = torch.tensor(params.height)
+    first = torch.round(height)
+    if first == 0.:
+        first = torch.tensor(1.)
+    second = torch.round(height * 20.)
+    sc = torch.tensor(scale)
+    first_g = torch.round(first * sc)
+    first_g = torch.tensor(1.) if first_g < 1 else first_g
+    second_g = torch.round(second * sc)
+    return F32(first_g.item()), F32(second_g.item())
+
+
 @torch.inference_mode()
 def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, location, scale, amax, rows, cols,
                  props: LandCoverProps, params: ModelParams = None, time_start=0, time_stop=None,
@@ -883,16 +900,7 @@ def build_series(*, met_file, altitude, azimuth, zen, jday, dectime, altmax, loc
     fdl, ldl = params.firstdayleaf, params.lastdayleaf
     leaf = ((DOY > fdl) | (DOY < ldl)) if fdl > ldl else ((DOY > fdl) & (DOY < ldl))
     psi = np.where(leaf, F32(1) * F32(params.transVeg), F32(0.5)).astype(F32)
-    height = torch.tensor(params.height)
-    first = torch.round(height)
-    if first == 0.:
-        first = torch.tensor(1.)
-    second = torch.round(height * 20.)
-    sc = torch.tensor(scale)
-    first_g = torch.round(first * sc)
-    first_g = torch.tensor(1.) if first_g < 1 else first_g
-    second_g = torch.round(second * sc)
-    first_f, second_f = F32(first_g.item()), F32(second_g.item())
+    first_f, second_f = walk_steps(params, scale)
     timestepdec = 0 if met_file.shape[0] == 1 else dectime[1] - dectime[0]
     if initial_scalars is None:
         timeadd, firstdaytime, CI = 0., 1., 1.0

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.sw100_abi_version() == 2
+    assert lib.sw100_abi_version() == N.ABI_VERSION == 3
 
 
 def test_workspace_queries(lib):

@@ -57,13 +57,13 @@ SVF_GATHER_BYTES_PER_STEP = 12    # 3 float32 gathers per march step
 # each kernel, from ncu captures: the flux loop at 500 x 500 x 24 (the default
 # workload), the SVF sweep and sun march at 1024 x 1024 scaled to a launch of
 # the measured size by pixel count (their traffic is per pixel).
-NCU_TRAFFIC = {"flux_loop": (500 * 500, 220_064_512), "svf_sweep": (1024 * 1024, 206_271_744),
+NCU_TRAFFIC = {"flux_loop": (500 * 500, 349_762_816), "svf_sweep": (1024 * 1024, 281_261_824),
                "sun_march": (1024 * 1024, 340_633_088)}
 # issue-slot utilisation (smsp__issue_active) of the same captures: the
 # binding roofline of these integer / FP32 kernels is instruction issue
-NCU_ISSUE_ACTIVE = {"flux_loop": 0.495, "svf_sweep": 0.758, "sun_march": 0.791, "patch_sums_tc": 0.386}
+NCU_ISSUE_ACTIVE = {"flux_loop": 0.516, "svf_sweep": 0.726, "sun_march": 0.791, "patch_sums_tc": 0.386}
 # active lanes per issued warp instruction (of 32) in the same captures
-NCU_ACTIVE_LANES = {"flux_loop": 25.08, "svf_sweep": 24.42, "sun_march": 26.50, "patch_sums_tc": 30.67}
+NCU_ACTIVE_LANES = {"flux_loop": 25.05, "svf_sweep": 24.27, "sun_march": 26.50, "patch_sums_tc": 30.67}
 # tensor-pipe activity (sm__pipe_tensor_cycles_active) of the patch-sum product at 500 x 500 x 24
 NCU_TENSOR_ACTIVE = {"patch_sums_tc": 0.142}
 # end-to-end calls timed after 2 warm-up calls; the median is reported (the

@@ -354,7 +354,7 @@ int sw100_pack_cubes(const float* shmat, const float* vegshmat, const float* vbs
  * that overlap on the GPU, on different streams or from different threads,
  * race on it and must be serialised by the caller.  Results are identical
  * to sw100_svf_sweep. */
-#define SW100_SVF_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024 + 256 * 1024 + 64 * 1024)
+#define SW100_SVF_NOALLOC_SCRATCH_BYTES (16 * 1024 * 1024 + 256 * 1024 + 64 * 1024 + 256)
 int sw100_svf_sweep_noalloc(const sw100_site_planes* site, int rows, int cols, const sw100_svf_plan* plan,
                             const sw100_step* steps, int n_steps, float* out_planes, uint32_t* out_bits,
                             void* stream);

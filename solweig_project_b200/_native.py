@@ -24,7 +24,7 @@ N_GVF_AZ = 18
 UTCI_TERMS = 210
 MAX_GVF_STEPS = 64
 SVF_PLANES = 19
-SVF_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024 + 256 * 1024 + 64 * 1024
+SVF_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024 + 256 * 1024 + 64 * 1024 + 256
 
 OUT_UTCI, OUT_TMRT, OUT_KUP, OUT_KDOWN, OUT_LUP, OUT_LDOWN, OUT_SHADOW = (1 << i for i in range(7))
 OUT_BITS = {"utci": OUT_UTCI, "tmrt": OUT_TMRT, "kup": OUT_KUP, "kdown": OUT_KDOWN, "lup": OUT_LUP,

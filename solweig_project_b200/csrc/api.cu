@@ -23,7 +23,7 @@ namespace sw100 {
 __global__ void pack4_kernel(const float* a, const float* b, const float* c, const float* d, size_t n, float4* out);
 __global__ void svf_sweep_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                  const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
-                                 uint32_t* bits, int n_steps, const float* skipmap);
+                                 uint32_t* bits, int n_steps, const float* skipmap, unsigned int* next, int n_patch);
 __global__ void svf_sweep_count_kernel(const float4* src4, int rows, int cols, const sw100_svf_plan* plan_g,
                                        const sw100_step* steps, const uint32_t* bflags, float vmax, float* out,
                                        uint32_t* bits, int n_steps, const float* skipmap,
@@ -208,6 +208,19 @@ int validate_series(const sw100_series* s) {
 }
 
 // Bytes of a site's skip map (one float per 8 x 8 cell block), aligned.
+// Blocks of `threads` threads of `kernel` resident on the current device at
+// once (occupancy x SM count): the grid of a persistent kernel.
+template <class K>
+int resident_blocks(K kernel, int threads, int* blocks) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  if (e != cudaSuccess) return fail((int)e, "occupancy query: %s", cudaGetErrorString(e));
+  *blocks = std::max(1, per_sm) * std::max(1, sms);
+  return 0;
+}
+
 int64_t skipmap_bytes(int rows, int cols) { return align_up((int64_t)((rows + 7) / 8) * ((cols + 7) / 8) * 4); }
 
 int launch_skipmap(const float4* src4, int rows, int cols, float* skipmap, cudaStream_t st) {
@@ -260,7 +273,9 @@ int sw100_svf_workspace_bytes(int rows, int cols, int n_steps, int64_t* bytes) {
   if ((rc = check_grid(rows, cols))) return rc;
   if ((rc = check_ptr(bytes, "bytes"))) return rc;
   if (n_steps < 0) return fail(SW100_E_ARG, "n_steps must be >= 0");
-  *bytes = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4) + skipmap_bytes(rows, cols);
+  // packed rasters, bush flags, skip map, the persistent sweep's patch counter
+  *bytes = align_up((int64_t)rows * cols * 16) + align_up((int64_t)n_steps * 4) + skipmap_bytes(rows, cols) +
+           kAlign;
   return 0;
 }
 
@@ -301,8 +316,15 @@ int run_svf_sweep(const sw100_site_planes* site, int rows, int cols, const sw100
   const dim3 sblock(kMarchBx, kMarchBy);
   const dim3 sgrid((cols + kMarchBx - 1) / kMarchBx, (rows + kMarchBy - 1) / kMarchBy);
   if (executed == nullptr) {
-    svf_sweep_kernel<<<sgrid, sblock, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
-                                               site->vmax, out_planes, out_bits, n_steps, skipmap);
+    unsigned int* next = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(skipmap) + skipmap_bytes(rows, cols));
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return fail((int)e, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+    const int n_patch = ((rows + 3) / 4) * ((cols + 7) / 8);
+    int blocks = 0;
+    if ((rc = resident_blocks(svf_sweep_kernel, 128, &blocks))) return rc;
+    blocks = std::max(1, std::min(blocks, (n_patch + 3) / 4));
+    svf_sweep_kernel<<<blocks, 128, 0, st>>>(src4, rows, cols, plan, steps, site->bush_any ? flags : nullptr,
+                                             site->vmax, out_planes, out_bits, n_steps, skipmap, next, n_patch);
     return check_launch("svf_sweep_kernel");
   }
   cudaError_t e = cudaMemsetAsync(executed, 0, sizeof(unsigned long long), st);

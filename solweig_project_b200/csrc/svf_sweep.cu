@@ -387,16 +387,30 @@ __global__ void svf_skipmap_kernel(const float4* __restrict__ src4, int rows, in
   skipmap_block_warp(src4, rows, cols, m, ccol, b, threadIdx.x & 31);
 }
 
+// Persistent sweep: as many 128-thread blocks as fit on the device at once;
+// each warp takes the next 8 x 4 pixel patch (k: rows 4 (k / pc) .. + 3,
+// columns 8 (k % pc) .. + 7, pc = ceil(cols / 8)) from the counter *next
+// (zero at launch) until all n_patch are taken.  The patches go out in grid
+// order, so the warps at work march neighbouring pixels; a warp that drew
+// short marches takes the next patch at once instead of idling until its
+// block is done, and there is no last partial wave of blocks.
 __global__ void __launch_bounds__(128, 12) svf_sweep_kernel(
     const float4* __restrict__ src4, int rows, int cols, const sw100_svf_plan* __restrict__ plan_g,
     const sw100_step* __restrict__ steps, const uint32_t* __restrict__ bflags, float vmax,
-    float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps, const float* __restrict__ skipmap) {
+    float* __restrict__ out, uint32_t* __restrict__ bits, int n_steps, const float* __restrict__ skipmap,
+    unsigned int* __restrict__ next, int n_patch) {
   __shared__ sw100_svf_plan plan;
   load_plan(plan_g, plan, n_steps);
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
-  if (r >= rows || c >= cols) return;
-  svf_sweep_pixel(src4, rows, cols, plan, steps, bflags, vmax, out, bits, r, c, SkipMap{skipmap, (cols + 7) / 8});
+  const int lane = threadIdx.x & 31, pcols = (cols + 7) >> 3;
+  for (;;) {
+    int k = 0;
+    if (lane == 0) k = (int)atomicAdd(next, 1u);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    if (k >= n_patch) break;  // warp-uniform
+    const int r = (k / pcols) * 4 + (lane >> 3), c = (k % pcols) * 8 + (lane & 7);
+    if (r < rows && c < cols)
+      svf_sweep_pixel(src4, rows, cols, plan, steps, bflags, vmax, out, bits, r, c, SkipMap{skipmap, pcols});
+  }
 }
 
 // The same sweep, also counting the source gathers its marches execute

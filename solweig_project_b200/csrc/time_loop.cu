@@ -733,7 +733,8 @@ __global__ void __launch_bounds__(kTileThreads, 6) time_loop_sums_kernel(
 // Ground-view walk work of the loops' 8 x 4 pixel patches, one warp per
 // patch: per azimuth the longest walk of its pixels to the first building
 // sample in the grid (at most `second` steps; 0 for a building pixel), as
-// gvf_walk stops, summed over the 18 azimuths.
+// gvf_walk stops, summed over the 18 azimuths.  The samples are read four
+// steps at a time (independent loads in flight, one test per group).
 __global__ void __launch_bounds__(128) walk_work_kernel(const float* __restrict__ buildings, int rows, int cols,
                                                          const sw100_gvf_azimuth* __restrict__ gvf, int second,
                                                          int32_t* __restrict__ work, int n_patch) {
@@ -745,13 +746,21 @@ __global__ void __launch_bounds__(128) walk_work_kernel(const float* __restrict_
   const bool ground = live && buildings[(size_t)r * cols + c] != 0.f;
   int total = 0;
   for (int az = 0; az < SW100_N_GVF_AZ; ++az) {
-    int n0 = 0;
-    if (ground) {
-      n0 = second;
-      for (int n = 0; n < second; ++n) {
-        const int sr = r + gvf[az].dx[n], sc = c + gvf[az].dy[n];
-        if (in_grid(sr, sc, rows, cols) && buildings[(size_t)sr * cols + sc] == 0.f) { n0 = n; break; }
+    int n0 = ground ? second : 0;
+    for (int n = 0; ground && n < second && n0 == second; n += 4) {
+      float v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int m = n + j;
+        v[j] = 1.f;
+        if (m < second) {
+          const int sr = r + gvf[az].dx[m], sc = c + gvf[az].dy[m];
+          if (in_grid(sr, sc, rows, cols)) v[j] = buildings[(size_t)sr * cols + sc];
+        }
       }
+#pragma unroll
+      for (int j = 3; j >= 0; --j)
+        if (v[j] == 0.f) n0 = n + j;  // the first building of the group wins
     }
     total += __reduce_max_sync(0xffffffffu, n0);
   }

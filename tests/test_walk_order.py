@@ -44,7 +44,7 @@ def walk_work_numpy(buildings, gvf, second):
 @pytest.mark.parametrize("shape", [(72, 61), (33, 17), (4, 8)])
 def test_walk_work_matches_definition(cuda, shape):
     import torch
-    from solweig_project_b200 import tables as T, timeseries as TS
+    from solweig_project_b200 import engine as E, tables as T, timeseries as TS
     _, site = _site(*shape)
     second = int(TS.walk_steps(site.params, site.scale)[1])
     order = site.walk_order()
@@ -56,9 +56,10 @@ def test_walk_work_matches_definition(cuda, shape):
     assert np.array_equal(got, want)
     o = order.cpu().numpy()
     assert np.array_equal(np.sort(o), np.arange(len(want)))             # a permutation of the patches
-    assert np.all(np.diff(got[o]) <= 0)                                  # heaviest first
-    ties = [o[got[o] == v] for v in np.unique(got)]
-    assert all(np.all(np.diff(t) > 0) for t in ties)                     # ties in grid order
+    level = got // max(1, (18 * second) // E.WALK_LEVELS)
+    assert np.all(np.diff(level[o]) <= 0)                                # heaviest level first
+    ties = [o[level[o] == v] for v in np.unique(level)]
+    assert all(np.all(np.diff(t) > 0) for t in ties)                     # grid order within a level
 
 
 @pytest.mark.gpu

@@ -265,10 +265,10 @@ def march_tables(consts: np.ndarray, first_index: int, amax, rows: int, cols: in
     counts = np.zeros(max(n, 1), np.int32)
     total = C.c_int64(0)
     cp = consts.ctypes.data if n else None
-    call("sw100_march_tables", cp, n, int(first_index), C.c_float(np.float32(amax)), int(rows), int(cols), None,
-         0, counts.ctypes.data, C.byref(total))
-    steps = np.zeros(int(total.value), STEP_DTYPE)
-    if total.value:
-        call("sw100_march_tables", cp, n, int(first_index), C.c_float(np.float32(amax)), int(rows), int(cols),
-             steps.ctypes.data, int(total.value), counts.ctypes.data, C.byref(total))
-    return steps, counts[:n].astype(np.int64)
+    # room for every march at its longest (max(rows, cols) + 3 - first_index
+    # steps): one call that counts and fills in one pass
+    cap = n * max(0, max(int(rows), int(cols)) + 3 - int(first_index))
+    buf = np.empty(max(cap, 1), STEP_DTYPE)
+    call("sw100_march_tables", cp, n, int(first_index), C.c_float(np.float32(amax)), int(rows), int(cols),
+         buf.ctypes.data, cap, counts.ctypes.data, C.byref(total))
+    return buf[:int(total.value)], counts[:n].astype(np.int64)

@@ -1103,6 +1103,33 @@ extern "C" int sw100_march_tables(const sw100_march_const* marches, int n_marche
   const int last = std::max(rows, cols) + 2;
   const int64_t len = last >= first_index ? (int64_t)last - first_index + 1 : 0;
   int64_t sum = 0;
+  if (steps && capacity >= (int64_t)n_marches * len) {
+    // room for every march at full length: count and fill in one pass, each
+    // march's steps written where the packed table puts them
+    sw100_step* t = steps;
+    for (int q = 0; q < n_marches; ++q) {
+      int64_t n = 0;
+      if (amax >= 0.f) {
+        n = len;
+        for (int64_t j = 0; j < len; ++j) {
+          const MarchStep s = march_step(marches[q], (float)(first_index + j));
+          t[j].dx = to_i32(s.dx);
+          t[j].dy = to_i32(s.dy);
+          t[j].dz = s.dz;
+          if (!step_ok(s, amax, rows, cols)) {
+            n = j + 1;
+            break;
+          }
+        }
+      }
+      counts[q] = (int32_t)n;
+      skip_flags(t, n);
+      t += n;
+      sum += n;
+    }
+    *total = sum;
+    return 0;
+  }
   for (int q = 0; q < n_marches; ++q) {
     int64_t n = 0;
     if (amax >= 0.f) {

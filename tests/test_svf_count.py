@@ -1,6 +1,7 @@
 """The counting SVF sweep (sw100_svf_sweep_count, used by bench.py for the
-sweep's algorithmic bytes) returns the plain sweep's planes and bits bit for
-bit, and counts no more source gathers than the step tables hold."""
+sweep's algorithmic bytes; one block per 8 x 16 tile) returns the plain,
+persistent sweep's planes and bits bit for bit, and counts no more source
+gathers than the step tables hold."""
 import numpy as np
 import pytest
 
@@ -32,3 +33,10 @@ def test_counting_sweep_matches_and_bounds(case, cuda):
     assert 0 < n <= table_steps * site.rows * site.cols
     # a second call restarts the count
     assert site.count_svf_gathers(planes, bits) == n
+    # the persistent sweep resets its patch counter: another sweep into
+    # fresh buffers writes the same result again
+    planes2 = torch.full_like(ref.planes, float("nan"))
+    bits2 = torch.full_like(ref.bits, -1)
+    site.launch_svf(planes2, bits2)
+    assert torch.equal(planes2.view(torch.int32), ref.planes.view(torch.int32))
+    assert torch.equal(bits2, ref.bits)

@@ -263,6 +263,10 @@ class DeviceSite:
                 getattr(table, k)[:] = [float(v) for v in tab[k]]
             table.valid = valid
         stats = torch.empty(N.SITE_STATS_WORDS, dtype=torch.int32, device=d)
+        if WALK_ORDER and self.rows * self.cols <= WALK_ORDER_MAX_PIXELS:
+            # the loops' azimuth table, copied (and synchronised on, once per
+            # process) while the stats read below waits for the device anyway
+            _gvf_dev(d, self._walk_second())
         t = self.t
         N.call("sw100_prepare_site", _ptr(t["dsm"]), _ptr(t["trees"]), _ptr(t["dem"]), _ptr(aspect_d), _ptr(lc_d),
                C.byref(table), self.rows, self.cols, _ptr(t["vegdsm"]), _ptr(t["vegdsm2"]), _ptr(t["bush"]),
@@ -346,7 +350,7 @@ class DeviceSite:
         buildings raster."""
         hit = self._cache.get("walk_order")
         if hit is None:
-            second = min(int(TS.walk_steps(self.params, self.scale)[1]), N.MAX_GVF_STEPS)
+            second = self._walk_second()
             gvf = _gvf_dev(self.device, second)
             n = ((self.rows + 3) // 4) * ((self.cols + 7) // 8)
             work = torch.empty(n, dtype=torch.int32, device=self.device)
@@ -356,6 +360,11 @@ class DeviceSite:
             order = torch.argsort(work // q, descending=True, stable=True).to(torch.int32)
             hit = self._cache["walk_order"] = (order, work, gvf)
         return hit[0]
+
+    def _walk_second(self) -> int:
+        """Steps of the ground-view walks (`second`, at most the tables'
+        MAX_GVF_STEPS)."""
+        return min(int(TS.walk_steps(self.params, self.scale)[1]), N.MAX_GVF_STEPS)
 
     def loop_site_struct(self) -> N.SitePlanes:
         """site_struct() with the patch order of the time / flux loops

@@ -221,6 +221,31 @@ def test_native_march_tables_equal_numpy_form(amax, first_index, rows, cols):
     assert steps.tobytes() == ref.tobytes()
 
 
+@pytest.mark.parametrize("amax", [40.0, 3.0])
+def test_native_march_tables_exact_capacity_equals_full_capacity(amax):
+    """A buffer of exactly the total step count (the count-then-fill path)
+    and one with room for every march at full length (the one-pass path)
+    give the same table and counts."""
+    import ctypes
+    rng = np.random.default_rng(5)
+    consts = np.zeros(40, N.MARCH_CONST_DTYPE)
+    consts["branch_y"] = rng.integers(0, 2, 40)
+    consts["ssin"] = rng.choice([-1.0, 1.0], 40)
+    consts["scos"] = rng.choice([-1.0, 1.0], 40)
+    consts["tan_a"] = rng.uniform(-3, 3, 40).astype(np.float32)
+    consts["ds"] = np.float32(1.0)
+    consts["tanalt"] = np.float32(10.0) ** rng.uniform(-1, 1, 40).astype(np.float32)
+    full, counts = N.march_tables(consts, 1, np.float32(amax), 90, 70)
+    lib = N.load()
+    exact = np.zeros(len(full), N.STEP_DTYPE)
+    c2 = np.zeros(40, np.int32)
+    total = ctypes.c_int64(0)
+    rc = lib.sw100_march_tables(consts.ctypes.data, 40, 1, ctypes.c_float(amax), 90, 70, exact.ctypes.data,
+                                len(exact), c2.ctypes.data, ctypes.byref(total))
+    assert rc == 0 and total.value == len(full) < 40 * (90 + 2)
+    assert exact.tobytes() == full.tobytes() and list(c2) == list(counts)
+
+
 def test_native_march_tables_refuse_small_capacity():
     import ctypes
     consts = np.zeros(2, N.MARCH_CONST_DTYPE)
